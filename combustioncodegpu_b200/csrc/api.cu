@@ -1,0 +1,873 @@
+// C ABI of the sm_100a residual path (include/cc_b200.h).
+//
+// A context owns: the arena layout of all blocks, the device fields, the
+// halo program, the tile list of the stage kernel and one captured CUDA graph
+// per (time scheme, parity of the ping-pong buffers).  Everything up to
+// cc_init is host-only, so set-up errors surface without a device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cc_b200.h"
+#include "halo_plan.h"
+#include "launch.h"
+
+using namespace ccb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                                           \
+  do {                                                                                                     \
+    cudaError_t e_ = (call);                                                                               \
+    if (e_ != cudaSuccess)                                                                                 \
+      return fail(CC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_) + " (" + __FILE__ + ":" + \
+                                   std::to_string(__LINE__) + ")");                                        \
+  } while (0)
+
+template <typename T>
+struct Tag {
+  using type = T;
+};
+template <int V>
+struct IntC {
+  static constexpr int value = V;
+};
+
+}  // namespace
+
+struct cc_ctx {
+  ChemParams chem{};
+  int ngg = 2;
+  std::vector<HostBlock> blocks;
+  std::vector<std::vector<double>> h_geo;  // per block [10][Ng] user layout (jac, metric)
+  std::vector<HostBc> bcs;
+  std::vector<std::vector<double>> pend_bv, pend_yk;
+  std::vector<char> pend;  // block has pending host state
+
+  bool initialized = false;
+  bool state_dirty = false;
+  int precision = CC_FP64;
+  size_t elem = 8;
+  int ns_key = -1;  // 0, 9 or -1 (runtime)
+
+  int64_t N = 0, n_int = 0;
+  std::vector<BlockInfo> hblocks;
+  std::vector<Tile> htiles;
+  BlockInfo *d_blocks = nullptr;
+  Tile *d_tiles = nullptr;
+  void *P[2] = {nullptr, nullptr};
+  void *Pr[2] = {nullptr, nullptr};
+  void *G = nullptr;
+  double *Q[2] = {nullptr, nullptr};
+  double *stage64 = nullptr;  // FP64 staging [6+ns][N] of the uploaded state
+  double *tmp64 = nullptr;    // [N]
+  int cur = 0;                // P/Pr buffer holding the current state
+  int qcur = 0;               // Q buffer holding the current state
+
+  HaloPlan plan;
+  HaloNode *d_nodes = nullptr;
+  HaloCopy *d_copies = nullptr;
+  void *sP = nullptr, *sPr = nullptr;
+  double *sQ = nullptr;
+  int64_t ns_cap = 1;
+  BcDevice *d_bcs = nullptr;
+
+  double *d_dt = nullptr;
+  unsigned long long *d_dt_next = nullptr;
+  unsigned *d_status = nullptr;
+  double *d_res = nullptr;
+  double *d_partials = nullptr;
+  double *d_last = nullptr;
+  int n_partials = 296;
+
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool use_graph = true;
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int64_t device_bytes = 0;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+int nv_of(const cc_ctx *c) { return 5 + c->chem.ns; }
+int np_of(const cc_ctx *c) { return 6 + c->chem.ns; }
+int npr_of(const cc_ctx *c) { return 2 + c->chem.ns; }
+
+int dev_alloc(cc_ctx *c, void **p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  CK(cudaMalloc(p, bytes));
+  CK(cudaMemset(*p, 0, bytes));
+  c->allocs.push_back(*p);
+  c->device_bytes += (int64_t)bytes;
+  return 0;
+}
+
+template <typename F>
+int dispatch(cc_ctx *c, F &&f) {
+  const bool dbl = c->precision == CC_FP64;
+  switch (c->ns_key) {
+    case 0:
+      return dbl ? f(Tag<double>{}, IntC<0>{}) : f(Tag<float>{}, IntC<0>{});
+    case 9:
+      return dbl ? f(Tag<double>{}, IntC<9>{}) : f(Tag<float>{}, IntC<9>{});
+    default:
+      return dbl ? f(Tag<double>{}, IntC<-1>{}) : f(Tag<float>{}, IntC<-1>{});
+  }
+}
+
+template <typename T>
+void fill_tables(SpecTables<T> &S, const cc_params *p) {
+  std::memset(&S, 0, sizeof(S));
+  const int ns = p->n_spec;
+  for (int k = 0; k < ns; ++k) {
+    const double mw = p->mw[k];
+    S.mw[k] = (T)mw;
+    S.inv_mw[k] = (T)(1.0 / mw);
+    S.r_over_mw[k] = (T)(kRu / mw);
+    S.cv_shift[k] = (T)(kRu / mw);
+    S.t_low[k] = (T)p->t_low[k];
+    S.t_mid[k] = (T)p->t_mid[k];
+    const double *lo = p->low_temp_coeff + 7 * k, *hi = p->high_temp_coeff + 7 * k;
+    for (int c = 0; c < 5; ++c) S.cp_lo[k][c] = (T)lo[c], S.cp_hi[k][c] = (T)hi[c];
+    const double sc[5] = {1.0, 0.5, 1.0 / 3.0, 0.25, 0.2};
+    for (int c = 0; c < 5; ++c) S.h_lo[k][c] = (T)(lo[c] * sc[c]), S.h_hi[k][c] = (T)(hi[c] * sc[c]);
+    S.h_lo[k][2] = (T)(lo[2] / 3), S.h_hi[k][2] = (T)(hi[2] / 3);
+    S.h_lo[k][5] = (T)lo[5], S.h_hi[k][5] = (T)hi[5];
+    S.lj_inv[k] = (T)p->LJ_potent_inv[k];
+    S.vis_coeff[k] = (T)p->vis_coeff[k];
+    S.lam_shift[k] = (T)(1.25 * kRu / mw);
+    for (int n = 0; n < ns; ++n) {
+      S.wj[k * kMaxSpec + n] = (T)p->WjDivWi_to_One4th[k * ns + n];
+      S.sw[k * kMaxSpec + n] = (T)p->sqrt_WiDivWjPl1Mul8[k * ns + n];
+    }
+  }
+}
+
+int64_t ng_user(const HostBlock &b) {
+  return (int64_t)(b.mx + 2 * b.g) * (b.my + 2 * b.g) * (b.mz + 2 * b.g);
+}
+
+// host [nf][Ng] user layout <-> arena rows (pitched copy per field)
+int copy_fields_h2d(cc_ctx *c, const HostBlock &b, const double *host, double *dev, int nf) {
+  const size_t w = (size_t)(b.mx + 2 * b.g) * sizeof(double);
+  const size_t rows = (size_t)(b.my + 2 * b.g) * (b.mz + 2 * b.g);
+  const int64_t ng = ng_user(b);
+  for (int f = 0; f < nf; ++f)
+    CK(cudaMemcpy2DAsync(dev + (int64_t)f * c->N + b.off, (size_t)b.nx * sizeof(double), host + (int64_t)f * ng, w, w,
+                         rows, cudaMemcpyHostToDevice, c->stream));
+  return 0;
+}
+
+int copy_field_d2h(cc_ctx *c, const HostBlock &b, const double *dev_field, double *host_field) {
+  const size_t w = (size_t)(b.mx + 2 * b.g) * sizeof(double);
+  const size_t rows = (size_t)(b.my + 2 * b.g) * (b.mz + 2 * b.g);
+  CK(cudaMemcpy2DAsync(host_field, w, dev_field + b.off, (size_t)b.nx * sizeof(double), w, rows,
+                       cudaMemcpyDeviceToHost, c->stream));
+  return 0;
+}
+
+// T-precision field f of arena `src` -> FP64 tmp64
+int field_to64(cc_ctx *c, const void *src, int f) {
+  if (c->precision == CC_FP64) {
+    CK(cudaMemcpyAsync(c->tmp64, (const double *)src + (int64_t)f * c->N, sizeof(double) * c->N,
+                       cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    CK(launch_convert_f2d((const float *)src + (int64_t)f * c->N, c->tmp64, c->N, c->stream));
+  }
+  return 0;
+}
+
+int from64(cc_ctx *c, const double *src, void *dst, int64_t count) {
+  if (c->precision == CC_FP64)
+    CK(cudaMemcpyAsync(dst, src, sizeof(double) * count, cudaMemcpyDeviceToDevice, c->stream));
+  else
+    CK(launch_convert_d2f(src, (float *)dst, count, c->stream));
+  return 0;
+}
+
+// Stage-kernel work list: kTX x kTY columns, k split into chunks of kz.
+void build_tiles(cc_ctx *c) {
+  int slots_per_sm = c->precision == CC_FP64 ? 1 : 2;
+  int n_sm = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  const int slots = n_sm * slots_per_sm;
+  int max_mz = 1;
+  for (const auto &b : c->blocks) max_mz = std::max(max_mz, b.mz);
+  int best_kz = max_mz;
+  double best_cost = 1e300;
+  const char *env = std::getenv("CC_KZ");
+  if (env && std::atoi(env) > 0) {
+    best_kz = std::atoi(env);
+  } else {
+    for (int kz = 1; kz <= max_mz; ++kz) {
+      int64_t tiles = 0;
+      for (const auto &b : c->blocks)
+        tiles += (int64_t)((b.mx + kTX - 1) / kTX) * ((b.my + kTY - 1) / kTY) * ((b.mz + kz - 1) / kz);
+      const double waves = std::ceil((double)tiles / slots);
+      const double cost = waves * (kz + 1.0);
+      if (cost < best_cost - 1e-9) best_cost = cost, best_kz = kz;
+    }
+  }
+  c->htiles.clear();
+  for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
+    const auto &b = c->blocks[bi];
+    for (int k0 = 0; k0 < b.mz; k0 += best_kz)
+      for (int j0 = 0; j0 < b.my; j0 += kTY)
+        for (int i0 = 0; i0 < b.mx; i0 += kTX) {
+          Tile t{};
+          t.blk = bi, t.i0 = i0, t.j0 = j0, t.k0 = k0, t.k1 = std::min(b.mz, k0 + best_kz);
+          c->htiles.push_back(t);
+        }
+  }
+}
+
+int upload_bcs(cc_ctx *c) {
+  std::vector<BcDevice> h(std::max<size_t>(1, c->bcs.size()));
+  for (size_t i = 0; i < c->bcs.size(); ++i) {
+    const HostBc &b = c->bcs[i];
+    BcDevice &d = h[i];
+    std::memset(&d, 0, sizeof d);
+    d.kind = b.kind, d.thermal_type = b.thermal_type, d.t_wall = b.t_wall;
+    d.rho = b.rho, d.u = b.u, d.v = b.v, d.w = b.w, d.p = b.p, d.T = b.T;
+    for (int l = 0; l < kMaxSpec; ++l) d.yk[l] = b.yk[l];
+  }
+  CK(cudaMemcpyAsync(c->d_bcs, h.data(), sizeof(BcDevice) * h.size(), cudaMemcpyHostToDevice, c->stream));
+  return 0;
+}
+
+// Layout, device allocation, halo program, geometry.  Runs once.
+int setup_device(cc_ctx *c) {
+  const int ns = c->chem.ns;
+  c->elem = c->precision == CC_FP64 ? 8 : 4;
+  c->ns_key = ns == 0 ? 0 : (ns == 9 ? 9 : -1);
+  // arena layout: rows padded to 32 points, interior i=0 on a 32-point boundary
+  int64_t end = 0, n_int = 0;
+  c->hblocks.clear();
+  for (auto &b : c->blocks) {
+    b.g = c->ngg;
+    b.nx = ((b.mx + 2 * b.g + 31) / 32) * 32;
+    b.ny = b.my + 2 * b.g;
+    b.nz = b.mz + 2 * b.g;
+    int64_t off = ((end + b.g + 31) / 32) * 32 - b.g;
+    b.off = off;
+    b.base = off + b.g + (int64_t)b.nx * b.g + (int64_t)b.nx * b.ny * b.g;
+    end = off + (int64_t)b.nx * b.ny * b.nz;
+    BlockInfo bi{};
+    bi.mx = b.mx, bi.my = b.my, bi.mz = b.mz, bi.g = b.g, bi.nx = b.nx, bi.ny = b.ny, bi.nz = b.nz;
+    bi.base = b.base, bi.off = b.off, bi.ng = (int64_t)b.nx * b.ny * b.nz, bi.interior_off = n_int;
+    n_int += (int64_t)b.mx * b.my * b.mz;
+    c->hblocks.push_back(bi);
+  }
+  c->N = ((end + 31) / 32) * 32;
+  c->n_int = n_int;
+
+  std::vector<HostBc> bcs = c->bcs;
+  if (!build_halo_plan(c->blocks, bcs, c->plan)) return fail(CC_ERR_TOPOLOGY, "halo program: " + c->plan.error);
+  build_tiles(c);
+
+  const size_t E = c->elem;
+  const int64_t N = c->N;
+  void *p;
+  if (dev_alloc(c, &p, sizeof(BlockInfo) * c->hblocks.size())) return CC_ERR_CUDA;
+  c->d_blocks = (BlockInfo *)p;
+  if (dev_alloc(c, &p, sizeof(Tile) * std::max<size_t>(1, c->htiles.size()))) return CC_ERR_CUDA;
+  c->d_tiles = (Tile *)p;
+  for (int b = 0; b < 2; ++b) {
+    if (dev_alloc(c, &c->P[b], E * N * np_of(c))) return CC_ERR_CUDA;
+    if (dev_alloc(c, &c->Pr[b], E * N * npr_of(c))) return CC_ERR_CUDA;
+    if (dev_alloc(c, &p, sizeof(double) * N * nv_of(c))) return CC_ERR_CUDA;
+    c->Q[b] = (double *)p;
+  }
+  if (dev_alloc(c, &c->G, E * N * 10)) return CC_ERR_CUDA;
+  if (dev_alloc(c, &p, sizeof(double) * N * std::max(np_of(c), 10))) return CC_ERR_CUDA;
+  c->stage64 = (double *)p;
+  if (dev_alloc(c, &p, sizeof(double) * N)) return CC_ERR_CUDA;
+  c->tmp64 = (double *)p;
+  c->ns_cap = std::max<int64_t>(1, c->plan.n_slots);
+  if (dev_alloc(c, &c->sP, E * c->ns_cap * np_of(c))) return CC_ERR_CUDA;
+  if (dev_alloc(c, &c->sPr, E * c->ns_cap * npr_of(c))) return CC_ERR_CUDA;
+  if (dev_alloc(c, &p, sizeof(double) * c->ns_cap * nv_of(c))) return CC_ERR_CUDA;
+  c->sQ = (double *)p;
+  if (dev_alloc(c, &p, sizeof(HaloNode) * std::max<size_t>(1, c->plan.nodes.size()))) return CC_ERR_CUDA;
+  c->d_nodes = (HaloNode *)p;
+  if (dev_alloc(c, &p, sizeof(HaloCopy) * std::max<size_t>(1, c->plan.copies.size()))) return CC_ERR_CUDA;
+  c->d_copies = (HaloCopy *)p;
+  if (dev_alloc(c, &p, sizeof(BcDevice) * std::max<size_t>(1, c->bcs.size()))) return CC_ERR_CUDA;
+  c->d_bcs = (BcDevice *)p;
+  if (dev_alloc(c, &p, sizeof(double) * 4)) return CC_ERR_CUDA;
+  c->d_dt = (double *)p;
+  if (dev_alloc(c, &p, sizeof(unsigned long long))) return CC_ERR_CUDA;
+  c->d_dt_next = (unsigned long long *)p;
+  if (dev_alloc(c, &p, sizeof(unsigned) * 4)) return CC_ERR_CUDA;
+  c->d_status = (unsigned *)p;
+  if (dev_alloc(c, &p, sizeof(double) * 4)) return CC_ERR_CUDA;
+  c->d_res = (double *)p;
+  if (dev_alloc(c, &p, sizeof(double) * 4 * c->n_partials)) return CC_ERR_CUDA;
+  c->d_partials = (double *)p;
+  if (dev_alloc(c, &p, sizeof(double) * 4 * std::max<int64_t>(1, c->n_int))) return CC_ERR_CUDA;
+  c->d_last = (double *)p;
+
+  CK(cudaMemcpyAsync(c->d_blocks, c->hblocks.data(), sizeof(BlockInfo) * c->hblocks.size(), cudaMemcpyHostToDevice,
+                     c->stream));
+  if (!c->htiles.empty())
+    CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+  if (!c->plan.nodes.empty())
+    CK(cudaMemcpyAsync(c->d_nodes, c->plan.nodes.data(), sizeof(HaloNode) * c->plan.nodes.size(),
+                       cudaMemcpyHostToDevice, c->stream));
+  if (!c->plan.copies.empty())
+    CK(cudaMemcpyAsync(c->d_copies, c->plan.copies.data(), sizeof(HaloCopy) * c->plan.copies.size(),
+                       cudaMemcpyHostToDevice, c->stream));
+  const unsigned long long inf_bits = 0x7ff0000000000000ull;
+  CK(cudaMemcpyAsync(c->d_dt_next, &inf_bits, sizeof inf_bits, cudaMemcpyHostToDevice, c->stream));
+  if (int r = upload_bcs(c)) return r;
+
+  // geometry: user layout -> FP64 staging -> bulk precision
+  CK(cudaMemsetAsync(c->stage64, 0, sizeof(double) * N * 10, c->stream));
+  for (size_t b = 0; b < c->blocks.size(); ++b)
+    if (int r = copy_fields_h2d(c, c->blocks[b], c->h_geo[b].data(), c->stage64, 10)) return r;
+  if (int r = from64(c, c->stage64, c->G, N * 10)) return r;
+  CK(cudaMemsetAsync(c->stage64, 0, sizeof(double) * N * std::max(np_of(c), 10), c->stream));
+  return 0;
+}
+
+template <typename T, int NS>
+HaloArgs<T> halo_args(cc_ctx *c, int pn, int pp, double *qn, const double *qp) {
+  HaloArgs<T> h{};
+  h.N = c->N;
+  h.NS_cap = c->ns_cap;
+  h.P = (T *)c->P[pn];
+  h.Pprev = (const T *)c->P[pp];
+  h.Pr = (T *)c->Pr[pn];
+  h.Prprev = (const T *)c->Pr[pp];
+  h.Q = qn;
+  h.Qprev = qp;
+  h.sP = (T *)c->sP;
+  h.sPr = (T *)c->sPr;
+  h.sQ = c->sQ;
+  h.bcs = c->d_bcs;
+  h.nodes = c->d_nodes;
+  h.copies = c->d_copies;
+  return h;
+}
+
+template <typename T, int NS>
+int run_halo(cc_ctx *c, int pn, int pp, double *qn, const double *qp) {
+  HaloArgs<T> h = halo_args<T, NS>(c, pn, pp, qn, qp);
+  const auto &lb = c->plan.level_begin;
+  for (size_t l = 0; l + 1 < lb.size(); ++l) {
+    h.begin = lb[l], h.end = lb[l + 1];
+    CK((Launch<T, NS>::halo_nodes(h, c->chem, c->stream)));
+  }
+  h.begin = 0, h.end = (int64_t)c->plan.copies.size();
+  CK((Launch<T, NS>::halo_copies(h, np_of(c), npr_of(c), nv_of(c), c->stream)));
+  return 0;
+}
+
+// Driver::initialize_computation from the FP64 staging arena: conserved
+// variables at every point, properties, boundary conditions and interfaces,
+// time step.  Afterwards the current state is P[1], Pr[1], Q[0].
+template <typename T, int NS>
+int derive_state(cc_ctx *c) {
+  const int64_t N = c->N;
+  c->qcur = 0;
+  CK((Launch<T, NS>::configure()));
+  CK((Launch<T, NS>::cv_from_bv(c->chem, c->stage64, c->Q[0], N, c->stream)));
+  CK(cudaMemcpyAsync(c->Q[1], c->Q[0], sizeof(double) * N * nv_of(c), cudaMemcpyDeviceToDevice, c->stream));
+  if (int r = from64(c, c->stage64, c->P[0], N * np_of(c))) return r;
+  CK((Launch<T, NS>::props_all(c->chem, (const T *)c->P[0], (T *)c->Pr[0], N, c->stream)));
+  CK(cudaMemcpyAsync(c->P[1], c->P[0], c->elem * N * np_of(c), cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->Pr[1], c->Pr[0], c->elem * N * npr_of(c), cudaMemcpyDeviceToDevice, c->stream));
+  if (int r = run_halo<T, NS>(c, 1, 0, c->Q[0], c->Q[1])) return r;
+  c->cur = 1;
+  // inflow transport properties: evaluated once by the same point function
+  CK((Launch<T, NS>::dt_reduce(c->chem, c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[1],
+                               (const T *)c->Pr[1], (const T *)c->G, N, c->n_int, c->d_dt_next, c->stream)));
+  CK(launch_dt_finalize(c->d_dt, c->d_dt_next, c->d_status, nullptr, c->stream));
+  c->state_dirty = false;
+  return 0;
+}
+
+// Inflow conditions need rho*E and transport properties of their state;
+// evaluated on the device through a one-point arena slice of stage64.
+template <typename T, int NS>
+int prepare_inflow(cc_ctx *c) {
+  bool any = false;
+  for (const auto &b : c->bcs) any = any || b.kind == 5;
+  if (!any) return 0;
+  const int ns = c->chem.ns;
+  const int np = np_of(c);
+  const int64_t M = (int64_t)c->bcs.size();
+  // host FP64 primitives [np][M]
+  std::vector<double> h((size_t)np * M, 0.0);
+  for (int64_t i = 0; i < M; ++i) {
+    const HostBc &b = c->bcs[i];
+    const double v[6] = {b.rho, b.u, b.v, b.w, b.p, b.T};
+    for (int f = 0; f < 6; ++f) h[f * M + i] = b.kind == 5 ? v[f] : 0.0;
+    for (int l = 0; l < ns; ++l) h[(6 + l) * M + i] = b.yk[l];
+  }
+  double *dP = nullptr, *dQ = nullptr;
+  void *dPT = nullptr, *dPr = nullptr;
+  CK(cudaMalloc(&dP, sizeof(double) * np * M));
+  CK(cudaMalloc(&dQ, sizeof(double) * nv_of(c) * M));
+  CK(cudaMalloc(&dPT, c->elem * np * M));
+  CK(cudaMalloc(&dPr, c->elem * npr_of(c) * M));
+  CK(cudaMemcpyAsync(dP, h.data(), sizeof(double) * np * M, cudaMemcpyHostToDevice, c->stream));
+  CK((Launch<T, NS>::cv_from_bv(c->chem, dP, dQ, M, c->stream)));
+  if (int r = from64(c, dP, dPT, np * M)) return r;
+  CK((Launch<T, NS>::props_all(c->chem, (const T *)dPT, (T *)dPr, M, c->stream)));
+  std::vector<double> q((size_t)nv_of(c) * M);
+  std::vector<T> pr((size_t)npr_of(c) * M);
+  CK(cudaMemcpyAsync(q.data(), dQ, sizeof(double) * q.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(pr.data(), dPr, sizeof(T) * pr.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(dP), cudaFree(dQ), cudaFree(dPT), cudaFree(dPr);
+  std::vector<BcDevice> hb(M);
+  for (int64_t i = 0; i < M; ++i) {
+    const HostBc &b = c->bcs[i];
+    BcDevice &d = hb[i];
+    std::memset(&d, 0, sizeof d);
+    d.kind = b.kind, d.thermal_type = b.thermal_type, d.t_wall = b.t_wall;
+    d.rho = b.rho, d.u = b.u, d.v = b.v, d.w = b.w, d.p = b.p, d.T = b.T;
+    for (int l = 0; l < kMaxSpec; ++l) d.yk[l] = b.yk[l];
+    if (b.kind == 5) {
+      d.rhoE = q[4 * M + i];
+      d.mu = (double)pr[i];
+      d.lam = (double)pr[M + i];
+      for (int l = 0; l < ns; ++l) d.rho_d[l] = (double)pr[(2 + l) * M + i];
+    }
+  }
+  CK(cudaMemcpyAsync(c->d_bcs, hb.data(), sizeof(BcDevice) * M, cudaMemcpyHostToDevice, c->stream));
+  return 0;
+}
+
+template <typename T, int NS>
+int enqueue_step(cc_ctx *c, int scheme) {
+  StageArgs<T> a{};
+  a.blocks = c->d_blocks;
+  a.tiles = c->d_tiles;
+  a.N = c->N;
+  a.G = (const T *)c->G;
+  a.dt = c->d_dt;
+  a.status = c->d_status;
+  a.renorm_y = (c->precision != CC_FP64 && c->chem.ns > 0) ? 1 : 0;
+  const int nt = (int)c->htiles.size();
+  if (scheme == CC_STEADY_EULER) {
+    const int pc = c->cur, pn = 1 - c->cur;
+    a.P = (const T *)c->P[pc], a.Pn = (T *)c->P[pn], a.Pr = (const T *)c->Pr[pc], a.Prn = (T *)c->Pr[pn];
+    a.Qin = c->Q[c->qcur], a.Qn = nullptr, a.Qout = c->Q[c->qcur];
+    a.a = 0.0, a.b = 1.0, a.local_dt = 1, a.dt_next = nullptr;
+    CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
+    if (int r = run_halo<T, NS>(c, pn, pc, c->Q[c->qcur], c->Q[c->qcur])) return r;
+    c->cur = pn;
+    return 0;
+  }
+  static const double A[3] = {0.0, 0.75, 1.0 / 3.0};
+  static const double Bc[3] = {1.0, 0.25, 2.0 / 3.0};
+  double *qa = c->Q[c->qcur], *qb = c->Q[1 - c->qcur];
+  for (int st = 0; st < 3; ++st) {
+    const int pc = c->cur, pn = 1 - c->cur;
+    a.P = (const T *)c->P[pc], a.Pn = (T *)c->P[pn], a.Pr = (const T *)c->Pr[pc], a.Prn = (T *)c->Pr[pn];
+    const double *qin = st == 0 ? qa : qb;
+    double *qout = st == 2 ? qa : qb;
+    a.Qin = qin, a.Qn = qa, a.Qout = qout;
+    a.a = A[st], a.b = Bc[st], a.local_dt = 0;
+    a.dt_next = (st == 2 && !c->plan.has_wall) ? c->d_dt_next : nullptr;
+    CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
+    if (int r = run_halo<T, NS>(c, pn, pc, qout, qin)) return r;
+    c->cur = pn;
+  }
+  if (c->plan.has_wall)
+    CK((Launch<T, NS>::dt_reduce(c->chem, c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur],
+                                 (const T *)c->Pr[c->cur], (const T *)c->G, c->N, c->n_int, c->d_dt_next,
+                                 c->stream)));
+  CK(launch_dt_finalize(c->d_dt, c->d_dt_next, c->d_status, c->d_dt + 1, c->stream));
+  return 0;
+}
+
+void destroy_graphs(cc_ctx *c) {
+  for (auto &row : c->graph)
+    for (auto &g : row)
+      if (g) cudaGraphExecDestroy(g), g = nullptr;
+}
+
+template <typename T, int NS>
+int step_once(cc_ctx *c, int scheme) {
+  if (!c->use_graph) return enqueue_step<T, NS>(c, scheme);
+  cudaGraphExec_t &ge = c->graph[scheme][c->cur];
+  if (!ge) {
+    const int cur0 = c->cur;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int r = enqueue_step<T, NS>(c, scheme);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->cur = cur0;
+    if (r) return r;
+    if (e != cudaSuccess) return fail(CC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(CC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  CK(cudaGraphLaunch(ge, c->stream));
+  c->cur = (scheme == CC_RK3) ? 1 - c->cur : 1 - c->cur;  // 3 or 1 buffer swaps: odd either way
+  return 0;
+}
+
+int validate_params(const cc_params *p) {
+  if (!p) return fail(CC_ERR_ARG, "params is null");
+  if (p->n_spec < 0 || p->n_spec > CC_MAX_SPECIES) return fail(CC_ERR_ARG, "n_spec out of range [0,16]");
+  if (p->ngg != 2) return fail(CC_ERR_ARG, "only ngg = 2 is supported (MUSCL/AUSM+ and 2nd-order viscous)");
+  if (p->inviscid_scheme != 3) return fail(CC_ERR_ARG, "only inviscid_scheme 3 (AUSM+) exists in the reference");
+  if (p->viscous_order != 0 && p->viscous_order != 2) return fail(CC_ERR_ARG, "viscous_order must be 0 or 2");
+  if (p->limiter != 0 && p->limiter != 1) return fail(CC_ERR_ARG, "limiter must be 0 or 1 (minmod)");
+  if (!(p->cfl > 0) || !(p->prandtl_number > 0)) return fail(CC_ERR_ARG, "cfl and prandtl_number must be positive");
+  if (p->n_spec > 0) {
+    if (!p->mw || !p->t_low || !p->t_mid || !p->low_temp_coeff || !p->high_temp_coeff || !p->LJ_potent_inv ||
+        !p->vis_coeff || !p->WjDivWi_to_One4th || !p->sqrt_WiDivWjPl1Mul8)
+      return fail(CC_ERR_ARG, "species tables missing");
+    if (!(p->schmidt_number > 0)) return fail(CC_ERR_ARG, "schmidt_number must be positive");
+  }
+  return 0;
+}
+
+int check_ctx(cc_ctx *c) { return c ? 0 : fail(CC_ERR_ARG, "context is null"); }
+
+}  // namespace
+
+extern "C" {
+
+const char *cc_last_error(void) { return g_err.c_str(); }
+
+int cc_version(void) { return 10000; }
+
+int cc_device_count(int *n) {
+  if (!n) return fail(CC_ERR_ARG, "n is null");
+  int k = 0;
+  cudaError_t e = cudaGetDeviceCount(&k);
+  if (e != cudaSuccess) k = 0, cudaGetLastError();
+  *n = k;
+  return 0;
+}
+
+int cc_create(const cc_params *params, cc_ctx **out) {
+  if (!out) return fail(CC_ERR_ARG, "out is null");
+  *out = nullptr;
+  if (int r = validate_params(params)) return r;
+  cc_ctx *c = new cc_ctx;
+  c->ngg = params->ngg;
+  c->chem.ns = params->n_spec;
+  c->chem.nv = 5 + params->n_spec;
+  c->chem.reconstruction = params->reconstruction;
+  c->chem.viscous = params->viscous_order == 2 ? 1 : 0;
+  c->chem.Pr = params->prandtl_number;
+  c->chem.cfl = params->cfl;
+  c->chem.Sc = params->n_spec > 0 ? params->schmidt_number : 1.0;
+  fill_tables(c->chem.d, params);
+  fill_tables(c->chem.f, params);
+  *out = c;
+  return 0;
+}
+
+int cc_destroy(cc_ctx *c) {
+  if (!c) return 0;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  destroy_graphs(c);
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+int cc_add_block(cc_ctx *c, int mx, int my, int mz, const double *jac, const double *metric, int *block_id) {
+  if (int r = check_ctx(c)) return r;
+  if (c->initialized) return fail(CC_ERR_STATE, "blocks must be added before cc_init");
+  if (mx < 1 || my < 1 || mz < 1) return fail(CC_ERR_ARG, "block extents must be positive");
+  if (!jac || !metric) return fail(CC_ERR_ARG, "jac and metric are required");
+  HostBlock b{};
+  b.mx = mx, b.my = my, b.mz = mz, b.g = c->ngg;
+  const int64_t ng = ng_user(b);
+  std::vector<double> geo((size_t)ng * 10);
+  std::memcpy(geo.data(), jac, sizeof(double) * ng);
+  std::memcpy(geo.data() + ng, metric, sizeof(double) * ng * 9);
+  c->blocks.push_back(b);
+  c->h_geo.push_back(std::move(geo));
+  c->pend_bv.emplace_back();
+  c->pend_yk.emplace_back();
+  c->pend.push_back(0);
+  if (block_id) *block_id = (int)c->blocks.size() - 1;
+  return 0;
+}
+
+int cc_register_boundary(const int raw[7], int ngg, cc_boundary *out) {
+  if (!raw || !out) return fail(CC_ERR_ARG, "null argument");
+  HostBoundary b;
+  register_boundary(raw, ngg, b);
+  static_assert(sizeof(HostBoundary) == sizeof(cc_boundary), "layout");
+  std::memcpy(out, &b, sizeof b);
+  return 0;
+}
+
+int cc_register_inner_face(const int raw[13], int ngg, cc_inner_face *out) {
+  if (!raw || !out) return fail(CC_ERR_ARG, "null argument");
+  HostInnerFace f;
+  register_inner_face(raw, ngg, f);
+  static_assert(sizeof(HostInnerFace) == sizeof(cc_inner_face), "layout");
+  std::memcpy(out, &f, sizeof f);
+  return 0;
+}
+
+int cc_add_boundary(cc_ctx *c, int block, const cc_boundary *b) {
+  if (int r = check_ctx(c)) return r;
+  if (c->initialized) return fail(CC_ERR_STATE, "faces must be added before cc_init");
+  if (!b || block < 0 || block >= (int)c->blocks.size()) return fail(CC_ERR_ARG, "bad block or boundary");
+  if (b->face < 0 || b->face > 2) return fail(CC_ERR_ARG, "boundary face must be 0, 1 or 2");
+  HostBoundary h;
+  std::memcpy(&h, b, sizeof h);
+  c->blocks[block].bnd.push_back(h);
+  return 0;
+}
+
+int cc_add_inner_face(cc_ctx *c, int block, const cc_inner_face *f) {
+  if (int r = check_ctx(c)) return r;
+  if (c->initialized) return fail(CC_ERR_STATE, "faces must be added before cc_init");
+  if (!f || block < 0 || block >= (int)c->blocks.size()) return fail(CC_ERR_ARG, "bad block or inner face");
+  if (f->face < 0 || f->face > 2) return fail(CC_ERR_ARG, "inner face normal must be 0, 1 or 2");
+  HostInnerFace h;
+  std::memcpy(&h, f, sizeof h);
+  c->blocks[block].inf.push_back(h);
+  return 0;
+}
+
+int cc_add_bc(cc_ctx *c, const cc_bc *bc) {
+  if (int r = check_ctx(c)) return r;
+  if (c->initialized) return fail(CC_ERR_STATE, "conditions must be added before cc_init");
+  if (!bc || (bc->kind != 2 && bc->kind != 5 && bc->kind != 6))
+    return fail(CC_ERR_ARG, "bc kind must be 2 (wall), 5 (inflow) or 6 (outflow)");
+  HostBc h{};
+  h.label = bc->label, h.kind = bc->kind, h.thermal_type = bc->thermal_type, h.t_wall = bc->t_wall;
+  h.rho = bc->density, h.u = bc->u, h.v = bc->v, h.w = bc->w, h.p = bc->pressure, h.T = bc->temperature;
+  for (int l = 0; l < kMaxSpec; ++l) h.yk[l] = bc->yk[l];
+  c->bcs.push_back(h);
+  // BoundCond.cu:218-230: wall faces exclude the tangential ghost layers
+  if (bc->kind == 2)
+    for (auto &b : c->blocks)
+      for (auto &f : b.bnd)
+        if (f.type_label == bc->label)
+          for (int q = 0; q < 3; ++q)
+            if (q != f.face) f.range_start[q] += c->ngg, f.range_end[q] -= c->ngg;
+  return 0;
+}
+
+int cc_set_state(cc_ctx *c, int block, const double *bv, const double *yk) {
+  if (int r = check_ctx(c)) return r;
+  if (block < 0 || block >= (int)c->blocks.size()) return fail(CC_ERR_ARG, "bad block");
+  if (!bv || (c->chem.ns > 0 && !yk)) return fail(CC_ERR_ARG, "bv (and yk when n_spec > 0) required");
+  const HostBlock &b = c->blocks[block];
+  const int64_t ng = ng_user(b);
+  if (!c->initialized) {
+    c->pend_bv[block].assign(bv, bv + 6 * ng);
+    if (c->chem.ns > 0) c->pend_yk[block].assign(yk, yk + c->chem.ns * ng);
+    c->pend[block] = 1;
+    return 0;
+  }
+  if (int r = copy_fields_h2d(c, b, bv, c->stage64, 6)) return r;
+  if (c->chem.ns > 0)
+    if (int r = copy_fields_h2d(c, b, yk, c->stage64 + 6 * c->N, c->chem.ns)) return r;
+  c->state_dirty = true;
+  return 0;
+}
+
+int cc_init(cc_ctx *c, int precision) {
+  if (int r = check_ctx(c)) return r;
+  if (precision != CC_FP64 && precision != CC_MIXED) return fail(CC_ERR_ARG, "precision must be 0 or 1");
+  if (c->blocks.empty()) return fail(CC_ERR_STATE, "no blocks");
+  if (!c->initialized) {
+    for (size_t b = 0; b < c->blocks.size(); ++b)
+      if (!c->pend[b]) return fail(CC_ERR_STATE, "block " + std::to_string(b) + " has no state (cc_set_state)");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      return fail(CC_ERR_NODEVICE, "no CUDA device");
+    }
+    if (!c->stream) {
+      CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      c->own_stream = true;
+    }
+    c->precision = precision;
+    if (int r = setup_device(c)) return r;
+    for (size_t b = 0; b < c->blocks.size(); ++b) {
+      if (int r = copy_fields_h2d(c, c->blocks[b], c->pend_bv[b].data(), c->stage64, 6)) return r;
+      if (c->chem.ns > 0)
+        if (int r = copy_fields_h2d(c, c->blocks[b], c->pend_yk[b].data(), c->stage64 + 6 * c->N, c->chem.ns))
+          return r;
+    }
+    c->initialized = true;
+    int r = dispatch(c, [&](auto tt, auto nn) { return prepare_inflow<typename decltype(tt)::type, decltype(nn)::value>(c); });
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    for (auto &v : c->pend_bv) std::vector<double>().swap(v);
+    for (auto &v : c->pend_yk) std::vector<double>().swap(v);
+  } else if (precision != c->precision) {
+    return fail(CC_ERR_STATE, "a context keeps the precision of its first cc_init");
+  }
+  destroy_graphs(c);
+  int r = dispatch(c, [&](auto tt, auto nn) { return derive_state<typename decltype(tt)::type, decltype(nn)::value>(c); });
+  if (r) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int cc_step(cc_ctx *c, int n_steps, int scheme, int want_residual) {
+  if (int r = check_ctx(c)) return r;
+  if (!c->initialized) return fail(CC_ERR_STATE, "cc_step before cc_init");
+  if (scheme != CC_RK3 && scheme != CC_STEADY_EULER) return fail(CC_ERR_ARG, "unknown time scheme");
+  if (n_steps < 0) return fail(CC_ERR_ARG, "n_steps must be >= 0");
+  if (c->state_dirty) {
+    destroy_graphs(c);
+    int r = dispatch(c, [&](auto tt, auto nn) { return derive_state<typename decltype(tt)::type, decltype(nn)::value>(c); });
+    if (r) return r;
+  }
+  return dispatch(c, [&](auto tt, auto nn) -> int {
+    using T = typename decltype(tt)::type;
+    constexpr int NS = decltype(nn)::value;
+    for (int s = 0; s < n_steps; ++s) {
+      if (want_residual && s == n_steps - 1)
+        CK(launch_store_last<T>(c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur], c->N, c->n_int,
+                                c->d_last, c->stream));
+      if (int r = step_once<T, NS>(c, scheme)) return r;
+    }
+    if (want_residual && n_steps > 0)
+      CK(launch_residual<T>(c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur], c->N, c->n_int,
+                            c->d_last, c->d_partials, c->n_partials, c->d_res, c->stream));
+    return 0;
+  });
+}
+
+int cc_residual(cc_ctx *c, double out[4]) {
+  if (int r = check_ctx(c)) return r;
+  if (!c->initialized) return fail(CC_ERR_STATE, "cc_residual before cc_init");
+  if (!out) return fail(CC_ERR_ARG, "out is null");
+  CK(cudaMemcpyAsync(out, c->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int cc_get_state(cc_ctx *c, int block, double *bv, double *yk, double *cv) {
+  if (int r = check_ctx(c)) return r;
+  if (!c->initialized) return fail(CC_ERR_STATE, "cc_get_state before cc_init");
+  if (block < 0 || block >= (int)c->blocks.size()) return fail(CC_ERR_ARG, "bad block");
+  if (c->state_dirty) {
+    destroy_graphs(c);
+    int r = dispatch(c, [&](auto tt, auto nn) { return derive_state<typename decltype(tt)::type, decltype(nn)::value>(c); });
+    if (r) return r;
+  }
+  const HostBlock &b = c->blocks[block];
+  const int64_t ng = ng_user(b);
+  for (int f = 0; f < 6 && bv; ++f) {
+    if (int r = field_to64(c, c->P[c->cur], f)) return r;
+    if (int r = copy_field_d2h(c, b, c->tmp64, bv + f * ng)) return r;
+  }
+  for (int l = 0; l < c->chem.ns && yk; ++l) {
+    if (int r = field_to64(c, c->P[c->cur], 6 + l)) return r;
+    if (int r = copy_field_d2h(c, b, c->tmp64, yk + l * ng)) return r;
+  }
+  for (int f = 0; f < nv_of(c) && cv; ++f)
+    if (int r = copy_field_d2h(c, b, c->Q[c->qcur] + (int64_t)f * c->N, cv + f * ng)) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int cc_get_props(cc_ctx *c, int block, double *mul, double *conductivity, double *rho_d) {
+  if (int r = check_ctx(c)) return r;
+  if (!c->initialized) return fail(CC_ERR_STATE, "cc_get_props before cc_init");
+  if (block < 0 || block >= (int)c->blocks.size()) return fail(CC_ERR_ARG, "bad block");
+  const HostBlock &b = c->blocks[block];
+  const int64_t ng = ng_user(b);
+  double *outs[2] = {mul, conductivity};
+  for (int f = 0; f < 2; ++f) {
+    if (!outs[f]) continue;
+    if (int r = field_to64(c, c->Pr[c->cur], f)) return r;
+    if (int r = copy_field_d2h(c, b, c->tmp64, outs[f])) return r;
+  }
+  for (int l = 0; l < c->chem.ns && rho_d; ++l) {
+    if (int r = field_to64(c, c->Pr[c->cur], 2 + l)) return r;
+    if (int r = copy_field_d2h(c, b, c->tmp64, rho_d + l * ng)) return r;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int cc_last_dt(cc_ctx *c, double *dt) {
+  if (int r = check_ctx(c)) return r;
+  if (!c->initialized || !dt) return fail(CC_ERR_STATE, "cc_last_dt before cc_init");
+  double h[2];
+  CK(cudaMemcpyAsync(h, c->d_dt, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *dt = h[1];
+  return 0;
+}
+
+int cc_status(cc_ctx *c, unsigned *flags) {
+  if (int r = check_ctx(c)) return r;
+  if (!flags) return fail(CC_ERR_ARG, "flags is null");
+  if (!c->initialized) {
+    *flags = 0;
+    return 0;
+  }
+  CK(cudaMemcpyAsync(flags, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int cc_set_stream(cc_ctx *c, void *stream) {
+  if (int r = check_ctx(c)) return r;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  destroy_graphs(c);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  c->stream = (cudaStream_t)stream;
+  c->own_stream = false;
+  return 0;
+}
+
+void *cc_get_stream(cc_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int cc_use_graph(cc_ctx *c, int enable) {
+  if (int r = check_ctx(c)) return r;
+  c->use_graph = enable != 0;
+  return 0;
+}
+
+int cc_info(cc_ctx *c, int64_t *n_points, int64_t *device_bytes, int *n_tiles, int *n_halo_levels) {
+  if (int r = check_ctx(c)) return r;
+  int64_t n = 0;
+  for (const auto &b : c->blocks) n += (int64_t)b.mx * b.my * b.mz;
+  if (n_points) *n_points = n;
+  if (device_bytes) *device_bytes = c->device_bytes;
+  if (n_tiles) *n_tiles = (int)c->htiles.size();
+  if (n_halo_levels) *n_halo_levels = (int)c->plan.level_begin.size() - 1;
+  return 0;
+}
+
+int cc_sync(cc_ctx *c) {
+  if (int r = check_ctx(c)) return r;
+  if (c->stream) CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+}  // extern "C"

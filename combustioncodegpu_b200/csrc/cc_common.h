@@ -1,0 +1,145 @@
+// Shared host/device definitions of the sm_100a residual path.
+#pragma once
+#include <cstdint>
+
+namespace ccb {
+
+constexpr double kRu = 8314.462618;    // Constants.h:19
+constexpr double kGammaAir = 1.4;      // Constants.h:23
+constexpr double kMwAir = 28.9647;     // Constants.h:28
+constexpr int kMaxSpec = 16;           // species supported by one context
+constexpr int kTX = 32;                // stage tile: points along i (one warp)
+constexpr int kTY = 8;                 // stage tile: points along j (warps)
+
+// Per-precision species tables, passed to every kernel by value (constant
+// bank).  Horner-form NASA-7 coefficients: for T >= t_mid the `hi` set.
+template <typename T>
+struct SpecTables {
+  T mw[kMaxSpec];
+  T inv_mw[kMaxSpec];
+  T r_over_mw[kMaxSpec];      // R_u / W_k
+  T cv_shift[kMaxSpec];       // R_u / W_k (cp - cv per species)
+  T t_low[kMaxSpec], t_mid[kMaxSpec];
+  T cp_lo[kMaxSpec][5], cp_hi[kMaxSpec][5];   // cp/R   = a0 + a1 T + ... + a4 T^4
+  T h_lo[kMaxSpec][6], h_hi[kMaxSpec][6];     // h/R    = a5 + T(a0 + T(a1/2 + T(a2/3 + T(a3/4 + T a4/5))))
+  T lj_inv[kMaxSpec];
+  T vis_coeff[kMaxSpec];
+  T lam_shift[kMaxSpec];      // 1.25 R_u / W_k
+  T wj[kMaxSpec * kMaxSpec];  // (W_j/W_i)^(1/4)
+  T sw[kMaxSpec * kMaxSpec];  // 1/sqrt(8 (1 + W_i/W_j))
+};
+
+struct ChemParams {
+  int ns;              // 0 = calorically perfect air
+  int nv;              // 5 + ns
+  int reconstruction;  // 2 = MUSCL, else first order
+  int viscous;         // 1 = second-order central viscous fluxes
+  double Pr, cfl, Sc;
+  SpecTables<double> d;
+  SpecTables<float> f;
+};
+
+// One block of the multiblock grid in the concatenated field arena.
+struct BlockInfo {
+  int mx, my, mz, g;
+  int nx, ny, nz, pad;  // ghosted extents (nx padded)
+  int64_t base;         // arena index of interior point (0,0,0)
+  int64_t off;          // arena index of ghost corner (-g,-g,-g)
+  int64_t ng;           // points in the ghosted box (nx*ny*nz)
+  int64_t interior_off; // offset of this block in interior-only arrays
+};
+
+// Work unit of the stage kernel: a kTX x kTY column of points swept over k.
+struct Tile {
+  int blk, i0, j0, k0, k1, pad0, pad1, pad2;
+};
+
+// Halo program entry: one destination point filled from resolved sources.
+enum HaloOp : int {
+  kHaloCopy = 0,       // dst <- src
+  kHaloAvg = 1,        // dst <- (src + src2) / 2       (coincident interface layer)
+  kHaloInflow = 2,     // dst <- inflow state bc
+  kHaloWallFace = 3,   // wall point: p, Y from src (i-dir), T_wall or T(src)
+  kHaloWallGhost = 4,  // mirror of src; T reference from src2 (i-dir)
+  kHaloKeep = 5,       // dst <- previous buffer value of dst
+};
+
+struct BcDevice {
+  int kind;           // 2 wall, 5 inflow, 6 outflow
+  int thermal_type;   // wall: 0 isothermal, 1 adiabatic
+  double t_wall;
+  double rho, u, v, w, p, T;
+  double yk[kMaxSpec];
+  double rhoE;                     // inflow total energy (compute_total_energy)
+  double mu, lam, rho_d[kMaxSpec]; // inflow transport properties
+};
+
+// Status bits reported by cc_status.
+enum StatusBits : unsigned {
+  kStatusNewtonCap = 1u,     // temperature Newton hit its iteration cap
+  kStatusNonFinite = 2u,     // NaN/Inf or non-positive rho/p/T after an update
+  kStatusBadDt = 4u,         // global time step not positive and finite
+};
+
+// Arguments of one stage launch (see stage.cuh).
+template <typename T>
+struct StageArgs {
+  const BlockInfo *blocks;
+  const Tile *tiles;
+  int64_t N;                 // arena stride in points
+  const T *P;                // primitives of the current state
+  T *Pn;                     // primitives of the new state
+  const T *Pr;               // transport properties, current
+  T *Prn;                    // transport properties, new
+  const T *G;                // geometry
+  const double *Qin;         // conserved, current stage
+  const double *Qn;          // conserved, step start (read when a != 0)
+  double *Qout;              // conserved, new (may alias Qin)
+  double a, b;               // Q = a Qn + b (Qin + dt dq / J)
+  const double *dt;          // global time step
+  unsigned long long *dt_next;  // next global time step (atomicMin), or null
+  unsigned *status;
+  int local_dt;              // 1: per-point time step of the current state
+  int renorm_y;              // 1: renormalise Y_k to sum 1
+};
+
+// A source reference of the halo program: kind 0 = point of the new state,
+// 1 = point of the previous state, 2 = scratch slot of an evaluated node.
+struct HaloRef {
+  int64_t idx;
+  int kind;
+  int pad;
+};
+
+struct HaloNode {
+  int64_t slot;
+  HaloRef a, b;
+  int op;
+  int bc;
+};
+
+struct HaloCopy {
+  int64_t dst;
+  HaloRef src;
+};
+
+template <typename T>
+struct HaloArgs {
+  int64_t N;       // arena stride
+  int64_t NS_cap;  // scratch stride (slots)
+  T *P;            // new state (written by phase B)
+  const T *Pprev;
+  T *Pr;
+  const T *Prprev;
+  double *Q;
+  const double *Qprev;
+  T *sP;           // scratch [6+ns][NS_cap]
+  T *sPr;          // scratch [2+ns][NS_cap]
+  double *sQ;      // scratch [nv][NS_cap]
+  const BcDevice *bcs;
+  const HaloNode *nodes;
+  const HaloCopy *copies;
+  int64_t begin, end;
+};
+
+}  // namespace ccb

@@ -1,0 +1,71 @@
+// Definitions of the templated launchers (included by inst_*.cu only).
+#pragma once
+#include "launch.h"
+#include "stage.cuh"
+
+namespace ccb {
+
+template <typename T, int NS>
+size_t Launch<T, NS>::stage_smem() {
+  constexpr int NV = 5 + SpecCount<NS>::kArr;
+  return sizeof(T) * NV * (kTY * (kTX + 1) + (kTY + 1) * kTX + 2 * kTY * kTX);
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::configure() {
+  return cudaFuncSetAttribute(k_stage<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem());
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::stage(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s) {
+  if (n_tiles <= 0) return cudaSuccess;
+  k_stage<T, NS><<<n_tiles, dim3(kTX, kTY), stage_smem(), s>>>(a, C);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s) {
+  const int64_t n = a.end - a.begin;
+  if (n <= 0) return cudaSuccess;
+  const int tpb = 128;
+  k_halo_nodes<T, NS><<<(unsigned)((n + tpb - 1) / tpb), tpb, 0, s>>>(a, C);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::halo_copies(const HaloArgs<T> &a, int np, int npr, int nq, cudaStream_t s) {
+  const int64_t n = a.end - a.begin;
+  if (n <= 0) return cudaSuccess;
+  const int tpb = 256;
+  k_halo_copies<T><<<(unsigned)((n + tpb - 1) / tpb), tpb, 0, s>>>(a, np, npr, nq);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, cudaStream_t s) {
+  const int tpb = 256;
+  k_cv_from_bv<NS><<<(unsigned)((N + tpb - 1) / tpb), tpb, 0, s>>>(C, P0, Q, N);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::props_all(const ChemParams &C, const T *P, T *Pr, int64_t N, cudaStream_t s) {
+  const int tpb = 128;
+  k_props_all<T, NS><<<(unsigned)((N + tpb - 1) / tpb), tpb, 0, s>>>(C, P, Pr, N);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::dt_reduce(const ChemParams &C, const BlockInfo *blocks, int nblocks, const T *P,
+                                     const T *Pr, const T *G, int64_t N, int64_t n_interior,
+                                     unsigned long long *dt_out, cudaStream_t s) {
+  const int tpb = 256;
+  int64_t nb = (n_interior + tpb - 1) / tpb;
+  if (nb > 148 * 16) nb = 148 * 16;
+  k_dt_reduce<T, NS><<<(unsigned)nb, tpb, 0, s>>>(C, blocks, nblocks, P, Pr, G, N, n_interior, dt_out);
+  return cudaGetLastError();
+}
+
+#define CCB_INSTANTIATE(T, NS) template struct Launch<T, NS>;
+
+}  // namespace ccb

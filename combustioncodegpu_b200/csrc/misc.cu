@@ -1,0 +1,143 @@
+// Small kernels: precision conversion, time-step bookkeeping and the
+// convergence residual of Driver::compute_residual (Driver.cu:219-277,
+// TimeAdvanceFunc.cu:13-24 and 292-303), reduced deterministically in FP64.
+#include "launch.h"
+
+namespace ccb {
+
+__global__ void k_convert_d2f(const double *src, float *dst, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (float)src[i];
+}
+
+__global__ void k_convert_f2d(const float *src, double *dst, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (double)src[i];
+}
+
+cudaError_t launch_convert_d2f(const double *src, float *dst, int64_t n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_convert_d2f<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, dst, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_convert_f2d(const float *src, double *dst, int64_t n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_convert_f2d<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, dst, n);
+  return cudaGetLastError();
+}
+
+// dt <- dt_next (when a candidate was reduced), dt_next <- +inf; the step's
+// dt is appended to the history slot.
+__global__ void k_dt_finalize(double *dt, unsigned long long *dt_next, unsigned *status, double *dt_hist) {
+  if (dt_hist) *dt_hist = *dt;  // the step just finished used *dt
+  const unsigned long long bits = *dt_next;
+  const double v = __longlong_as_double((long long)bits);
+  if (bits != 0x7ff0000000000000ull) {
+    if (v > 0.0 && isfinite(v))
+      *dt = v;
+    else
+      atomicOr(status, kStatusBadDt);
+  } else {
+    atomicOr(status, kStatusBadDt);
+  }
+  *dt_next = 0x7ff0000000000000ull;
+}
+
+cudaError_t launch_dt_finalize(double *dt, unsigned long long *dt_next, unsigned *status, double *dt_hist,
+                               cudaStream_t s) {
+  k_dt_finalize<<<1, 1, 0, s>>>(dt, dt_next, status, dt_hist);
+  return cudaGetLastError();
+}
+
+__device__ __forceinline__ int64_t interior_point(const BlockInfo *blocks, int nblocks, int64_t g) {
+  int lo = 0, hi = nblocks - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (blocks[mid].interior_off <= g)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const BlockInfo &B = blocks[lo];
+  const int64_t r = g - B.interior_off;
+  const int64_t i = r % B.mx;
+  const int64_t j = (r / B.mx) % B.my;
+  const int64_t k = r / ((int64_t)B.mx * B.my);
+  return B.base + i + (int64_t)B.nx * j + (int64_t)B.nx * B.ny * k;
+}
+
+// store_last_step: (rho, |V|, p, T) of every interior point.
+template <typename T>
+__global__ void k_store_last(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_int,
+                             double *last) {
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= n_int) return;
+  const int64_t p = interior_point(blocks, nblocks, g);
+  const double u = P[N + p], v = P[2 * N + p], w = P[3 * N + p];
+  last[g] = P[p];
+  last[n_int + g] = sqrt(u * u + v * v + w * w);
+  last[2 * n_int + g] = P[4 * N + p];
+  last[3 * n_int + g] = P[5 * N + p];
+}
+
+// compute_square_of_dbv + per-CTA sums (fixed order), then one CTA sums the
+// partials in fixed order: the result does not depend on scheduling.
+template <typename T>
+__global__ void k_residual_partial(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_int,
+                                   const double *last, double *partials) {
+  double acc[4] = {0, 0, 0, 0};
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_int; g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = interior_point(blocks, nblocks, g);
+    const double u = P[N + p], v = P[2 * N + p], w = P[3 * N + p];
+    const double d0 = (double)P[p] - last[g];
+    const double d1 = sqrt(u * u + v * v + w * w) - last[n_int + g];
+    const double d2 = (double)P[4 * N + p] - last[2 * n_int + g];
+    const double d3 = (double)P[5 * N + p] - last[3 * n_int + g];
+    acc[0] += d0 * d0, acc[1] += d1 * d1, acc[2] += d2 * d2, acc[3] += d3 * d3;
+  }
+  __shared__ double sh[4][256];
+  for (int l = 0; l < 4; ++l) sh[l][threadIdx.x] = acc[l];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+      for (int l = 0; l < 4; ++l) sh[l][threadIdx.x] += sh[l][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int l = 0; l < 4; ++l) partials[4 * blockIdx.x + l] = sh[l][0];
+}
+
+__global__ void k_residual_final(const double *partials, int n_partials, int64_t n_int, double *res) {
+  if (threadIdx.x != 0) return;
+  double r[4] = {0, 0, 0, 0};
+  for (int b = 0; b < n_partials; ++b)
+    for (int l = 0; l < 4; ++l) r[l] += partials[4 * b + l];
+  for (int l = 0; l < 4; ++l) res[l] = sqrt(r[l] / (double)n_int);
+}
+
+template <typename T>
+cudaError_t launch_store_last(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_interior,
+                              double *bv_last, cudaStream_t s) {
+  k_store_last<T><<<(unsigned)((n_interior + 255) / 256), 256, 0, s>>>(blocks, nblocks, P, N, n_interior, bv_last);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_residual(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_interior,
+                            const double *bv_last, double *partials, int n_partials, double *res, cudaStream_t s) {
+  k_residual_partial<T><<<n_partials, 256, 0, s>>>(blocks, nblocks, P, N, n_interior, bv_last, partials);
+  k_residual_final<<<1, 32, 0, s>>>(partials, n_partials, n_interior, res);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_store_last<double>(const BlockInfo *, int, const double *, int64_t, int64_t, double *,
+                                               cudaStream_t);
+template cudaError_t launch_store_last<float>(const BlockInfo *, int, const float *, int64_t, int64_t, double *,
+                                              cudaStream_t);
+template cudaError_t launch_residual<double>(const BlockInfo *, int, const double *, int64_t, int64_t,
+                                             const double *, double *, int, double *, cudaStream_t);
+template cudaError_t launch_residual<float>(const BlockInfo *, int, const float *, int64_t, int64_t, const double *,
+                                            double *, int, double *, cudaStream_t);
+
+}  // namespace ccb

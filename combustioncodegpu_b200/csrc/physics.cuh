@@ -1,0 +1,337 @@
+// Device physics of the residual path, templated on the bulk precision T
+// (double for the plain path, float for the mixed path) and on the species
+// count NS (compile-time; -1 = runtime count up to kMaxSpec, 0 = perfect air).
+//
+// Reference counterparts (file:line in CombustionCodeGPU):
+//   NASA-7 h/cp with linear h below T_low ......... Thermo.cu:7-63
+//   total energy .................................. Thermo.cu:66-86
+//   temperature Newton (FP64 in every precision) .. Thermo.cu:89-125
+//   Sutherland ..................................... Transport.cu:7-10
+//   Wilke / constant-Schmidt transport ............. Transport.cu:43-96 (X[l])
+//   MUSCL + minmod + face thermo ................... Reconstruction.cu:26-89, Limiter.cuh:13-16
+//   AUSM+ ........................................... InviscidScheme.cu:24-108
+// The polynomials are evaluated in Horner form and sqrt(mu_m/mu_n) as
+// sqrt(mu_m)/sqrt(mu_n); both differ from the reference only by rounding.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "cc_common.h"
+
+namespace ccb {
+
+template <typename T>
+__device__ __forceinline__ const SpecTables<T> &tab(const ChemParams &C);
+template <>
+__device__ __forceinline__ const SpecTables<double> &tab<double>(const ChemParams &C) {
+  return C.d;
+}
+template <>
+__device__ __forceinline__ const SpecTables<float> &tab<float>(const ChemParams &C) {
+  return C.f;
+}
+
+template <int NS>
+struct SpecCount {
+  static constexpr int kArr = NS > 0 ? NS : (NS == 0 ? 1 : kMaxSpec);
+  __device__ __forceinline__ static int n(const ChemParams &C) { return NS >= 0 ? NS : C.ns; }
+};
+
+template <typename T>
+__device__ __forceinline__ T ld(const T *p) {
+  return __ldg(p);
+}
+
+// NASA-7 enthalpy and cp of species k at temperature t (per unit mass).
+template <typename T>
+__device__ __forceinline__ void nasa_h_cp(const SpecTables<T> &S, int k, T t, T &h, T &cp) {
+  const T tl = S.t_low[k];
+  const bool below = t < tl;
+  const T te = below ? tl : t;
+  const bool lo = below || t < S.t_mid[k];
+  const T *a = lo ? S.cp_lo[k] : S.cp_hi[k];
+  const T *b = lo ? S.h_lo[k] : S.h_hi[k];
+  T c = a[0] + te * (a[1] + te * (a[2] + te * (a[3] + te * a[4])));
+  T hh = b[5] + te * (b[0] + te * (b[1] + te * (b[2] + te * (b[3] + te * b[4]))));
+  if (below) hh += c * (t - te);
+  h = hh * S.r_over_mw[k];
+  cp = c * S.r_over_mw[k];
+}
+
+template <typename T>
+__device__ __forceinline__ T nasa_h(const SpecTables<T> &S, int k, T t) {
+  T h, cp;
+  nasa_h_cp(S, k, t, h, cp);
+  return h;
+}
+
+template <typename T>
+__device__ __forceinline__ T nasa_cp(const SpecTables<T> &S, int k, T t) {
+  const T tl = S.t_low[k];
+  const T te = t < tl ? tl : t;
+  const T *a = (t < S.t_mid[k]) ? S.cp_lo[k] : S.cp_hi[k];
+  return (a[0] + te * (a[1] + te * (a[2] + te * (a[3] + te * a[4])))) * S.r_over_mw[k];
+}
+
+template <typename T>
+__device__ __forceinline__ T sutherland(T t) {
+  // 1.716e-5 (T/273)^1.5 (273+111)/(T+111)
+  const T r = t / T(273);
+  return T(1.716e-5) * (r * sqrt(r)) * T(384) / (t + T(111));
+}
+
+template <typename T>
+__device__ __forceinline__ T pow_m0145(T x);
+template <>
+__device__ __forceinline__ double pow_m0145<double>(double x) {
+  return pow(x, -0.145);
+}
+template <>
+__device__ __forceinline__ float pow_m0145<float>(float x) {
+  return powf(x, -0.145f);
+}
+
+// Wilke mixture viscosity, modified-Wilke conductivity and constant-Schmidt
+// rho*D_k.  cp[k] is the species cp per unit mass at temp.
+template <typename T, int NS>
+__device__ __forceinline__ void transport(const ChemParams &C, T temp, const T *Y, T mw_total, const T *cp,
+                                          T &mu_out, T &lam_out, T *rhod) {
+  const SpecTables<T> &S = tab<T>(C);
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  T X[A], vis[A], svis[A], isvis[A];
+  const T sqt = sqrt(temp);
+#pragma unroll
+  for (int l = 0; l < A; ++l) {
+    if (l < ns) {
+      X[l] = Y[l] * mw_total * S.inv_mw[l];
+      const T t_dl = temp * S.lj_inv[l];
+      const T tp = t_dl + T(0.5);
+      const T omega = T(1.147) * pow_m0145<T>(t_dl) + T(1) / (tp * tp);
+      vis[l] = S.vis_coeff[l] * sqt / omega;
+      svis[l] = sqrt(vis[l]);
+      isvis[l] = T(1) / svis[l];
+    }
+  }
+  T viscosity = 0, conductivity = 0;
+#pragma unroll
+  for (int m = 0; m < A; ++m) {
+    if (m < ns) {
+      T vt = 0;
+#pragma unroll
+      for (int n = 0; n < A; ++n) {
+        if (n < ns) {
+          T phi;
+          if (m == n) {
+            phi = T(1);
+          } else {
+            const T num = T(1) + svis[m] * isvis[n] * S.wj[m * kMaxSpec + n];
+            phi = num * num * S.sw[m * kMaxSpec + n];
+          }
+          vt += phi * X[n];
+        }
+      }
+      const T lam_m = vis[m] * (cp[m] + S.lam_shift[m]);
+      viscosity += vis[m] * X[m] / vt;
+      conductivity += lam_m * X[m] / (T(1.065) * vt - T(0.065) * X[m]);
+    }
+  }
+  mu_out = viscosity;
+  lam_out = conductivity;
+  const T inv_sc = T(1) / T(C.Sc);
+#pragma unroll
+  for (int l = 0; l < A; ++l) {
+    if (l < ns) {
+      const T d = X[l] - T(1);
+      rhod[l] = (fabs(d) < T(1e-3)) ? viscosity * inv_sc : (T(1) - Y[l]) * viscosity / ((T(1) - X[l]) * T(C.Sc));
+    }
+  }
+}
+
+// Point properties used by the stage update and the time step:
+// mu, lambda, rho*D_k (stored) and gamma, acoustic speed (for dt).
+template <typename T, int NS>
+__device__ __forceinline__ void point_props(const ChemParams &C, T temp, const T *Y, T &mu, T &lam, T *rhod, T &gamma,
+                                            T &c) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  if (NS == 0 || (NS < 0 && ns == 0)) {
+    const T c_temp = T(kGammaAir * kRu / kMwAir);
+    c = sqrt(c_temp * temp);
+    mu = sutherland<T>(temp);
+    lam = mu * c_temp / T(kGammaAir - 1) / T(C.Pr);
+    gamma = T(kGammaAir);
+    return;
+  }
+  const SpecTables<T> &S = tab<T>(C);
+  T cp[A];
+  T mwi = 0, cp_tot = 0, cvv = 0;
+#pragma unroll
+  for (int l = 0; l < A; ++l) {
+    if (l < ns) {
+      cp[l] = nasa_cp<T>(S, l, temp);
+      mwi += Y[l] * S.inv_mw[l];
+      cp_tot += Y[l] * cp[l];
+      cvv += Y[l] * (cp[l] - S.cv_shift[l]);
+    }
+  }
+  const T mw = T(1) / mwi;
+  gamma = cp_tot / cvv;
+  c = sqrt(gamma * T(kRu) * temp / mw);
+  transport<T, NS>(C, temp, Y, mw, cp, mu, lam, rhod);
+}
+
+// Temperature from internal energy by Newton iteration, always in FP64
+// (tolerance 1e-3 on |1 - T1/T|, at most 1000 iterations, warm start t).
+template <int NS>
+__device__ __forceinline__ double newton_temperature(const ChemParams &C, double e, const double *Y, double gas_const,
+                                                     double t, bool &capped) {
+  const SpecTables<double> &S = C.d;
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  double err = 1;
+  int iter = 0;
+  while (err > 1e-3 && iter++ < 1000) {
+    double cp_tot = 0, h = 0;
+#pragma unroll
+    for (int l = 0; l < A; ++l) {
+      if (l < ns) {
+        double hl, cpl;
+        nasa_h_cp<double>(S, l, t, hl, cpl);
+        cp_tot += cpl * Y[l];
+        h += hl * Y[l];
+      }
+    }
+    const double e_t = h - gas_const * t;
+    const double cvv = cp_tot - gas_const;
+    const double t1 = t - (e_t - e) / cvv;
+    err = fabs(1 - t1 / t);
+    t = t1;
+  }
+  capped = err > 1e-3;
+  return t;
+}
+
+template <typename T>
+__device__ __forceinline__ T sgn1(T a) {
+  return T((T(0) < a) - (a < T(0)));
+}
+
+template <typename T>
+__device__ __forceinline__ T minmod(T a, T b) {
+  return T(0.5) * (sgn1(a) + sgn1(b)) * fmin(fabs(a), fabs(b));
+}
+
+// MUSCL (kappa = 1/3, minmod) or first-order states at the face between
+// points 1 and 2 of v[0..3], face thermodynamics, then AUSM+.
+// v[t][0..4] = rho,u,v,w,p ; v[t][5+l] = Y_l.  F receives n_var values.
+template <typename T, int NS>
+__device__ __forceinline__ void face_inviscid(const ChemParams &C, const T (&v)[4][5 + SpecCount<NS>::kArr],
+                                              const T k[3], T *F) {
+  constexpr int A = SpecCount<NS>::kArr;
+  constexpr int NV = 5 + A;
+  const int ns = SpecCount<NS>::n(C);
+  const int nv = 5 + ns;
+  T L[NV], R[NV];
+  if (C.reconstruction == 2) {
+    const T kappa = T(1.0 / 3.0);
+    const T w1 = T(0.25) * (T(1) - kappa), w2 = T(0.25) * (T(1) + kappa);
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
+      if (l < nv) {
+        const T d_i = v[1][l] - v[0][l];
+        const T d_i1 = v[2][l] - v[1][l];
+        const T d_i2 = v[3][l] - v[2][l];
+        const T m1 = minmod(d_i, d_i1);
+        const T m2 = minmod(d_i1, d_i2);
+        // minmod is symmetric: (1-k) mm(a,b) + (1+k) mm(b,a) = 2 mm(a,b)
+        L[l] = v[1][l] + (w1 * m1 + w2 * m1);
+        R[l] = v[2][l] - (w1 * m2 + w2 * m2);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int l = 0; l < NV; ++l)
+      if (l < nv) L[l] = v[1][l], R[l] = v[2][l];
+  }
+  T el = T(0.5) * (L[1] * L[1] + L[2] * L[2] + L[3] * L[3]);
+  T er = T(0.5) * (R[1] * R[1] + R[2] * R[2] + R[3] * R[3]);
+  T El, Er, gam_l, gam_r;
+  if (NS == 0 || (NS < 0 && ns == 0)) {
+    El = el * L[0] + L[4] / T(kGammaAir - 1);
+    Er = er * R[0] + R[4] / T(kGammaAir - 1);
+    gam_l = gam_r = T(kGammaAir);
+  } else {
+    const SpecTables<T> &S = tab<T>(C);
+    T mwl = 0, mwr = 0;
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) mwl += L[5 + l] * S.inv_mw[l], mwr += R[5 + l] * S.inv_mw[l];
+    const T t_l = L[4] / (L[0] * T(kRu) * mwl);
+    const T t_r = R[4] / (R[0] * T(kRu) * mwr);
+    T cpl = 0, cpr = 0, cvl = 0, cvr = 0;
+#pragma unroll
+    for (int l = 0; l < A; ++l) {
+      if (l < ns) {
+        T hl, cl, hr, cr;
+        nasa_h_cp<T>(S, l, t_l, hl, cl);
+        nasa_h_cp<T>(S, l, t_r, hr, cr);
+        cpl += cl * L[5 + l];
+        cpr += cr * R[5 + l];
+        cvl += L[5 + l] * (cl - S.cv_shift[l]);
+        cvr += R[5 + l] * (cr - S.cv_shift[l]);
+        el += hl * L[5 + l];
+        er += hr * R[5 + l];
+      }
+    }
+    El = L[0] * el - L[4];
+    Er = R[0] * er - R[4];
+    gam_l = cpl / cvl;
+    gam_r = cpr / cvr;
+  }
+  const T alpha = T(3.0 / 16.0);
+  const T k1 = k[0], k2 = k[1], k3 = k[2];
+  const T gk = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
+  const T igk = T(1) / gk;
+  const T ul = (k1 * L[1] + k2 * L[2] + k3 * L[3]) * igk;
+  const T ur = (k1 * R[1] + k2 * R[2] + k3 * R[3]) * igk;
+  const T pl = L[4], pr = R[4], rho_l = L[0], rho_r = R[0];
+  const T c = T(0.5) * (sqrt(gam_l * pl / rho_l) + sqrt(gam_r * pr / rho_r));
+  const T ic = T(1) / c;
+  const T mach_l = ul * ic, mach_r = ur * ic;
+  T mlp, mrn, plp, prn;
+  if (fabs(mach_l) > T(1)) {
+    mlp = T(0.5) * (mach_l + fabs(mach_l));
+    plp = mlp / mach_l;
+  } else {
+    const T a = (mach_l + T(1)) * (mach_l + T(1)) * T(0.25);
+    const T b = (mach_l * mach_l - T(1)) * (mach_l * mach_l - T(1));
+    mlp = a + T(0.125) * b;
+    plp = a * (T(2) - mach_l) + alpha * mach_l * b;
+  }
+  if (fabs(mach_r) > T(1)) {
+    mrn = T(0.5) * (mach_r - fabs(mach_r));
+    prn = mrn / mach_r;
+  } else {
+    const T a = (mach_r - T(1)) * (mach_r - T(1)) * T(0.25);
+    const T b = (mach_r * mach_r - T(1)) * (mach_r * mach_r - T(1));
+    mrn = -a - T(0.125) * b;
+    prn = a * (T(2) + mach_r) - alpha * mach_r * b;
+  }
+  const T p_coeff = plp * pl + prn * pr;
+  const T m_half = mlp + mrn;
+  const T mach_pos = T(0.5) * (m_half + fabs(m_half));
+  const T mach_neg = T(0.5) * (m_half - fabs(m_half));
+  const T mass_flux_half = c * (rho_l * mach_pos + rho_r * mach_neg);
+  const T coeff = mass_flux_half * gk;
+  const bool up = mass_flux_half >= T(0);
+  F[0] = coeff;
+  F[1] = coeff * (up ? L[1] : R[1]) + p_coeff * k1;
+  F[2] = coeff * (up ? L[2] : R[2]) + p_coeff * k2;
+  F[3] = coeff * (up ? L[3] : R[3]) + p_coeff * k3;
+  F[4] = up ? coeff * (El + pl) / rho_l : coeff * (Er + pr) / rho_r;
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) F[5 + l] = coeff * (up ? L[5 + l] : R[5 + l]);
+}
+
+}  // namespace ccb

@@ -1,0 +1,622 @@
+// Stage, halo and setup kernels of the residual path (sm_100a).
+//
+// One RK stage is one launch of k_stage over a list of tiles.  A tile is a
+// kTX x kTY column of points of one block swept along k: per k-plane every
+// thread computes the +x, +y and +z face fluxes of its point (inviscid AUSM+
+// minus second-order viscous), the tile's -x / -y boundary faces are computed
+// by warps 1 and 0, the -z face is carried from the previous plane, all in
+// shared memory; then each thread differences the six faces (the reference's
+// dq, TimeAdvanceFunc.cu:61-243), applies the RK update in FP64, recovers the
+// primitives (FP64 Newton, Thermo.cu:89-125) and evaluates the transport
+// properties of the new state (Field.cu:178-210).  Stage 3 also reduces the
+// next global time step (TemporalScheme.cu:11-43) with warp shuffles and a
+// 64-bit atomicMin on the bit pattern of the positive double.
+//
+// Field arenas are structure-of-arrays over all blocks: field f of point p at
+// [f * N + p], point p = BlockInfo.base + i + nx*j + nx*ny*k.
+//   P   : rho, u, v, w, p, T, Y_0..Y_{ns-1}         (bulk precision T)
+//   Pr  : mu, lambda, rhoD_0..rhoD_{ns-1}           (bulk precision T)
+//   G   : J, xi_x, xi_y, xi_z, eta_x, ..., zeta_z   (bulk precision T)
+//   Q   : rho, rho u, rho v, rho w, rho E, rho Y_k  (FP64 always)
+#pragma once
+#include "physics.cuh"
+
+namespace ccb {
+
+__device__ __forceinline__ void atomic_min_pos_double(unsigned long long *dst, double v) {
+  if (!(v > 0.0) || !(v < 1e300)) return;
+  atomicMin(dst, (unsigned long long)__double_as_longlong(v));
+}
+
+// TemporalScheme.cu:11-43: CFL / (inviscid + viscous spectral radius).
+template <typename T>
+__device__ __forceinline__ double local_time_step(const ChemParams &C, const T *G, int64_t N, int64_t p, double rho,
+                                                  double u, double v, double w, double c, double gamma, double mu,
+                                                  bool three_d) {
+  double m[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) m[r] = (double)G[(1 + r) * N + p];
+  const double gxi = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+  const double get = sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
+  const double gze = sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
+  const double U = u * m[0] + v * m[1] + w * m[2];
+  const double V = u * m[3] + v * m[4] + w * m[5];
+  const double W = u * m[6] + v * m[7] + w * m[8];
+  double sri = fabs(U) + fabs(V) + c * (gxi + get);
+  if (three_d) sri += fabs(W) + c * gze;
+  const double c1 = fmax(gamma, 4.0 / 3.0);
+  const double c2 = mu / rho / C.Pr;
+  double srv = gxi * gxi + get * get;
+  if (three_d) srv += gze * gze;
+  srv *= c1 * c2;
+  return C.cfl / (sri + srv);
+}
+
+// Face flux (inviscid minus viscous) of the face between p and p + e_d.
+template <typename T, int NS>
+__device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restrict__ P, const T *__restrict__ Pr,
+                                          const T *__restrict__ G, int64_t N, int64_t p, int d, const int64_t s[3],
+                                          T *F) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  const int64_t sd = s[d];
+  const int64_t p1 = p + sd;
+  T v[4][5 + A];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int64_t q = p + (t - 1) * sd;
+#pragma unroll
+    for (int f = 0; f < 5; ++f) v[t][f] = P[f * N + q];
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) v[t][5 + l] = P[(6 + l) * N + q];
+  }
+  T k[3];
+  const T J0 = G[p], J1 = G[p1];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) k[c] = T(0.5) * (J0 * G[(1 + 3 * d + c) * N + p] + J1 * G[(1 + 3 * d + c) * N + p1]);
+  face_inviscid<T, NS>(C, v, k, F);
+  if (!C.viscous) return;
+
+  // ViscousScheme.cu:11-342, metrics averaged over both points (m and m1)
+  T met[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) met[r][c] = T(0.5) * (G[(1 + 3 * r + c) * N + p] + G[(1 + 3 * r + c) * N + p1]);
+  auto deriv = [&](const T *__restrict__ f, T out[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (c == d) {
+        out[c] = f[p1] - f[p];
+      } else {
+        const int64_t sc = s[c];
+        out[c] = T(0.25) * (f[p + sc] - f[p - sc] + f[p1 + sc] - f[p1 - sc]);
+      }
+    }
+  };
+  auto grad = [&](const T dd[3], T g[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g[c] = dd[0] * met[0][c] + dd[1] * met[1][c] + dd[2] * met[2][c];
+  };
+  T du[3], dv[3], dw[3], dT[3], gu[3], gv[3], gw[3], gT[3];
+  deriv(P + 1 * N, du);
+  deriv(P + 2 * N, dv);
+  deriv(P + 3 * N, dw);
+  deriv(P + 5 * N, dT);
+  grad(du, gu);
+  grad(dv, gv);
+  grad(dw, gw);
+  grad(dT, gT);
+  const T mu = T(0.5) * (Pr[p] + Pr[p1]);
+  const T txx = mu * (T(4) * gu[0] - T(2) * gv[1] - T(2) * gw[2]) / T(3);
+  const T tyy = mu * (T(4) * gv[1] - T(2) * gu[0] - T(2) * gw[2]) / T(3);
+  const T tzz = mu * (T(4) * gw[2] - T(2) * gu[0] - T(2) * gv[1]) / T(3);
+  const T txy = mu * (gu[1] + gv[0]);
+  const T txz = mu * (gu[2] + gw[0]);
+  const T tyz = mu * (gv[2] + gw[1]);
+  const T kx = k[0], ky = k[1], kz = k[2];
+  const T f1 = kx * txx + ky * txy + kz * txz;
+  const T f2 = kx * txy + ky * tyy + kz * tyz;
+  const T f3 = kx * txz + ky * tyz + kz * tzz;
+  const T um = T(0.5) * (P[1 * N + p] + P[1 * N + p1]);
+  const T vm = T(0.5) * (P[2 * N + p] + P[2 * N + p1]);
+  const T wm = T(0.5) * (P[3 * N + p] + P[3 * N + p1]);
+  const T lam = T(0.5) * (Pr[N + p] + Pr[N + p1]);
+  T f4 = um * f1 + vm * f2 + wm * f3 + lam * (kx * gT[0] + ky * gT[1] + kz * gT[2]);
+  F[1] -= f1;
+  F[2] -= f2;
+  F[3] -= f3;
+  if (NS == 0 || (NS < 0 && ns == 0)) {
+    F[4] -= f4;
+    return;
+  }
+  const SpecTables<T> &S = tab<T>(C);
+  const T tm = T(0.5) * (P[5 * N + p] + P[5 * N + p1]);
+  T D[A], gy[A][3];
+  T rho_uc = 0, rho_vc = 0, rho_wc = 0;
+#pragma unroll
+  for (int l = 0; l < A; ++l) {
+    if (l < ns) {
+      D[l] = T(0.5) * (Pr[(2 + l) * N + p] + Pr[(2 + l) * N + p1]);
+      T dy[3];
+      deriv(P + (6 + l) * N, dy);
+      grad(dy, gy[l]);
+      const T DMulH = D[l] * nasa_h<T>(S, l, tm);
+      f4 += kx * DMulH * gy[l][0];
+      f4 += ky * DMulH * gy[l][1];
+      f4 += kz * DMulH * gy[l][2];
+      rho_uc += D[l] * gy[l][0];
+      rho_vc += D[l] * gy[l][1];
+      rho_wc += D[l] * gy[l][2];
+    }
+  }
+  F[4] -= f4;
+  const T corr = kx * rho_uc + ky * rho_vc + kz * rho_wc;
+#pragma unroll
+  for (int l = 0; l < A; ++l) {
+    if (l < ns) {
+      const T ym = T(0.5) * (P[(6 + l) * N + p] + P[(6 + l) * N + p1]);
+      F[5 + l] -= D[l] * (kx * gy[l][0] + ky * gy[l][1] + kz * gy[l][2]) - ym * corr;
+    }
+  }
+}
+
+// gamma and acoustic speed of a point (Field.cu:187-200)
+template <typename T, int NS>
+__device__ __forceinline__ void gamma_and_c(const ChemParams &C, T temp, const T *Y, T &gamma, T &c) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  if (NS == 0 || (NS < 0 && ns == 0)) {
+    gamma = T(kGammaAir);
+    c = sqrt(T(kGammaAir * kRu / kMwAir) * temp);
+    return;
+  }
+  const SpecTables<T> &S = tab<T>(C);
+  T mwi = 0, cp_tot = 0, cvv = 0;
+#pragma unroll
+  for (int l = 0; l < A; ++l) {
+    if (l < ns) {
+      const T cp = nasa_cp<T>(S, l, temp);
+      mwi += Y[l] * S.inv_mw[l];
+      cp_tot += Y[l] * cp;
+      cvv += Y[l] * (cp - S.cv_shift[l]);
+    }
+  }
+  gamma = cp_tot / cvv;
+  c = sqrt(gamma * T(kRu) * temp * mwi);
+}
+
+template <typename T, int NS>
+__global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
+    k_stage(const StageArgs<T> a, const __grid_constant__ ChemParams C) {
+  constexpr int A = SpecCount<NS>::kArr;
+  constexpr int NV = 5 + A;
+  const int ns = SpecCount<NS>::n(C);
+  const int nv = 5 + ns;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sFx = reinterpret_cast<T *>(smem_raw);              // [NV][kTY][kTX+1]
+  T *sFy = sFx + NV * kTY * (kTX + 1);                   // [NV][kTY+1][kTX]
+  T *sFz0 = sFy + NV * (kTY + 1) * kTX;                  // [NV][kTY][kTX]
+  T *sFz1 = sFz0 + NV * kTY * kTX;
+  constexpr int XS = kTY * (kTX + 1), YS = (kTY + 1) * kTX, ZS = kTY * kTX;
+
+  const Tile t = a.tiles[blockIdx.x];
+  const BlockInfo B = a.blocks[t.blk];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = t.i0 + tx, j = t.j0 + ty;
+  const bool act = (i < B.mx) && (j < B.my);
+  const int64_t N = a.N;
+  const int64_t s[3] = {1, (int64_t)B.nx, (int64_t)B.nx * B.ny};
+  const int64_t col = B.base + i + s[1] * j;
+  const T *__restrict__ P = a.P;
+  const T *__restrict__ Pr = a.Pr;
+  const T *__restrict__ G = a.G;
+  const bool three_d = B.mz > 1;
+  T F[NV];
+
+  const bool ex_x = (ty == 1) && (tx < kTY) && (t.j0 + tx < B.my);  // -x boundary face of row tx
+  const bool ex_y = (ty == 0) && act;                               // -y boundary face of column tx
+  unsigned flags = 0;
+  double dt_min = 1e300;
+  T *zprev = sFz1, *zcur = sFz0;
+
+  // k = k0-1 only produces the -z face of the first plane.  Every face flux
+  // goes through the single call site below, so a face shared by two tiles
+  // or two blocks is computed by identical instructions.
+  for (int k = t.k0 - 1; k < t.k1; ++k) {
+    const int64_t p = col + s[2] * k;
+    const bool first = (k < t.k0);
+#pragma unroll 1
+    for (int it = 0; it < 5; ++it) {
+      bool doit;
+      int d;
+      int64_t pf = p;
+      T *dst;
+      int ds;
+      if (it == 0) {
+        doit = act && three_d;
+        d = 2, dst = zcur + ty * kTX + tx, ds = ZS;
+      } else if (it == 1) {
+        doit = act && !first;
+        d = 0, dst = sFx + ty * (kTX + 1) + tx + 1, ds = XS;
+      } else if (it == 2) {
+        doit = act && !first;
+        d = 1, dst = sFy + (ty + 1) * kTX + tx, ds = YS;
+      } else if (it == 3) {
+        doit = ex_x && !first;
+        d = 0, dst = sFx + tx * (kTX + 1), ds = XS;
+        pf = B.base + (t.i0 - 1) + s[1] * (t.j0 + tx) + s[2] * k;
+      } else {
+        doit = ex_y && !first;
+        d = 1, dst = sFy + tx, ds = YS;
+        pf = p - s[1];
+      }
+      if (doit) {
+        face_flux<T, NS>(C, P, Pr, G, N, pf, d, s, F);
+#pragma unroll
+        for (int l = 0; l < NV; ++l)
+          if (l < nv) dst[l * ds] = F[l];
+      }
+    }
+    if (first) {
+      T *tmp = zprev;
+      zprev = zcur;
+      zcur = tmp;
+      continue;
+    }
+    __syncthreads();
+    if (act) {
+      // dq = -(sum over directions of F(+1/2) - F(-1/2))
+      double dq[NV];
+#pragma unroll
+      for (int l = 0; l < NV; ++l) {
+        if (l < nv) {
+          T acc = (sFx[l * XS + ty * (kTX + 1) + tx + 1] - sFx[l * XS + ty * (kTX + 1) + tx]);
+          acc += (sFy[l * YS + (ty + 1) * kTX + tx] - sFy[l * YS + ty * kTX + tx]);
+          if (three_d) acc += (zcur[l * ZS + ty * kTX + tx] - zprev[l * ZS + ty * kTX + tx]);
+          dq[l] = -(double)acc;
+        }
+      }
+      // time step of this point: global (RK) or local (steady, from the current state)
+      double dt;
+      if (a.local_dt) {
+        T Y[A];
+#pragma unroll
+        for (int l = 0; l < A; ++l)
+          if (l < ns) Y[l] = P[(6 + l) * N + p];
+        T gam, c;
+        gamma_and_c<T, NS>(C, P[5 * N + p], Y, gam, c);
+        dt = local_time_step<T>(C, G, N, p, (double)P[p], (double)P[N + p], (double)P[2 * N + p],
+                                (double)P[3 * N + p], (double)c, (double)gam, (double)Pr[p], three_d);
+      } else {
+        dt = *a.dt;
+      }
+      const double dtj = dt / (double)G[p];
+      double q[NV];
+#pragma unroll
+      for (int l = 0; l < NV; ++l) {
+        if (l < nv) {
+          double qs = a.Qin[l * N + p] + dq[l] * dtj;
+          if (l == 3 && !three_d) qs = 0;
+          q[l] = (a.a != 0.0) ? a.a * a.Qn[l * N + p] + a.b * qs : qs;
+          a.Qout[l * N + p] = q[l];
+        }
+      }
+      // primitives (TimeAdvanceFunc.cu:266-289), FP64
+      const double rho = q[0];
+      const double inv = 1.0 / rho;
+      const double u = q[1] * inv, v = q[2] * inv, w = q[3] * inv;
+      const double vel2 = u * u + v * v + w * w;
+      double pres, temp;
+      double Yd[A];
+      if (NS == 0 || (NS < 0 && ns == 0)) {
+        pres = (kGammaAir - 1) * (q[4] - 0.5 * rho * vel2);
+        temp = pres * kMwAir * inv / kRu;
+      } else {
+        double ysum = 0;
+#pragma unroll
+        for (int l = 0; l < A; ++l)
+          if (l < ns) Yd[l] = q[5 + l] * inv, ysum += Yd[l];
+        if (a.renorm_y) {
+          const double r = 1.0 / ysum;
+#pragma unroll
+          for (int l = 0; l < A; ++l)
+            if (l < ns) Yd[l] *= r;
+        }
+        double mwi = 0;
+#pragma unroll
+        for (int l = 0; l < A; ++l)
+          if (l < ns) mwi += Yd[l] * C.d.inv_mw[l];
+        const double gas_const = kRu * mwi;
+        const double e = q[4] * inv - 0.5 * vel2;
+        bool capped;
+        temp = newton_temperature<NS>(C, e, Yd, gas_const, (double)P[5 * N + p], capped);
+        if (capped) flags |= kStatusNewtonCap;
+        pres = rho * temp * gas_const;
+      }
+      if (!(rho > 0) || !(pres > 0) || !(temp > 0) || !isfinite(q[4])) flags |= kStatusNonFinite;
+      T* Pn = a.Pn;
+      Pn[p] = T(rho);
+      Pn[N + p] = T(u);
+      Pn[2 * N + p] = T(v);
+      Pn[3 * N + p] = T(w);
+      Pn[4 * N + p] = T(pres);
+      Pn[5 * N + p] = T(temp);
+      T Yt[A];
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) Yt[l] = T(Yd[l]), Pn[(6 + l) * N + p] = Yt[l];
+      T mu, lam, rd[A], gam, c;
+      point_props<T, NS>(C, T(temp), Yt, mu, lam, rd, gam, c);
+      T* Prn = a.Prn;
+      Prn[p] = mu;
+      Prn[N + p] = lam;
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) Prn[(2 + l) * N + p] = rd[l];
+      if (a.dt_next) {
+        const double dtl = local_time_step<T>(C, G, N, p, rho, u, v, w, (double)c, (double)gam, (double)mu, three_d);
+        dt_min = fmin(dt_min, dtl);
+      }
+    }
+    T *tmp = zprev;
+    zprev = zcur;
+    zcur = tmp;
+    __syncthreads();
+  }
+  if (a.dt_next) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dt_min = fmin(dt_min, __shfl_xor_sync(0xffffffffu, dt_min, o));
+    if (tx == 0) atomic_min_pos_double(a.dt_next, dt_min);
+  }
+  const unsigned any = __reduce_or_sync(0xffffffffu, flags);
+  if (any && tx == 0) atomicOr(a.status, any);
+}
+
+// ---------------------------------------------------------------- halo
+
+template <typename T>
+struct RefPtrs {
+  const T *P;
+  const T *Pr;
+  const double *Q;
+  int64_t stride;
+  int64_t idx;
+};
+
+template <typename T>
+__device__ __forceinline__ RefPtrs<T> resolve(const HaloArgs<T> &a, const HaloRef &r) {
+  if (r.kind == 0) return {a.P, a.Pr, a.Q, a.N, r.idx};
+  if (r.kind == 1) return {a.Pprev, a.Prprev, a.Qprev, a.N, r.idx};
+  return {a.sP, a.sPr, a.sQ, a.NS_cap, r.idx};
+}
+
+// Total energy of a point from primitives (Thermo.cu:66-86), FP64.
+template <int NS>
+__device__ __forceinline__ double total_energy(const ChemParams &C, double rho, double u, double v, double w, double p,
+                                               double t, const double *Y) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  double e = 0.5 * rho * (u * u + v * v + w * w);
+  if (NS == 0 || (NS < 0 && ns == 0)) return e + p / (kGammaAir - 1);
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) e += nasa_h<double>(C.d, l, t) * (rho * Y[l]);
+  return e - p;
+}
+
+// Phase A: evaluate the halo nodes of one level into scratch slots.
+template <typename T, int NS>
+__global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemParams C) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  const int nv = 5 + ns;
+  const int64_t e = a.begin + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= a.end) return;
+  const HaloNode nd = a.nodes[e];
+  const int64_t o = nd.slot;
+  const int64_t S = a.NS_cap;
+  double pr[6];
+  double Y[A];
+  double q[5 + A];
+  bool props_copy = false;
+  RefPtrs<T> ra = resolve(a, nd.a);
+  if (nd.op == kHaloCopy) {
+    for (int f = 0; f < 6 + ns; ++f) a.sP[f * S + o] = ra.P[f * ra.stride + ra.idx];
+    for (int f = 0; f < 2 + ns; ++f) a.sPr[f * S + o] = ra.Pr[f * ra.stride + ra.idx];
+    for (int f = 0; f < nv; ++f) a.sQ[f * S + o] = ra.Q[f * ra.stride + ra.idx];
+    return;
+  }
+  if (nd.op == kHaloAvg) {
+    RefPtrs<T> rb = resolve(a, nd.b);
+    bool same = true;
+    for (int f = 0; f < 6 + ns; ++f) {
+      const T x = ra.P[f * ra.stride + ra.idx], y = rb.P[f * rb.stride + rb.idx];
+      same = same && (x == y);
+      a.sP[f * S + o] = T(0.5) * (y + x);
+    }
+    for (int f = 0; f < nv; ++f) a.sQ[f * S + o] = 0.5 * (rb.Q[f * rb.stride + rb.idx] + ra.Q[f * ra.stride + ra.idx]);
+    if (same) {
+      for (int f = 0; f < 2 + ns; ++f) a.sPr[f * S + o] = ra.Pr[f * ra.stride + ra.idx];
+      return;
+    }
+    // averaged state: recompute its transport properties below
+    for (int f = 0; f < 6; ++f) pr[f] = (double)a.sP[f * S + o];
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) Y[l] = (double)a.sP[(6 + l) * S + o];
+  } else {
+    const BcDevice &bc = a.bcs[nd.bc];
+    if (nd.op == kHaloInflow) {
+      pr[0] = bc.rho, pr[1] = bc.u, pr[2] = bc.v, pr[3] = bc.w, pr[4] = bc.p, pr[5] = bc.T;
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) Y[l] = bc.yk[l];
+      for (int f = 0; f < 6; ++f) a.sP[f * S + o] = T(pr[f]);
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) a.sP[(6 + l) * S + o] = T(Y[l]);
+      a.sQ[o] = bc.rho;
+      a.sQ[S + o] = bc.rho * bc.u;
+      a.sQ[2 * S + o] = bc.rho * bc.v;
+      a.sQ[3 * S + o] = bc.rho * bc.w;
+      a.sQ[4 * S + o] = bc.rhoE;
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) a.sQ[(5 + l) * S + o] = bc.rho * bc.yk[l];
+      a.sPr[o] = T(bc.mu);
+      a.sPr[S + o] = T(bc.lam);
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) a.sPr[(2 + l) * S + o] = T(bc.rho_d[l]);
+      props_copy = true;
+    } else {
+      // BoundCond.cu:529-629 apply_wall
+      const double t_in = (double)ra.P[5 * ra.stride + ra.idx];
+      const double p_in = (double)ra.P[4 * ra.stride + ra.idx];
+      double mwi = 0;
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) Y[l] = (double)ra.P[(6 + l) * ra.stride + ra.idx], mwi += Y[l] * C.d.inv_mw[l];
+      const double mw = (NS == 0 || (NS < 0 && ns == 0)) ? kMwAir : 1.0 / mwi;
+      if (nd.op == kHaloWallFace) {
+        const double tw = bc.thermal_type == 1 ? t_in : bc.t_wall;
+        pr[0] = p_in * mw / (tw * kRu);
+        pr[1] = pr[2] = pr[3] = 0;
+        pr[4] = p_in;
+        pr[5] = tw;
+      } else {
+        RefPtrs<T> rb = resolve(a, nd.b);
+        const double tw = bc.thermal_type == 1 ? (double)rb.P[5 * rb.stride + rb.idx] : bc.t_wall;
+        double tg = t_in;
+        if (bc.thermal_type == 0) {
+          tg = 2 * tw - t_in;
+          if (tg <= 0.1 * tw) tg = tw;
+        }
+        pr[0] = p_in * mw / (tg * kRu);
+        pr[1] = -(double)ra.P[1 * ra.stride + ra.idx];
+        pr[2] = -(double)ra.P[2 * ra.stride + ra.idx];
+        pr[3] = -(double)ra.P[3 * ra.stride + ra.idx];
+        pr[4] = p_in;
+        pr[5] = tg;
+      }
+      for (int f = 0; f < 6; ++f) a.sP[f * S + o] = T(pr[f]);
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) a.sP[(6 + l) * S + o] = T(Y[l]);
+      q[0] = pr[0];
+      q[1] = pr[0] * pr[1];
+      q[2] = pr[0] * pr[2];
+      q[3] = pr[0] * pr[3];
+      q[4] = total_energy<NS>(C, pr[0], pr[1], pr[2], pr[3], pr[4], pr[5], Y);
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) q[5 + l] = Y[l] * pr[0];
+      for (int f = 0; f < nv; ++f) a.sQ[f * S + o] = q[f];
+    }
+  }
+  if (!props_copy) {
+    T Yt[A], mu, lam, rd[A], gam, c;
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) Yt[l] = T(Y[l]);
+    point_props<T, NS>(C, T(pr[5]), Yt, mu, lam, rd, gam, c);
+    a.sPr[o] = mu;
+    a.sPr[S + o] = lam;
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) a.sPr[(2 + l) * S + o] = rd[l];
+  }
+}
+
+// Phase B: write every changed point from its resolved source.
+template <typename T>
+__global__ void k_halo_copies(const HaloArgs<T> a, int np, int npr, int nq) {
+  const int64_t e = a.begin + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= a.end) return;
+  const HaloCopy c = a.copies[e];
+  const RefPtrs<T> r = resolve(a, c.src);
+  for (int f = 0; f < np; ++f) a.P[f * a.N + c.dst] = r.P[f * r.stride + r.idx];
+  for (int f = 0; f < npr; ++f) a.Pr[f * a.N + c.dst] = r.Pr[f * r.stride + r.idx];
+  for (int f = 0; f < nq; ++f) a.Q[f * a.N + c.dst] = r.Q[f * r.stride + r.idx];
+}
+
+// ------------------------------------------------------------ setup / misc
+
+// Field.cu:150-176 compute_cv_from_bv over every arena point (FP64 input).
+template <int NS>
+__global__ void k_cv_from_bv(const __grid_constant__ ChemParams C, const double *P0, double *Q, int64_t N) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const double rho = P0[p], u = P0[N + p], v = P0[2 * N + p], w = P0[3 * N + p], pr = P0[4 * N + p], t = P0[5 * N + p];
+  if (!(rho > 0)) return;  // padding points of the arena
+  double Y[A];
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) Y[l] = P0[(6 + l) * N + p];
+  Q[p] = rho;
+  Q[N + p] = rho * u;
+  Q[2 * N + p] = rho * v;
+  Q[3 * N + p] = rho * w;
+  Q[4 * N + p] = total_energy<NS>(C, rho, u, v, w, pr, t, Y);
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) Q[(5 + l) * N + p] = rho * Y[l];
+}
+
+// Transport properties at every arena point (Field.cu:178-210).
+template <typename T, int NS>
+__global__ void k_props_all(const __grid_constant__ ChemParams C, const T *P, T *Pr, int64_t N) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  if (!(P[p] > T(0))) return;
+  T Y[A], mu, lam, rd[A], gam, c;
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) Y[l] = P[(6 + l) * N + p];
+  point_props<T, NS>(C, P[5 * N + p], Y, mu, lam, rd, gam, c);
+  Pr[p] = mu;
+  Pr[N + p] = lam;
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) Pr[(2 + l) * N + p] = rd[l];
+}
+
+// Global time step of the current state over interior points.
+template <typename T, int NS>
+__global__ void k_dt_reduce(const __grid_constant__ ChemParams C, const BlockInfo *blocks, int nblocks, const T *P,
+                            const T *Pr, const T *G, int64_t N, int64_t n_interior_total,
+                            unsigned long long *dt_out) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  double m = 1e300;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_interior_total;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    int b = 0;
+    while (b + 1 < nblocks && blocks[b + 1].interior_off <= g) ++b;
+    const BlockInfo B = blocks[b];
+    const int64_t r = g - B.interior_off;
+    const int i = (int)(r % B.mx);
+    const int j = (int)((r / B.mx) % B.my);
+    const int k = (int)(r / ((int64_t)B.mx * B.my));
+    const int64_t p = B.base + i + (int64_t)B.nx * j + (int64_t)B.nx * B.ny * k;
+    T Y[A], gam, c;
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) Y[l] = P[(6 + l) * N + p];
+    gamma_and_c<T, NS>(C, P[5 * N + p], Y, gam, c);
+    const double dtl = local_time_step<T>(C, G, N, p, (double)P[p], (double)P[N + p], (double)P[2 * N + p],
+                                          (double)P[3 * N + p], (double)c, (double)gam, (double)Pr[p], B.mz > 1);
+    m = fmin(m, dtl);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomic_min_pos_double(dt_out, m);
+}
+
+}  // namespace ccb

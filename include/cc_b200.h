@@ -1,0 +1,169 @@
+/*
+ * cc_b200.h -- C ABI of the B200 (sm_100a) residual path of CombustionCodeGPU.
+ *
+ * The reference has no FFI; its operator surface is the C++ stack
+ *   Driver(Parameter&, Mesh&, ChemData&)      Driver.h:17-26, main.cu:37-45
+ *   Driver::initialize_computation()          Driver.cu:59-97
+ *   Driver::simulate() / steady_simulation()  Driver.cu:99-192
+ *   Field{HZone, DZone*}, DParameter          Field.h:36-82, DParameter.h:9-39
+ *   Boundary / InnerFace                      Mesh.h:9-60
+ * Every entry point below names the reference interface it replaces.  All
+ * functions return 0 on success and a negative code on failure; the message
+ * of the last failure on the calling thread is returned by cc_last_error().
+ * Plain pointers and sizes only; the library owns all device memory.
+ *
+ * Array layout of host buffers: per block, structure-of-arrays over the full
+ * ghosted box (mx+2g) x (my+2g) x (mz+2g), i fastest, g = ngg ghost layers:
+ *   element (i,j,k) of field f at  f*Ng + (i+g) + (mx+2g)*((j+g) + (my+2g)*(k+g)).
+ */
+#ifndef CC_B200_H
+#define CC_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CC_MAX_SPECIES 16
+
+enum cc_status_code {
+  CC_OK = 0,
+  CC_ERR_ARG = -1,       /* invalid argument */
+  CC_ERR_STATE = -2,     /* call out of order (e.g. cc_step before cc_init) */
+  CC_ERR_CUDA = -3,      /* a CUDA call failed (message in cc_last_error) */
+  CC_ERR_TOPOLOGY = -4,  /* boundary/interface layout the halo program cannot express */
+  CC_ERR_NODEVICE = -5   /* no CUDA device */
+};
+
+enum cc_precision {
+  CC_FP64 = 0,   /* plain: every field and every operation in FP64 */
+  CC_MIXED = 1   /* reconstruction, fluxes, transport, stored primitives in FP32;
+                    conserved variables, RK accumulation, Newton, Y renormalisation,
+                    dt and residual reductions in FP64 */
+};
+
+enum cc_time_scheme {
+  CC_RK3 = 0,          /* SSP-RK3 with a global time step (min of the local CFL step) */
+  CC_STEADY_EULER = 1  /* the reference's loop: explicit Euler with the per-point local step */
+};
+
+/* Scalar parameters and species tables, as in DParameter (DParameter.h:9-39)
+ * and Species (ChemData.h:11-46).  n_spec == 0 selects the calorically
+ * perfect air model (the reference's MULTISPECIES=0 build).  Tables are
+ * copied by cc_create. */
+typedef struct cc_params {
+  int n_spec;
+  int inviscid_scheme;   /* 3 = AUSM+ (the only scheme of the reference) */
+  int reconstruction;    /* 2 = MUSCL, other = first order */
+  int limiter;           /* 0/1 = minmod */
+  int viscous_order;     /* 0 = inviscid, 2 = second-order central */
+  int ngg;               /* ghost layers, 2 (Parameter.cpp:32-36) */
+  double prandtl_number, cfl, schmidt_number;
+  const double *mw;                  /* [n_spec] molecular weights */
+  const double *t_low, *t_mid, *t_high;
+  const double *low_temp_coeff;      /* [n_spec][7] NASA-7, T < t_mid */
+  const double *high_temp_coeff;     /* [n_spec][7] NASA-7, T >= t_mid */
+  const double *LJ_potent_inv;       /* [n_spec] 1/(eps/k) */
+  const double *vis_coeff;           /* [n_spec] 2.6693e-6 sqrt(W)/sigma^2 */
+  const double *WjDivWi_to_One4th;   /* [n_spec][n_spec] */
+  const double *sqrt_WiDivWjPl1Mul8; /* [n_spec][n_spec] */
+} cc_params;
+
+/* Byte-compatible with cfd::Boundary after register_boundary (Mesh.h:9-32). */
+typedef struct cc_boundary {
+  int range_start[3];
+  int range_end[3];
+  int type_label;
+  int face;
+  int direction;
+} cc_boundary;
+
+/* Byte-compatible with cfd::InnerFace after register_boundary (Mesh.h:34-60). */
+typedef struct cc_inner_face {
+  int range_start[3];
+  int range_end[3];
+  int face;
+  int direction;
+  int target_start[3];
+  int target_end[3];
+  int target_block;
+  int target_face;
+  int target_direction;
+  int src_tar[3];
+  int loop_dir[3];
+  int target_loop_dir[3];
+} cc_inner_face;
+
+/* A boundary condition bound to a face label (BoundCond.h:14-64):
+ * kind 6 outflow, 5 inflow (Dirichlet state), 2 wall. */
+typedef struct cc_bc {
+  int label;
+  int kind;
+  int thermal_type;   /* wall: 0 isothermal, 1 adiabatic */
+  int pad;
+  double t_wall;
+  double density, u, v, w, pressure, temperature;  /* inflow */
+  double yk[CC_MAX_SPECIES];                       /* inflow mass fractions */
+} cc_bc;
+
+typedef struct cc_ctx cc_ctx;
+
+const char *cc_last_error(void);
+int cc_version(void);
+int cc_device_count(int *n);
+
+/* Driver::Driver + DParameter::DParameter (Driver.cu:17-57, DParameter.cu:4-45). */
+int cc_create(const cc_params *params, cc_ctx **out);
+int cc_destroy(cc_ctx *ctx);
+
+/* Mesh/Field setup for one block (Field::setup_device_memory, Field.cu:90-148):
+ * jac [Ng] and metric [9][Ng] (row r*3+c = m(r+1,c+1), Mesh.cpp:226-488). */
+int cc_add_block(cc_ctx *ctx, int mx, int my, int mz, const double *jac, const double *metric, int *block_id);
+/* Boundary::register_boundary (Mesh.cpp:14-32): raw = x1,x2,y1,y2,z1,z2,type. */
+int cc_register_boundary(const int raw[7], int ngg, cc_boundary *out);
+/* InnerFace::InnerFace + register_boundary (Mesh.cpp:35-143): 13 raw ints. */
+int cc_register_inner_face(const int raw[13], int ngg, cc_inner_face *out);
+/* Block::boundary / Block::inner_face entries (processed form). */
+int cc_add_boundary(cc_ctx *ctx, int block, const cc_boundary *b);
+int cc_add_inner_face(cc_ctx *ctx, int block, const cc_inner_face *f);
+/* DBoundCond::initialize_bc_on_GPU (BoundCond.cu:315-409); call after all
+ * faces are added.  Conditions are applied in the reference's priority order
+ * (outflow, inflow, wall; BoundCond.cu:251-313), then the block interfaces. */
+int cc_add_bc(cc_ctx *ctx, const cc_bc *bc);
+
+/* HZone::bv / HZone::yk (Field.h:13-32), copied host -> device:
+ * bv [6][Ng] = rho,u,v,w,p,T;  yk [n_spec][Ng].  Before cc_init it sets the
+ * initial field; afterwards it replaces the state (primitives, conserved
+ * variables and properties are re-derived as by cc_init). */
+int cc_set_state(cc_ctx *ctx, int block, const double *bv, const double *yk);
+/* Driver::initialize_computation (Driver.cu:59-97). */
+int cc_init(cc_ctx *ctx, int precision);
+/* Driver::simulate: n_steps steps of the chosen scheme (Driver.cu:113-192).
+ * want_residual != 0 also evaluates the residual of the last step. */
+int cc_step(cc_ctx *ctx, int n_steps, int scheme, int want_residual);
+/* Driver::compute_residual (Driver.cu:219-277): RMS change of rho, |V|, p, T
+ * over the last step, before the res_scale normalisation. */
+int cc_residual(cc_ctx *ctx, double out[4]);
+/* Device -> host: bv [6][Ng], yk [n_spec][Ng], cv [n_var][Ng]; null skips. */
+int cc_get_state(cc_ctx *ctx, int block, double *bv, double *yk, double *cv);
+/* DZone::mul / conductivity / rho_D (Field.h:52-56): [Ng], [Ng], [n_spec][Ng]. */
+int cc_get_props(cc_ctx *ctx, int block, double *mul, double *conductivity, double *rho_d);
+/* Time step of the last completed step (RK3). */
+int cc_last_dt(cc_ctx *ctx, double *dt);
+/* Device status word: bit 0 Newton iteration cap hit, bit 1 non-finite or
+ * non-positive rho/p/T, bit 2 invalid time step.  Cleared by the call. */
+int cc_status(cc_ctx *ctx, unsigned *flags);
+/* Stream used by every launch of the context (default: a private stream). */
+int cc_set_stream(cc_ctx *ctx, void *cuda_stream);
+void *cc_get_stream(cc_ctx *ctx);
+/* 1 = replay whole steps from a captured CUDA graph (default), 0 = launch. */
+int cc_use_graph(cc_ctx *ctx, int enable);
+/* Points updated per stage (sum of mx*my*mz) and arena bytes on the device. */
+int cc_info(cc_ctx *ctx, int64_t *n_points, int64_t *device_bytes, int *n_tiles, int *n_halo_levels);
+/* Synchronises the context's stream. */
+int cc_sync(cc_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
