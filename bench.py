@@ -1,0 +1,322 @@
+"""Benchmark of the residual path: Mcell-updates/s per RK stage, mixed vs FP64.
+
+Workload (default): the 3D viscous frozen-chemistry periodic box, 128^3
+points on a 2 mm cube, 9 species (synthetic data set in the reference's
+ChemData format), Fourier-mode T/p/Y fields with a Taylor-Green velocity,
+SSP-RK3 at CFL 0.5.  One step = 3 RK stages; value = points x 3 x steps /
+time (summed over ranks).  Inputs stay resident in HBM; the working set
+(~1.8 GB mixed) is far larger than the 126 MB L2, so no flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's CPU implementation of the path on the
+host cores: the reference itself has no CPU path and its CUDA kernels cannot
+be installed as a package, so the arm runs the C restatement of the
+reference's algorithm (oracle/cc_oracle.c, pinned to the reference kernels by
+tests/golden) with every host thread, on a bounded sample of the workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "box128_9sp_viscous_rk3"
+METRIC = "Mcell-updates/s per RK stage, mixed vs FP64 plain, at stated L2 err vs FP64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--err-steps", type=int, default=100, help="steps of the mixed-vs-FP64 error check")
+    return ap.parse_args()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(ns, precision):
+    """Bytes per point per RK stage (each array element once per stage):
+    n_var*(Q^k + Q^n + Q^(k+1)) + 2*T + 10*geometry, at the stored widths."""
+    nv = 5 + ns
+    if precision == "fp64":
+        return nv * 24 + 2 * 8 + 10 * 8
+    return nv * 24 + 2 * 4 + 10 * 4
+
+
+def ncu_traffic(kernel_tag):
+    """DRAM bytes per stage-kernel launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "%s.txt" % kernel_tag)
+    try:
+        for ln in open(path):
+            if ln.startswith("dram_bytes_per_launch:"):
+                return float(ln.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    import combustioncodegpu_b200 as cc
+    from combustioncodegpu_b200 import cases
+
+    torch.cuda.set_device(rank % max(1, torch.cuda.device_count()))
+    sp = cases.synthetic_species()
+    case = cases.case_box(args.n, species=sp, seed=1234)
+    out = {}
+    states = {}
+    for prec in ("fp64", "mixed"):
+        d = cc.Driver.from_case(case, prec)
+        d.initialize_computation()
+        s = torch.cuda.ExternalStream(d.stream())
+        info = d.info()
+        npts = info["n_points"]
+        d.simulate(args.warmup)
+        d.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            e0.record(s)
+            d.simulate(args.steps)
+            e1.record(s)
+            e1.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms], dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        kt = d.time_kernels(2)
+        out[prec] = {"ms_total": ms, "ms_per_step": ms / args.steps, "npts": npts, "clocks": clk.summary(),
+                     "kernels": kt, "info": info, "status": d.status()}
+        d.close()
+    # mixed vs FP64 error after err_steps steps from the same state
+    errs = {}
+    if args.err_steps > 0 and rank == 0:
+        res = {}
+        for prec in ("fp64", "mixed"):
+            d = cc.Driver.from_case(case, prec)
+            d.set_renormalize(True)  # same algorithm in both precisions
+            d.initialize_computation()
+            d.simulate(args.err_steps)
+            bv, yk, cv = d.field[0].get_state()
+            res[prec] = (bv, yk)
+            d.close()
+        n = args.n
+        sl = lambda a: a.reshape(a.shape[0], n + 4, n + 4, n + 4)[:, 2:-2, 2:-2, 2:-2].reshape(a.shape[0], -1)
+        b64, b32 = sl(res["fp64"][0]), sl(res["mixed"][0])
+        y64, y32 = sl(res["fp64"][1]), sl(res["mixed"][1])
+        l2 = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        li = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())
+        names = ["rho", "u", "v", "w", "p", "T"]
+        errs = {"steps": args.err_steps, "reference": "FP64 run of the same scheme (Y renormalised in FP64)"}
+        for i, nm in enumerate(names):
+            errs["l2_" + nm] = l2(b32[i], b64[i])
+            errs["linf_" + nm] = li(b32[i], b64[i])
+        errs["l2_Y"] = l2(y32, y64)
+        errs["linf_Y"] = li(y32, y64)
+    # end-to-end through the C ABI with host buffers (mixed): upload of the
+    # state from pinned memory, K steps each reading back the residual, and the
+    # download of the final state
+    e2e = None
+    if rank == 0:
+        blk = case["blocks"][0]
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        bv_h, yk_h = pin(blk["bv"]), pin(blk["yk"])
+        d = cc.Driver.from_case(case, "mixed")
+        d.initialize_computation()
+        d.simulate(2)
+        d.sync()
+        ng = bv_h.shape[1]
+        bv_o = pin(np.empty_like(bv_h))
+        yk_o = pin(np.empty_like(yk_h))
+        cv_o = pin(np.empty((14, ng)))
+        K = args.steps
+        t0 = time.perf_counter()
+        d.field[0].set_state(bv_h, yk_h)
+        for _ in range(K):
+            d.simulate(1, residual=True)
+            d.residual()
+        cc._check(d.lib.cc_get_state(d.ctx, 0, cc._ptr(bv_o), cc._ptr(yk_o), cc._ptr(cv_o)))
+        dt = time.perf_counter() - t0
+        npts = out["mixed"]["npts"]
+        up = bv_h.nbytes + yk_h.nbytes
+        down = bv_o.nbytes + yk_o.nbytes + cv_o.nbytes + 32 * K
+        e2e = {"value": npts * 3 * K / dt / 1e6, "unit": "Mcell-updates/s", "h2d_bytes_per_step": up / K,
+               "d2h_bytes_per_step": down / K, "timing": "host wall clock, synchronised, whole job"}
+        d.close()
+    return out, errs, e2e
+
+
+def cpu_baseline(args, n_threads, steps=1, n=64):
+    """The oracle on the host cores: bounded sample of the workload (an
+    n^3-point box with the same per-point work, `steps` RK3 steps)."""
+    from combustioncodegpu_b200 import cases
+    from oracle.oracle_py import Oracle
+
+    case = cases.case_box(n, species=cases.synthetic_species(), seed=1234)
+    o = Oracle(case, threads=n_threads)
+    o.init()
+    t0 = time.perf_counter()
+    o.rk3_step(steps)
+    dt = time.perf_counter() - t0
+    pts = n ** 3
+    return {"value": pts * 3 * steps / dt / 1e6, "unit": "Mcell-updates/s", "cores": n_threads, "kind": "port",
+            "sample": "%d^3-point box, same 9-species viscous workload, %d RK3 step(s), FP64" % (n, steps),
+            "seconds": dt}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        import datetime
+        tdist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    n_threads = os.cpu_count() or 1
+    if args.impl == "reference":
+        if rank == 0:
+            per_step = []
+            for _ in range(args.warmup):
+                cpu_baseline(args, n_threads)
+            for _ in range(max(1, args.steps)):
+                per_step.append(cpu_baseline(args, n_threads))
+            v = float(np.median([r["value"] for r in per_step]))
+            base = per_step[0]
+            line = {"metric": METRIC, "value": v, "unit": "Mcell-updates/s", "n_gpus": args.gpus,
+                    "steps": args.steps, "warmup": args.warmup,
+                    "ms_per_step": float(np.median([r["seconds"] for r in per_step])) * 1e3,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic", "impl": "reference",
+                    "config": {"workload": WORKLOAD, "grid": "%d^3 points sampled as 64^3" % args.n, "species": 9},
+                    "cpu_baseline": {"value": v, "unit": "Mcell-updates/s", "cores": n_threads, "kind": "port",
+                                     "sample": base["sample"]},
+                    "e2e": {"value": v, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    out, errs, e2e = run_ours(args, rank, world, dist)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peaks, peak_kind = load_peaks()
+    mixed, plain = out["mixed"], out["fp64"]
+    stages = 3 * args.steps
+    value = world * mixed["npts"] * stages / (mixed["ms_total"] / 1e3) / 1e6
+    value_plain = world * plain["npts"] * stages / (plain["ms_total"] / 1e3) / 1e6
+    bpp = algorithmic_bytes(9, "mixed")
+    stage_ms = mixed["kernels"]["stage_ms"]
+    achieved = bpp * mixed["npts"] / (stage_ms / 1e3) / 1e9
+    traffic = ncu_traffic("stage_kernel_box128_mixed")
+    cpu = cpu_baseline(args, os.cpu_count() or 1, steps=2, n=96)
+    levels = mixed["info"]["halo_levels"]
+    launches_per_step = 3 * (1 + levels + 1) + 1
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 fluxes/transport + f64 conserved/Newton/reductions", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": "%d^3 points, 2 mm periodic cube" % args.n, "species": 9,
+                   "scheme": "MUSCL-minmod + AUSM+ + 2nd-order viscous, SSP-RK3, CFL 0.5",
+                   "precision": "mixed", "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (no flush)", "graph": "one CUDA graph per step"},
+        "plain_fp64": {"value": value_plain, "unit": "Mcell-updates/s", "ms_per_step": plain["ms_per_step"]},
+        "mixed_over_fp64": value / value_plain,
+        "error_mixed_vs_fp64": errs,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "kernel": "k_stage<float,9>", "algorithmic_bytes_per_point": bpp,
+                     "stage_ms_per_launch": stage_ms, "peak_kind": peak_kind},
+        "cpu_baseline": {"value": cpu["value"], "unit": cpu["unit"], "cores": cpu["cores"], "kind": cpu["kind"],
+                         "sample": cpu["sample"]},
+        "e2e": e2e,
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": mixed["clocks"],
+        "status": {"mixed": mixed["status"], "fp64": plain["status"]},
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

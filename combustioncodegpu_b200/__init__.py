@@ -91,8 +91,10 @@ EXPORTS = {
     "cc_set_stream": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "cc_get_stream": ([ctypes.c_void_p], ctypes.c_void_p),
     "cc_use_graph": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "cc_set_renormalize": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_info": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "cc_time_kernels": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp], ctypes.c_int),
     "cc_sync": ([ctypes.c_void_p], ctypes.c_int),
 }
 
@@ -355,8 +357,21 @@ class Driver:
     def set_stream(self, stream_ptr):
         _check(self.lib.cc_set_stream(self.ctx, ctypes.c_void_p(stream_ptr)))
 
+    def set_renormalize(self, enable):
+        """Y renormalisation after each update: True/False, or None for the
+        precision's default (mixed on, FP64 off)."""
+        _check(self.lib.cc_set_renormalize(self.ctx, -1 if enable is None else (1 if enable else 0)))
+
     def use_graph(self, enable=True):
         _check(self.lib.cc_use_graph(self.ctx, 1 if enable else 0))
+
+    def time_kernels(self, n_steps, scheme="rk3"):
+        """Event-timed run without graph replay: dict of mean stage-kernel ms
+        per launch, mean halo ms per stage, launches, stage+halo ms per step."""
+        out = np.zeros(4)
+        sch = SCHEMES[scheme] if isinstance(scheme, str) else int(scheme)
+        _check(self.lib.cc_time_kernels(self.ctx, int(n_steps), sch, _ptr(out)))
+        return {"stage_ms": out[0], "halo_ms": out[1], "stage_launches": int(out[2]), "step_ms": out[3]}
 
     def sync(self):
         _check(self.lib.cc_sync(self.ctx))

@@ -85,6 +85,9 @@ def synthetic_species(species=H2O2_N2_SPECIES, seed=2024):
             A = np.vstack([T ** p for p in range(5)]).T
             cp = _cp_model(n_atoms, linear, thetas, T)
             out[k, :5] = np.linalg.lstsq(A, cp, rcond=None)[0]
+        # cp continuous at T_mid: shift the high-range constant term
+        at_mid = lambda c: sum(c[p] * T_MID ** p for p in range(5))
+        high[k, 0] += at_mid(low[k]) - at_mid(high[k])
 
         def h_poly(c, T):
             return c[0] * T + c[1] * T ** 2 / 2 + c[2] * T ** 3 / 3 + c[3] * T ** 4 / 4 + c[4] * T ** 5 / 5

@@ -91,6 +91,10 @@ struct cc_ctx {
   double *d_res = nullptr;
   double *d_partials = nullptr;
   double *d_last = nullptr;
+  double *d_vel = nullptr;        // DZone::vel: |V| of the last update
+  int64_t *d_vel_zero = nullptr;  // wall-face points (vel = 0 after the wall condition)
+  uint32_t *d_skip_dt = nullptr;  // bitmask: interior points the halo rewrites
+  int renorm = -1;                // Y renormalisation: -1 = by precision (mixed on, FP64 off)
   int n_partials = 296;
 
   cudaStream_t stream = nullptr;
@@ -99,6 +103,10 @@ struct cc_ctx {
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int64_t device_bytes = 0;
   std::vector<void *> allocs;
+  // kernel timing (cc_time_kernels): events around every stage and halo launch
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_stage, ev_halo;
+  size_t ev_next_stage = 0, ev_next_halo = 0;
 };
 
 namespace {
@@ -321,6 +329,21 @@ int setup_device(cc_ctx *c) {
   c->d_partials = (double *)p;
   if (dev_alloc(c, &p, sizeof(double) * 4 * std::max<int64_t>(1, c->n_int))) return CC_ERR_CUDA;
   c->d_last = (double *)p;
+  if (dev_alloc(c, &p, sizeof(double) * N)) return CC_ERR_CUDA;
+  c->d_vel = (double *)p;
+  {
+    std::vector<uint32_t> mask((size_t)(N / 32 + 1), 0u);
+    for (const auto &cp : c->plan.copies)
+      if (cp.src.pad & 1) mask[(size_t)(cp.dst >> 5)] |= 1u << (cp.dst & 31);
+    if (dev_alloc(c, &p, sizeof(uint32_t) * mask.size())) return CC_ERR_CUDA;
+    c->d_skip_dt = (uint32_t *)p;
+    CK(cudaMemcpy(c->d_skip_dt, mask.data(), sizeof(uint32_t) * mask.size(), cudaMemcpyHostToDevice));
+  }
+  if (dev_alloc(c, &p, sizeof(int64_t) * std::max<size_t>(1, c->plan.vel_zero.size()))) return CC_ERR_CUDA;
+  c->d_vel_zero = (int64_t *)p;
+  if (!c->plan.vel_zero.empty())
+    CK(cudaMemcpyAsync(c->d_vel_zero, c->plan.vel_zero.data(), sizeof(int64_t) * c->plan.vel_zero.size(),
+                       cudaMemcpyHostToDevice, c->stream));
 
   CK(cudaMemcpyAsync(c->d_blocks, c->hblocks.data(), sizeof(BlockInfo) * c->hblocks.size(), cudaMemcpyHostToDevice,
                      c->stream));
@@ -367,15 +390,17 @@ HaloArgs<T> halo_args(cc_ctx *c, int pn, int pp, double *qn, const double *qp) {
 }
 
 template <typename T, int NS>
-int run_halo(cc_ctx *c, int pn, int pp, double *qn, const double *qp) {
+int run_halo(cc_ctx *c, int pn, int pp, double *qn, const double *qp, unsigned long long *dt_next = nullptr) {
   HaloArgs<T> h = halo_args<T, NS>(c, pn, pp, qn, qp);
+  h.G = (const T *)c->G;
+  h.dt_next = dt_next;
   const auto &lb = c->plan.level_begin;
   for (size_t l = 0; l + 1 < lb.size(); ++l) {
     h.begin = lb[l], h.end = lb[l + 1];
     CK((Launch<T, NS>::halo_nodes(h, c->chem, c->stream)));
   }
   h.begin = 0, h.end = (int64_t)c->plan.copies.size();
-  CK((Launch<T, NS>::halo_copies(h, np_of(c), npr_of(c), nv_of(c), c->stream)));
+  CK((Launch<T, NS>::halo_copies(h, c->chem, c->stream)));
   return 0;
 }
 
@@ -387,13 +412,14 @@ int derive_state(cc_ctx *c) {
   const int64_t N = c->N;
   c->qcur = 0;
   CK((Launch<T, NS>::configure()));
-  CK((Launch<T, NS>::cv_from_bv(c->chem, c->stage64, c->Q[0], N, c->stream)));
+  CK((Launch<T, NS>::cv_from_bv(c->chem, c->stage64, c->Q[0], N, c->d_vel, c->stream)));
   CK(cudaMemcpyAsync(c->Q[1], c->Q[0], sizeof(double) * N * nv_of(c), cudaMemcpyDeviceToDevice, c->stream));
   if (int r = from64(c, c->stage64, c->P[0], N * np_of(c))) return r;
   CK((Launch<T, NS>::props_all(c->chem, (const T *)c->P[0], (T *)c->Pr[0], N, c->stream)));
   CK(cudaMemcpyAsync(c->P[1], c->P[0], c->elem * N * np_of(c), cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->Pr[1], c->Pr[0], c->elem * N * npr_of(c), cudaMemcpyDeviceToDevice, c->stream));
   if (int r = run_halo<T, NS>(c, 1, 0, c->Q[0], c->Q[1])) return r;
+  CK(launch_zero_points(c->d_vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream));
   c->cur = 1;
   // inflow transport properties: evaluated once by the same point function
   CK((Launch<T, NS>::dt_reduce(c->chem, c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[1],
@@ -428,7 +454,7 @@ int prepare_inflow(cc_ctx *c) {
   CK(cudaMalloc(&dPT, c->elem * np * M));
   CK(cudaMalloc(&dPr, c->elem * npr_of(c) * M));
   CK(cudaMemcpyAsync(dP, h.data(), sizeof(double) * np * M, cudaMemcpyHostToDevice, c->stream));
-  CK((Launch<T, NS>::cv_from_bv(c->chem, dP, dQ, M, c->stream)));
+  CK((Launch<T, NS>::cv_from_bv(c->chem, dP, dQ, M, nullptr, c->stream)));
   if (int r = from64(c, dP, dPT, np * M)) return r;
   CK((Launch<T, NS>::props_all(c->chem, (const T *)dPT, (T *)dPr, M, c->stream)));
   std::vector<double> q((size_t)nv_of(c) * M);
@@ -456,6 +482,30 @@ int prepare_inflow(cc_ctx *c) {
   return 0;
 }
 
+int prof_event(cc_ctx *c, std::vector<cudaEvent_t> &pool, size_t &next) {
+  if (!c->profiling) return 0;
+  if (next == pool.size()) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    pool.push_back(e);
+  }
+  CK(cudaEventRecord(pool[next++], c->stream));
+  return 0;
+}
+
+template <typename T, int NS>
+int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin) {
+  const int nt = (int)c->htiles.size();
+  if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
+  CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
+  if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
+  if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
+  if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next)) return r;
+  if (a.vel) CK(launch_zero_points(c->d_vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream));
+  if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
+  return 0;
+}
+
 template <typename T, int NS>
 int enqueue_step(cc_ctx *c, int scheme) {
   StageArgs<T> a{};
@@ -465,15 +515,14 @@ int enqueue_step(cc_ctx *c, int scheme) {
   a.G = (const T *)c->G;
   a.dt = c->d_dt;
   a.status = c->d_status;
-  a.renorm_y = (c->precision != CC_FP64 && c->chem.ns > 0) ? 1 : 0;
-  const int nt = (int)c->htiles.size();
+  a.skip_dt = c->d_skip_dt;
+  a.renorm_y = c->chem.ns > 0 && (c->renorm < 0 ? c->precision != CC_FP64 : c->renorm != 0);
   if (scheme == CC_STEADY_EULER) {
     const int pc = c->cur, pn = 1 - c->cur;
     a.P = (const T *)c->P[pc], a.Pn = (T *)c->P[pn], a.Pr = (const T *)c->Pr[pc], a.Prn = (T *)c->Pr[pn];
     a.Qin = c->Q[c->qcur], a.Qn = nullptr, a.Qout = c->Q[c->qcur];
-    a.a = 0.0, a.b = 1.0, a.local_dt = 1, a.dt_next = nullptr;
-    CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
-    if (int r = run_halo<T, NS>(c, pn, pc, c->Q[c->qcur], c->Q[c->qcur])) return r;
+    a.a = 0.0, a.b = 1.0, a.local_dt = 1, a.dt_next = nullptr, a.vel = c->d_vel;
+    if (int r = stage_and_halo<T, NS>(c, a, pn, pc, c->Q[c->qcur], c->Q[c->qcur])) return r;
     c->cur = pn;
     return 0;
   }
@@ -488,8 +537,8 @@ int enqueue_step(cc_ctx *c, int scheme) {
     a.Qin = qin, a.Qn = qa, a.Qout = qout;
     a.a = A[st], a.b = Bc[st], a.local_dt = 0;
     a.dt_next = (st == 2 && !c->plan.has_wall) ? c->d_dt_next : nullptr;
-    CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
-    if (int r = run_halo<T, NS>(c, pn, pc, qout, qin)) return r;
+    a.vel = st == 2 ? c->d_vel : nullptr;
+    if (int r = stage_and_halo<T, NS>(c, a, pn, pc, qout, qin)) return r;
     c->cur = pn;
   }
   if (c->plan.has_wall)
@@ -587,6 +636,8 @@ int cc_destroy(cc_ctx *c) {
   if (!c) return 0;
   if (c->stream) cudaStreamSynchronize(c->stream);
   destroy_graphs(c);
+  for (auto e : c->ev_stage) cudaEventDestroy(e);
+  for (auto e : c->ev_halo) cudaEventDestroy(e);
   for (void *p : c->allocs) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -747,13 +798,13 @@ int cc_step(cc_ctx *c, int n_steps, int scheme, int want_residual) {
     constexpr int NS = decltype(nn)::value;
     for (int s = 0; s < n_steps; ++s) {
       if (want_residual && s == n_steps - 1)
-        CK(launch_store_last<T>(c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur], c->N, c->n_int,
-                                c->d_last, c->stream));
+        CK(launch_store_last<T>(c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur], c->d_vel, c->N,
+                                c->n_int, c->d_last, c->stream));
       if (int r = step_once<T, NS>(c, scheme)) return r;
     }
     if (want_residual && n_steps > 0)
-      CK(launch_residual<T>(c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur], c->N, c->n_int,
-                            c->d_last, c->d_partials, c->n_partials, c->d_res, c->stream));
+      CK(launch_residual<T>(c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur], c->d_vel, c->N,
+                            c->n_int, c->d_last, c->d_partials, c->n_partials, c->d_res, c->stream));
     return 0;
   });
 }
@@ -847,6 +898,13 @@ int cc_set_stream(cc_ctx *c, void *stream) {
 
 void *cc_get_stream(cc_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
+int cc_set_renormalize(cc_ctx *c, int enable) {
+  if (int r = check_ctx(c)) return r;
+  c->renorm = enable < 0 ? -1 : (enable != 0);
+  destroy_graphs(c);
+  return 0;
+}
+
 int cc_use_graph(cc_ctx *c, int enable) {
   if (int r = check_ctx(c)) return r;
   c->use_graph = enable != 0;
@@ -861,6 +919,44 @@ int cc_info(cc_ctx *c, int64_t *n_points, int64_t *device_bytes, int *n_tiles, i
   if (device_bytes) *device_bytes = c->device_bytes;
   if (n_tiles) *n_tiles = (int)c->htiles.size();
   if (n_halo_levels) *n_halo_levels = (int)c->plan.level_begin.size() - 1;
+  return 0;
+}
+
+int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[4]) {
+  if (int r = check_ctx(c)) return r;
+  if (!c->initialized) return fail(CC_ERR_STATE, "cc_time_kernels before cc_init");
+  if (!out_ms || n_steps < 1) return fail(CC_ERR_ARG, "bad arguments");
+  if (c->state_dirty) {
+    destroy_graphs(c);
+    int r = dispatch(c, [&](auto tt, auto nn) { return derive_state<typename decltype(tt)::type, decltype(nn)::value>(c); });
+    if (r) return r;
+  }
+  c->profiling = true;
+  c->ev_next_stage = c->ev_next_halo = 0;
+  int r = dispatch(c, [&](auto tt, auto nn) -> int {
+    for (int s = 0; s < n_steps; ++s)
+      if (int e = enqueue_step<typename decltype(tt)::type, decltype(nn)::value>(c, scheme)) return e;
+    return 0;
+  });
+  c->profiling = false;
+  if (r) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  double st = 0, ha = 0;
+  for (size_t i = 0; i + 1 < c->ev_next_stage; i += 2) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev_stage[i], c->ev_stage[i + 1]));
+    st += ms;
+  }
+  for (size_t i = 0; i + 1 < c->ev_next_halo; i += 2) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev_halo[i], c->ev_halo[i + 1]));
+    ha += ms;
+  }
+  const double n_launch = (double)(c->ev_next_stage / 2);
+  out_ms[0] = n_launch > 0 ? st / n_launch : 0;
+  out_ms[1] = n_launch > 0 ? ha / n_launch : 0;
+  out_ms[2] = n_launch;
+  out_ms[3] = (st + ha) / n_steps;
   return 0;
 }
 

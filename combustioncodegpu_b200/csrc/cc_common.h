@@ -1,6 +1,7 @@
 // Shared host/device definitions of the sm_100a residual path.
 #pragma once
 #include <cstdint>
+#include <cstddef>
 
 namespace ccb {
 
@@ -99,6 +100,8 @@ struct StageArgs {
   const double *dt;          // global time step
   unsigned long long *dt_next;  // next global time step (atomicMin), or null
   unsigned *status;
+  double *vel;               // |V| of the updated points (DZone::vel), or null
+  const uint32_t *skip_dt;   // bitmask of points the halo rewrites (their dt is reduced there)
   int local_dt;              // 1: per-point time step of the current state
   int renorm_y;              // 1: renormalise Y_k to sum 1
 };
@@ -118,6 +121,7 @@ struct HaloNode {
   int bc;
 };
 
+// src.pad of a copy: bit 0 = dst is an interior point, bit 1 = its block is 3D.
 struct HaloCopy {
   int64_t dst;
   HaloRef src;
@@ -140,6 +144,8 @@ struct HaloArgs {
   const HaloNode *nodes;
   const HaloCopy *copies;
   int64_t begin, end;
+  const T *G;                     // geometry (time step of rewritten interior points)
+  unsigned long long *dt_next;    // next global time step, or null
 };
 
 }  // namespace ccb

@@ -43,6 +43,11 @@ class Replay {
   std::vector<int> inflow_node_;
   std::string err_;
 
+ public:
+  std::vector<int64_t> wall_points_;
+
+ private:
+
   bool in_box(int b, int i, int j, int k) const {
     const HostBlock &h = B_[b];
     return i >= -h.g && i < h.mx + h.g && j >= -h.g && j < h.my + h.g && k >= -h.g && k < h.mz + h.g;
@@ -111,6 +116,7 @@ bool Replay::face_bc(int b, const HostBoundary &f, int c) {
           Val in1;
           if (!get(b, i - dir[0], j - dir[1], k - dir[2], in1)) return false;
           w.push_back({b, i, j, k, node(kHaloWallFace, in1, in1, c)});
+          if (interior(b, i, j, k)) wall_points_.push_back(pt(b, i, j, k));
           for (int gg = 1; gg <= g; ++gg) {
             Val mir;
             if (!get(b, i - gg * dir[0], j - gg * dir[1], k - gg * dir[2], mir)) return false;
@@ -277,9 +283,27 @@ bool Replay::run(HaloPlan &plan) {
   }
   plan.level_begin.push_back((int64_t)plan.nodes.size());
   if (order.empty()) plan.level_begin.assign(1, 0);
+  std::sort(wall_points_.begin(), wall_points_.end());
+  wall_points_.erase(std::unique(wall_points_.begin(), wall_points_.end()), wall_points_.end());
+  plan.vel_zero = wall_points_;
   plan.copies.clear();
   plan.copies.reserve(changed.size());
-  for (const auto &kv : changed) plan.copies.push_back(HaloCopy{kv.first, to_ref(kv.second)});
+  for (const auto &kv : changed) {
+    HaloCopy hc{kv.first, to_ref(kv.second)};
+    // locate the block of the destination (blocks are contiguous in the arena)
+    int flags = 0;
+    for (size_t b = 0; b < B_.size(); ++b) {
+      const HostBlock &h = B_[b];
+      const int64_t r = kv.first - h.off;
+      if (r < 0 || r >= (int64_t)h.nx * h.ny * h.nz) continue;
+      const int i = (int)(r % h.nx) - h.g, j = (int)((r / h.nx) % h.ny) - h.g, k = (int)(r / ((int64_t)h.nx * h.ny)) - h.g;
+      if (interior((int)b, i, j, k)) flags |= 1;
+      if (h.mz > 1) flags |= 2;
+      break;
+    }
+    hc.src.pad = flags;
+    plan.copies.push_back(hc);
+  }
   return true;
 }
 

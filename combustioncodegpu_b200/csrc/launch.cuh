@@ -33,18 +33,19 @@ cudaError_t Launch<T, NS>::halo_nodes(const HaloArgs<T> &a, const ChemParams &C,
 }
 
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::halo_copies(const HaloArgs<T> &a, int np, int npr, int nq, cudaStream_t s) {
+cudaError_t Launch<T, NS>::halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s) {
   const int64_t n = a.end - a.begin;
   if (n <= 0) return cudaSuccess;
   const int tpb = 256;
-  k_halo_copies<T><<<(unsigned)((n + tpb - 1) / tpb), tpb, 0, s>>>(a, np, npr, nq);
+  k_halo_copies<T, NS><<<(unsigned)((n + tpb - 1) / tpb), tpb, 0, s>>>(a, C);
   return cudaGetLastError();
 }
 
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, cudaStream_t s) {
+cudaError_t Launch<T, NS>::cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, double *vel,
+                                      cudaStream_t s) {
   const int tpb = 256;
-  k_cv_from_bv<NS><<<(unsigned)((N + tpb - 1) / tpb), tpb, 0, s>>>(C, P0, Q, N);
+  k_cv_from_bv<NS><<<(unsigned)((N + tpb - 1) / tpb), tpb, 0, s>>>(C, P0, Q, N, vel);
   return cudaGetLastError();
 }
 

@@ -14,8 +14,9 @@ struct Launch {
   static cudaError_t configure();  // kernel attributes; call outside stream capture
   static cudaError_t stage(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s);
   static cudaError_t halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
-  static cudaError_t halo_copies(const HaloArgs<T> &a, int np, int npr, int nq, cudaStream_t s);
-  static cudaError_t cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, cudaStream_t s);
+  static cudaError_t halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
+  static cudaError_t cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, double *vel,
+                                cudaStream_t s);
   static cudaError_t props_all(const ChemParams &C, const T *P, T *Pr, int64_t N, cudaStream_t s);
   static cudaError_t dt_reduce(const ChemParams &C, const BlockInfo *blocks, int nblocks, const T *P, const T *Pr,
                                const T *G, int64_t N, int64_t n_interior, unsigned long long *dt_out,
@@ -36,11 +37,13 @@ cudaError_t launch_convert_d2f(const double *src, float *dst, int64_t n, cudaStr
 cudaError_t launch_convert_f2d(const float *src, double *dst, int64_t n, cudaStream_t s);
 cudaError_t launch_dt_finalize(double *dt, unsigned long long *dt_next, unsigned *status, double *dt_hist,
                                cudaStream_t s);
+cudaError_t launch_zero_points(double *field, const int64_t *points, int64_t n, cudaStream_t s);
 template <typename T>
-cudaError_t launch_store_last(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_interior,
-                              double *bv_last, cudaStream_t s);
+cudaError_t launch_store_last(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
+                              int64_t n_interior, double *bv_last, cudaStream_t s);
 template <typename T>
-cudaError_t launch_residual(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_interior,
-                            const double *bv_last, double *partials, int n_partials, double *res, cudaStream_t s);
+cudaError_t launch_residual(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
+                            int64_t n_interior, const double *bv_last, double *partials, int n_partials, double *res,
+                            cudaStream_t s);
 
 }  // namespace ccb

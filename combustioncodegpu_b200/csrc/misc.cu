@@ -67,16 +67,28 @@ __device__ __forceinline__ int64_t interior_point(const BlockInfo *blocks, int n
   return B.base + i + (int64_t)B.nx * j + (int64_t)B.nx * B.ny * k;
 }
 
-// store_last_step: (rho, |V|, p, T) of every interior point.
+__global__ void k_zero_points(double *field, const int64_t *points, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) field[points[i]] = 0.0;
+}
+
+cudaError_t launch_zero_points(double *field, const int64_t *points, int64_t n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_zero_points<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(field, points, n);
+  return cudaGetLastError();
+}
+
+// store_last_step: (rho, |V|, p, T) of every interior point; |V| is DZone::vel
+// (written by the update, zeroed by wall conditions, untouched by interface
+// exchanges; TimeAdvanceFunc.cu:13-24).
 template <typename T>
-__global__ void k_store_last(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_int,
-                             double *last) {
+__global__ void k_store_last(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
+                             int64_t n_int, double *last) {
   const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (g >= n_int) return;
   const int64_t p = interior_point(blocks, nblocks, g);
-  const double u = P[N + p], v = P[2 * N + p], w = P[3 * N + p];
   last[g] = P[p];
-  last[n_int + g] = sqrt(u * u + v * v + w * w);
+  last[n_int + g] = vel[p];
   last[2 * n_int + g] = P[4 * N + p];
   last[3 * n_int + g] = P[5 * N + p];
 }
@@ -84,14 +96,13 @@ __global__ void k_store_last(const BlockInfo *blocks, int nblocks, const T *P, i
 // compute_square_of_dbv + per-CTA sums (fixed order), then one CTA sums the
 // partials in fixed order: the result does not depend on scheduling.
 template <typename T>
-__global__ void k_residual_partial(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_int,
-                                   const double *last, double *partials) {
+__global__ void k_residual_partial(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
+                                   int64_t n_int, const double *last, double *partials) {
   double acc[4] = {0, 0, 0, 0};
   for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_int; g += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = interior_point(blocks, nblocks, g);
-    const double u = P[N + p], v = P[2 * N + p], w = P[3 * N + p];
     const double d0 = (double)P[p] - last[g];
-    const double d1 = sqrt(u * u + v * v + w * w) - last[n_int + g];
+    const double d1 = vel[p] - last[n_int + g];
     const double d2 = (double)P[4 * N + p] - last[2 * n_int + g];
     const double d3 = (double)P[5 * N + p] - last[3 * n_int + g];
     acc[0] += d0 * d0, acc[1] += d1 * d1, acc[2] += d2 * d2, acc[3] += d3 * d3;
@@ -117,27 +128,29 @@ __global__ void k_residual_final(const double *partials, int n_partials, int64_t
 }
 
 template <typename T>
-cudaError_t launch_store_last(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_interior,
-                              double *bv_last, cudaStream_t s) {
-  k_store_last<T><<<(unsigned)((n_interior + 255) / 256), 256, 0, s>>>(blocks, nblocks, P, N, n_interior, bv_last);
+cudaError_t launch_store_last(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
+                              int64_t n_interior, double *bv_last, cudaStream_t s) {
+  k_store_last<T><<<(unsigned)((n_interior + 255) / 256), 256, 0, s>>>(blocks, nblocks, P, vel, N, n_interior,
+                                                                        bv_last);
   return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_residual(const BlockInfo *blocks, int nblocks, const T *P, int64_t N, int64_t n_interior,
-                            const double *bv_last, double *partials, int n_partials, double *res, cudaStream_t s) {
-  k_residual_partial<T><<<n_partials, 256, 0, s>>>(blocks, nblocks, P, N, n_interior, bv_last, partials);
+cudaError_t launch_residual(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
+                            int64_t n_interior, const double *bv_last, double *partials, int n_partials, double *res,
+                            cudaStream_t s) {
+  k_residual_partial<T><<<n_partials, 256, 0, s>>>(blocks, nblocks, P, vel, N, n_interior, bv_last, partials);
   k_residual_final<<<1, 32, 0, s>>>(partials, n_partials, n_interior, res);
   return cudaGetLastError();
 }
 
-template cudaError_t launch_store_last<double>(const BlockInfo *, int, const double *, int64_t, int64_t, double *,
-                                               cudaStream_t);
-template cudaError_t launch_store_last<float>(const BlockInfo *, int, const float *, int64_t, int64_t, double *,
-                                              cudaStream_t);
-template cudaError_t launch_residual<double>(const BlockInfo *, int, const double *, int64_t, int64_t,
-                                             const double *, double *, int, double *, cudaStream_t);
-template cudaError_t launch_residual<float>(const BlockInfo *, int, const float *, int64_t, int64_t, const double *,
-                                            double *, int, double *, cudaStream_t);
+template cudaError_t launch_store_last<double>(const BlockInfo *, int, const double *, const double *, int64_t,
+                                               int64_t, double *, cudaStream_t);
+template cudaError_t launch_store_last<float>(const BlockInfo *, int, const float *, const double *, int64_t,
+                                              int64_t, double *, cudaStream_t);
+template cudaError_t launch_residual<double>(const BlockInfo *, int, const double *, const double *, int64_t,
+                                             int64_t, const double *, double *, int, double *, cudaStream_t);
+template cudaError_t launch_residual<float>(const BlockInfo *, int, const float *, const double *, int64_t, int64_t,
+                                            const double *, double *, int, double *, cudaStream_t);
 
 }  // namespace ccb

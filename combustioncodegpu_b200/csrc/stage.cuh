@@ -336,6 +336,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
         pres = rho * temp * gas_const;
       }
       if (!(rho > 0) || !(pres > 0) || !(temp > 0) || !isfinite(q[4])) flags |= kStatusNonFinite;
+      if (a.vel) a.vel[p] = sqrt(vel2);
       T* Pn = a.Pn;
       Pn[p] = T(rho);
       Pn[N + p] = T(u);
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
 #pragma unroll
       for (int l = 0; l < A; ++l)
         if (l < ns) Prn[(2 + l) * N + p] = rd[l];
-      if (a.dt_next) {
+      if (a.dt_next && !((a.skip_dt[p >> 5] >> (p & 31)) & 1u)) {
         const double dtl = local_time_step<T>(C, G, N, p, rho, u, v, w, (double)c, (double)gam, (double)mu, three_d);
         dt_min = fmin(dt_min, dtl);
       }
@@ -530,23 +531,48 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
   }
 }
 
-// Phase B: write every changed point from its resolved source.
-template <typename T>
-__global__ void k_halo_copies(const HaloArgs<T> a, int np, int npr, int nq) {
+// Phase B: write every changed point from its resolved source.  Interior
+// points rewritten here (coincident interface layers) contribute their
+// post-exchange local time step to the next global step, as the reference
+// evaluates the step after the exchange (Driver.cu:150-163).
+template <typename T, int NS>
+__global__ void k_halo_copies(const HaloArgs<T> a, const __grid_constant__ ChemParams C) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  const int np = 6 + ns, npr = 2 + ns, nq = 5 + ns;
   const int64_t e = a.begin + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (e >= a.end) return;
-  const HaloCopy c = a.copies[e];
-  const RefPtrs<T> r = resolve(a, c.src);
-  for (int f = 0; f < np; ++f) a.P[f * a.N + c.dst] = r.P[f * r.stride + r.idx];
-  for (int f = 0; f < npr; ++f) a.Pr[f * a.N + c.dst] = r.Pr[f * r.stride + r.idx];
-  for (int f = 0; f < nq; ++f) a.Q[f * a.N + c.dst] = r.Q[f * r.stride + r.idx];
+  double dt_min = 1e300;
+  if (e < a.end) {
+    const HaloCopy c = a.copies[e];
+    const RefPtrs<T> r = resolve(a, c.src);
+    for (int f = 0; f < np; ++f) a.P[f * a.N + c.dst] = r.P[f * r.stride + r.idx];
+    for (int f = 0; f < npr; ++f) a.Pr[f * a.N + c.dst] = r.Pr[f * r.stride + r.idx];
+    for (int f = 0; f < nq; ++f) a.Q[f * a.N + c.dst] = r.Q[f * r.stride + r.idx];
+    if (a.dt_next && (c.src.pad & 1)) {
+      const int64_t p = c.dst, N = a.N;
+      T Y[A], gam, cs;
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) Y[l] = a.P[(6 + l) * N + p];
+      gamma_and_c<T, NS>(C, a.P[5 * N + p], Y, gam, cs);
+      dt_min = local_time_step<T>(C, a.G, N, p, (double)a.P[p], (double)a.P[N + p], (double)a.P[2 * N + p],
+                                  (double)a.P[3 * N + p], (double)cs, (double)gam, (double)a.Pr[p],
+                                  (c.src.pad & 2) != 0);
+    }
+  }
+  if (a.dt_next) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dt_min = fmin(dt_min, __shfl_xor_sync(0xffffffffu, dt_min, o));
+    if ((threadIdx.x & 31) == 0) atomic_min_pos_double(a.dt_next, dt_min);
+  }
 }
 
 // ------------------------------------------------------------ setup / misc
 
 // Field.cu:150-176 compute_cv_from_bv over every arena point (FP64 input).
 template <int NS>
-__global__ void k_cv_from_bv(const __grid_constant__ ChemParams C, const double *P0, double *Q, int64_t N) {
+__global__ void k_cv_from_bv(const __grid_constant__ ChemParams C, const double *P0, double *Q, int64_t N,
+                             double *vel) {
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -562,6 +588,7 @@ __global__ void k_cv_from_bv(const __grid_constant__ ChemParams C, const double 
   Q[2 * N + p] = rho * v;
   Q[3 * N + p] = rho * w;
   Q[4 * N + p] = total_energy<NS>(C, rho, u, v, w, pr, t, Y);
+  if (vel) vel[p] = sqrt(u * u + v * v + w * w);
 #pragma unroll
   for (int l = 0; l < A; ++l)
     if (l < ns) Q[(5 + l) * N + p] = rho * Y[l];

@@ -156,10 +156,19 @@ int cc_status(cc_ctx *ctx, unsigned *flags);
 /* Stream used by every launch of the context (default: a private stream). */
 int cc_set_stream(cc_ctx *ctx, void *cuda_stream);
 void *cc_get_stream(cc_ctx *ctx);
+/* Renormalise the mass fractions to sum 1 after every update (FP64):
+ * 1 on, 0 off, -1 default (on for CC_MIXED, off for CC_FP64, which keeps the
+ * reference's update, TimeAdvanceFunc.cu:273-276, unchanged). */
+int cc_set_renormalize(cc_ctx *ctx, int enable);
 /* 1 = replay whole steps from a captured CUDA graph (default), 0 = launch. */
 int cc_use_graph(cc_ctx *ctx, int enable);
 /* Points updated per stage (sum of mx*my*mz) and arena bytes on the device. */
 int cc_info(cc_ctx *ctx, int64_t *n_points, int64_t *device_bytes, int *n_tiles, int *n_halo_levels);
+/* Runs n_steps steps without graph replay, timing every stage-kernel launch
+ * and every halo program with CUDA events on the context's stream:
+ * out_ms = {mean stage-kernel ms per launch, mean halo ms per stage,
+ *           number of stage launches, mean stage+halo ms per step}. */
+int cc_time_kernels(cc_ctx *ctx, int n_steps, int scheme, double out_ms[4]);
 /* Synchronises the context's stream. */
 int cc_sync(cc_ctx *ctx);
 

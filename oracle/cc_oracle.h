@@ -89,8 +89,8 @@ int oc_set_state(oc_solver *s, int blk, const double *bv, const double *yk);
 
 int oc_init(oc_solver *s);
 /* One pass of the reference's steady explicit-Euler loop body with the
- * per-point local time step (Driver.cu:189-244). */
-int oc_steady_step(oc_solver *s);
+ * per-point local time step (Driver.cu:189-244); renorm_y as for RK3. */
+int oc_steady_step(oc_solver *s, int renorm_y);
 /* One SSP-RK3 step with a global time step; renorm_y renormalises the
  * mass fractions to sum 1 after each stage. */
 int oc_rk3_step(oc_solver *s, int renorm_y);
@@ -106,6 +106,16 @@ double oc_last_dt(const oc_solver *s);
  * change of (rho,|V|,p,T) over the last step, before the res_scale division. */
 int oc_residual(const oc_solver *s, double out[4]);
 int oc_newton_failures(const oc_solver *s);
+
+/* Known-answer hooks: the face, thermo, transport and Newton routines of the
+ * restatement on single inputs, and the boundary/interface fill alone. */
+double oc_kat_minmod(double a, double b);
+void oc_kat_face_inviscid(const oc_params *p, const double *pv4, const double ml[3], double jl, const double mr[3],
+                          double jr, double *fc);
+void oc_kat_h_cp(const oc_params *p, double t, double *h, double *cp);
+void oc_kat_transport(const oc_params *p, double t, const double *Y, double *mu, double *lam, double *rhod);
+double oc_kat_temperature(const oc_params *p, const double *q5, const double *Y, double t0);
+int oc_apply_boundaries(oc_solver *s);
 
 #ifdef __cplusplus
 }

@@ -76,8 +76,8 @@ def lib():
         L.oc_add_bc.argtypes = [ctypes.c_void_p, ctypes.POINTER(OcBc)]
         L.oc_set_geometry.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.oc_set_state.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
-        for name in ("oc_init", "oc_steady_step"):
-            getattr(L, name).argtypes = [ctypes.c_void_p]
+        L.oc_init.argtypes = [ctypes.c_void_p]
+        L.oc_steady_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oc_rk3_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oc_compute_dq.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.oc_get_state.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
@@ -160,9 +160,9 @@ class Oracle:
     def init(self):
         lib().oc_init(self.s)
 
-    def steady_step(self, n=1):
+    def steady_step(self, n=1, renorm_y=False):
         for _ in range(n):
-            lib().oc_steady_step(self.s)
+            lib().oc_steady_step(self.s, 1 if renorm_y else 0)
 
     def rk3_step(self, n=1, renorm_y=False):
         for _ in range(n):
@@ -236,3 +236,78 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def make_params(species, reconstruction=2, viscous_order=2, Pr=0.72, cfl=0.5, Sc=0.9):
+    """OcParams for the known-answer hooks; returns (struct, keepalive)."""
+    p = OcParams()
+    p.n_spec = 0 if species is None else int(species["n_spec"])
+    p.reconstruction, p.limiter, p.viscous_order, p.ngg = reconstruction, 0, viscous_order, 2
+    p.Pr, p.cfl, p.Sc = Pr, cfl, Sc
+    keep = []
+    if p.n_spec:
+        for fld, key in (("mw", "mw"), ("t_low", "t_low"), ("t_mid", "t_mid"), ("t_high", "t_high"),
+                         ("low_coeff", "low_temp_coeff"), ("high_coeff", "high_temp_coeff"),
+                         ("LJ_potent_inv", "LJ_potent_inv"), ("vis_coeff", "vis_coeff"),
+                         ("WjDivWi_to_One4th", "WjDivWi_to_One4th"), ("sqrt_WiDivWjPl1Mul8", "sqrt_WiDivWjPl1Mul8")):
+            a = np.ascontiguousarray(species[key], dtype=np.float64).ravel()
+            keep.append(a)
+            setattr(p, fld, _p(a))
+    return p, keep
+
+
+def kat_minmod(a, b):
+    L = lib()
+    L.oc_kat_minmod.restype = ctypes.c_double
+    L.oc_kat_minmod.argtypes = [ctypes.c_double, ctypes.c_double]
+    return L.oc_kat_minmod(a, b)
+
+
+def kat_face_inviscid(species, pv4, k, reconstruction=2):
+    """AUSM+ face flux from 4 points of primitives (rho,u,v,w,p,Y...) and a
+    face normal k (metric row times J, equal on both sides)."""
+    p, keep = make_params(species, reconstruction)
+    pv = np.ascontiguousarray(pv4, dtype=np.float64)
+    m = np.ascontiguousarray(k, dtype=np.float64)
+    fc = np.zeros(5 + p.n_spec)
+    L = lib()
+    L.oc_kat_face_inviscid.argtypes = [ctypes.POINTER(OcParams), _dp, _dp, ctypes.c_double, _dp, ctypes.c_double, _dp]
+    L.oc_kat_face_inviscid(ctypes.byref(p), _p(pv), _p(m), 1.0, _p(m), 1.0, _p(fc))
+    return fc
+
+
+def kat_h_cp(species, T):
+    p, keep = make_params(species)
+    h, cp = np.zeros(p.n_spec), np.zeros(p.n_spec)
+    L = lib()
+    L.oc_kat_h_cp.argtypes = [ctypes.POINTER(OcParams), ctypes.c_double, _dp, _dp]
+    L.oc_kat_h_cp(ctypes.byref(p), float(T), _p(h), _p(cp))
+    return h, cp
+
+
+def kat_transport(species, T, Y, Sc=0.9):
+    p, keep = make_params(species, Sc=Sc)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    mu, lam = ctypes.c_double(), ctypes.c_double()
+    rd = np.zeros(p.n_spec)
+    L = lib()
+    L.oc_kat_transport.argtypes = [ctypes.POINTER(OcParams), ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double), _dp]
+    L.oc_kat_transport(ctypes.byref(p), float(T), _p(Y), ctypes.byref(mu), ctypes.byref(lam), _p(rd))
+    return mu.value, lam.value, rd
+
+
+def kat_temperature(species, q5, Y, t0):
+    p, keep = make_params(species)
+    q = np.ascontiguousarray(q5, dtype=np.float64)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    L = lib()
+    L.oc_kat_temperature.restype = ctypes.c_double
+    L.oc_kat_temperature.argtypes = [ctypes.POINTER(OcParams), _dp, _dp, ctypes.c_double]
+    return L.oc_kat_temperature(ctypes.byref(p), _p(q), _p(Y), float(t0))
+
+
+def apply_boundaries(oracle):
+    L = lib()
+    L.oc_apply_boundaries.argtypes = [ctypes.c_void_p]
+    return L.oc_apply_boundaries(oracle.s)

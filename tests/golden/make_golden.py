@@ -95,6 +95,56 @@ def write_case(path, case):
                 f.write(np.ascontiguousarray(b[key], dtype="<f8").tobytes())
 
 
+def read_case(path):
+    """Inverse of write_case: the case dict exactly as the harness read it."""
+    data = open(path, "rb").read()
+    assert data[:8] == b"CCCASE01", path
+    pos = 8
+
+    def take(fmt, n):
+        nonlocal pos
+        v = np.frombuffer(data, fmt, n, pos).copy()
+        pos += v.itemsize * n
+        return v
+
+    ns, nb, ngg, visc, rec, lim, n_steps, n_bc = (int(v) for v in take("<i4", 8))
+    Pr, cfl, Sc = (float(v) for v in take("<f8", 3))
+    prm = {"inviscid_scheme": 3, "reconstruction": rec, "limiter": lim, "viscous_order": visc, "ngg": ngg,
+           "cfl": cfl, "prandtl_number": Pr, "schmidt_number": Sc, "species": None}
+    if ns:
+        sp = {"n_spec": ns}
+        for key, n in (("mw", ns), ("t_low", ns), ("t_mid", ns), ("t_high", ns), ("low_temp_coeff", 7 * ns),
+                       ("high_temp_coeff", 7 * ns), ("LJ_potent_inv", ns), ("vis_coeff", ns),
+                       ("WjDivWi_to_One4th", ns * ns), ("sqrt_WiDivWjPl1Mul8", ns * ns)):
+            sp[key] = take("<f8", n)
+        for key in ("low_temp_coeff", "high_temp_coeff"):
+            sp[key] = sp[key].reshape(ns, 7)
+        for key in ("WjDivWi_to_One4th", "sqrt_WiDivWjPl1Mul8"):
+            sp[key] = sp[key].reshape(ns, ns)
+        prm["species"] = sp
+    bcs = []
+    for _ in range(n_bc):
+        label, kind, tt, _pad = (int(v) for v in take("<i4", 4))
+        t_wall, rho, u, v, w, p, T = (float(x) for x in take("<f8", 7))
+        yk = take("<f8", ns)
+        bcs.append({"label": label, "kind": kind, "thermal_type": tt, "t_wall": t_wall, "density": rho, "u": u,
+                    "v": v, "w": w, "pressure": p, "temperature": T, "yk": yk})
+    blocks = []
+    for _ in range(nb):
+        mx, my, mz, n_bnd, n_in = (int(v) for v in take("<i4", 5))
+        bnd = [list(map(int, take("<i4", 7))) for _ in range(n_bnd)]
+        inf = [list(map(int, take("<i4", 13))) for _ in range(n_in)]
+        ng = (mx + 2 * ngg) * (my + 2 * ngg) * (mz + 2 * ngg)
+        jac = take("<f8", ng)
+        met = take("<f8", 9 * ng).reshape(9, ng)
+        bv = take("<f8", 6 * ng).reshape(6, ng)
+        yk = take("<f8", ns * ng).reshape(ns, ng)
+        blocks.append({"dims": (mx, my, mz), "boundaries": bnd, "inner_faces": inf, "jac": jac, "metric": met,
+                       "bv": bv, "yk": yk})
+    assert pos == len(data)
+    return {"params": prm, "bcs": bcs, "blocks": blocks, "n_steps": n_steps}
+
+
 def read_output(path, case):
     sp = case["params"].get("species")
     ns = 0 if sp is None else int(sp["n_spec"])
@@ -213,9 +263,11 @@ def main():
             write_case(os.path.join(d, "%s.%s.bin" % (name, "ms" if ms else "air")), c)
         print("wrote", sorted(os.listdir(d)))
     elif cmd == "pack":
-        for name, c in cs.items():
-            ms = c["params"].get("species") is not None
-            ref = read_output(os.path.join(d, "%s.%s.bin.out" % (name, "ms" if ms else "air")), c)
+        for name, c0 in cs.items():
+            ms = c0["params"].get("species") is not None
+            fn = os.path.join(d, "%s.%s.bin" % (name, "ms" if ms else "air"))
+            c = read_case(fn)
+            ref = read_output(fn + ".out", c)
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **pack(c, ref))
             print("packed", name)
 

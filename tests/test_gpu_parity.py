@@ -1,0 +1,166 @@
+"""CUDA path (through the C ABI) against the CPU oracle and against the
+reference's own kernels (golden fixtures).
+
+Tolerances: FP64 plain path vs the FP64 oracle 1e-10 relative per field
+group after a few steps (rounding only: FMA contraction and evaluation order
+differ); mixed path (FP32 fluxes/transport, FP64 conserved variables and
+Newton) vs the FP64 oracle 1e-4 after two steps (the long-run L2 bound of
+1e-5 after 1000 steps is measured by bench.py)."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import combustioncodegpu_b200 as cc
+from combustioncodegpu_b200 import cases
+from oracle.oracle_py import Oracle
+
+sys.path.insert(0, os.path.dirname(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+from gpu_compare import bv_groups, cv_groups, group_errors, interior  # noqa: E402
+import make_golden as mg  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    sp = cases.synthetic_species()
+    return {
+        "sod": cases.case_sod(40, 6, 6),
+        "box": cases.case_box(12, species=sp, seed=3),
+        "channel": cases.case_channel((11, 8, 6), species=sp),
+        "multiblock": cases.case_multiblock(([6, 7], [6, 5], [5]), species=sp),
+        "air_visc": mg.load("air_visc_o1")[0],
+    }
+
+
+CASES = _cases()
+
+
+def compare(case, scheme, n, precision):
+    renorm = precision == "mixed" and case["params"].get("species") is not None
+    o = Oracle(case)
+    o.init()
+    d = cc.Driver.from_case(case, precision)
+    d.initialize_computation()
+    if scheme == "rk3":
+        o.rk3_step(n, renorm_y=renorm)
+    else:
+        o.steady_step(n, renorm_y=renorm)
+    d.simulate(n, scheme, residual=True)
+    errs = {}
+    ns = o.ns
+    for b, blk in enumerate(case["blocks"]):
+        bv, yk, cv = d.field[b].get_state()
+        obv, oyk, ocv = o.state(b)
+        for k, v in group_errors(bv, obv, bv_groups()).items():
+            errs["bv." + k] = max(errs.get("bv." + k, 0.0), v)
+        for k, v in group_errors(cv, ocv, cv_groups(ns)).items():
+            errs["cv." + k] = max(errs.get("cv." + k, 0.0), v)
+        if ns:
+            errs["yk"] = max(errs.get("yk", 0.0), float(np.abs(yk - oyk).max()))
+        mul, cond, rd = d.field[b].get_props()
+        omul, ocond, ord_ = o.props(b)
+        errs["mul"] = max(errs.get("mul", 0.0), float(np.abs(mul - omul).max() / np.abs(omul).max()))
+        errs["cond"] = max(errs.get("cond", 0.0), float(np.abs(cond - ocond).max() / np.abs(ocond).max()))
+    res, ores = d.residual(), o.residual()
+    errs["res"] = float(np.max(np.abs(res - ores) / np.maximum(np.abs(ores), 1e-300)))
+    if scheme == "rk3":
+        errs["dt"] = abs(d.last_dt() - o.last_dt()) / o.last_dt()
+    status = d.status()
+    d.close()
+    return errs, status
+
+
+@pytest.mark.parametrize("scheme", ["steady", "rk3"])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp64_matches_oracle(name, scheme):
+    errs, status = compare(CASES[name], scheme, 2, "fp64")
+    assert status == 0
+    bad = {k: v for k, v in errs.items() if not v < 1e-10}
+    assert not bad, errs
+
+
+@pytest.mark.parametrize("scheme", ["steady", "rk3"])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_mixed_close_to_oracle(name, scheme):
+    errs, status = compare(CASES[name], scheme, 2, "mixed")
+    assert status == 0
+    tol = {"res": 5e-3, "dt": 1e-5}
+    bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-4)}
+    assert not bad, errs
+
+
+@pytest.mark.parametrize("name", mg.NAMES)
+def test_fp64_matches_reference_kernels(name):
+    """Steady explicit-Euler loop on the golden inputs vs the reference's own
+    kernels' outputs (state, transport properties, residual)."""
+    case, ref = mg.load(name)
+    d = cc.Driver.from_case(case, "fp64")
+    d.initialize_computation()
+    d.simulate(case["n_steps"], "steady", residual=True)
+    ns = 0 if case["params"]["species"] is None else case["params"]["species"]["n_spec"]
+    for b in range(len(case["blocks"])):
+        bv, yk, cv = d.field[b].get_state()
+        for k, v in group_errors(bv, ref["b%d_bv" % b], bv_groups()).items():
+            assert v < 1e-10, (k, v)
+        for k, v in group_errors(cv, ref["b%d_cv" % b], cv_groups(ns)).items():
+            assert v < 1e-10, (k, v)
+        mul, cond, rd = d.field[b].get_props()
+        assert np.abs(mul - ref["b%d_mul" % b]).max() < 1e-10 * np.abs(ref["b%d_mul" % b]).max()
+        if ns:
+            assert np.abs(yk - ref["b%d_yk" % b]).max() < 1e-10
+    np.testing.assert_allclose(d.residual(), ref["residual"], rtol=1e-8)
+    d.close()
+
+
+def test_graph_replay_equals_launches():
+    case = CASES["box"]
+    out = []
+    for graph in (True, False):
+        d = cc.Driver.from_case(case, "mixed")
+        d.use_graph(graph)
+        d.initialize_computation()
+        d.simulate(3)
+        out.append(d.field[0].get_state()[2])
+        d.close()
+    assert np.array_equal(out[0], out[1])
+
+
+def test_status_flags_nonfinite_state():
+    """A non-physical point (negative pressure) is reported through the
+    status word; the context stays usable."""
+    case = cases.case_box(10, species=cases.synthetic_species(), seed=4)
+    bv = case["blocks"][0]["bv"].copy()
+    ng = bv.shape[1]
+    bv[4, ng // 2] = -1.0e5
+    case["blocks"][0]["bv"] = bv
+    d = cc.Driver.from_case(case, "fp64")
+    d.initialize_computation()
+    d.simulate(1)
+    assert d.status() & 2
+    assert d.status() == 0  # cleared by the read
+    d.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_full_size_conservation_and_mass_fractions(precision):
+    """128^3 periodic box: conserved totals over the unique points are kept
+    (flux form) and the mass fractions stay normalised."""
+    n = 128
+    case = cases.case_box(n, species=cases.synthetic_species(), seed=1234)
+    d = cc.Driver.from_case(case, precision)
+    d.initialize_computation()
+    sl = (slice(None), slice(2, -3), slice(2, -3), slice(2, -3))
+    cv0 = d.field[0].get_state()[2].reshape(14, n + 4, n + 4, n + 4)[sl].sum(axis=(1, 2, 3))
+    d.simulate(5)
+    bv, yk, cv = d.field[0].get_state()
+    cv1 = cv.reshape(14, n + 4, n + 4, n + 4)[sl].sum(axis=(1, 2, 3))
+    scale = np.abs(cv0).max()
+    assert np.abs(cv1 - cv0).max() < 1e-12 * scale
+    ysum = interior(yk, (n, n, n)).sum(axis=0)
+    assert np.abs(ysum - 1).max() < (1e-12 if precision == "fp64" else 5e-6)
+    assert np.isfinite(bv).all()
+    assert d.status() == 0
+    d.close()
