@@ -162,7 +162,7 @@ def run_ours(args, rank, world, dist):
             ms = float(t.item())
         kt = d.time_kernels(2)
         out[prec] = {"ms_total": ms, "ms_per_step": ms / args.steps, "npts": npts, "clocks": clk.summary(),
-                     "kernels": kt, "info": info, "status": d.status()}
+                     "kernels": kt, "info": info, "status": d.status(), "tuning": d.tuning()}
         d.close()
     # mixed vs FP64 error after err_steps steps from the same state
     errs = {}
@@ -312,6 +312,7 @@ def main():
         "gpu_launches": launches_per_step * args.steps,
         "clocks": mixed["clocks"],
         "status": {"mixed": mixed["status"], "fp64": plain["status"]},
+        "autotune": {"mixed": mixed["tuning"], "fp64": plain["tuning"]},
     }
     print(json.dumps(line), flush=True)
     if dist:

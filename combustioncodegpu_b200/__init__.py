@@ -95,6 +95,7 @@ EXPORTS = {
     "cc_info": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "cc_time_kernels": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp], ctypes.c_int),
+    "cc_tuning": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
     "cc_sync": ([ctypes.c_void_p], ctypes.c_int),
 }
 
@@ -380,6 +381,12 @@ class Driver:
         n, nb, nt, nl = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int(), ctypes.c_int()
         _check(self.lib.cc_info(self.ctx, ctypes.byref(n), ctypes.byref(nb), ctypes.byref(nt), ctypes.byref(nl)))
         return {"n_points": n.value, "device_bytes": nb.value, "n_tiles": nt.value, "halo_levels": nl.value}
+
+    def tuning(self):
+        """Stage-kernel configuration chosen by the autotuner."""
+        tma, kz, ms = ctypes.c_int(), ctypes.c_int(), np.zeros(1)
+        _check(self.lib.cc_tuning(self.ctx, ctypes.byref(tma), ctypes.byref(kz), _ptr(ms)))
+        return {"tma": bool(tma.value), "kz": kz.value, "stage_ms": float(ms[0])}
 
     def close(self):
         if getattr(self, "ctx", None):

@@ -4,6 +4,7 @@
 // halo program, the tile list of the stage kernel and one captured CUDA graph
 // per (time scheme, parity of the ping-pong buffers).  Everything up to
 // cc_init is host-only, so set-up errors surface without a device.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -95,6 +96,11 @@ struct cc_ctx {
   int64_t *d_vel_zero = nullptr;  // wall-face points (vel = 0 after the wall condition)
   uint32_t *d_skip_dt = nullptr;  // bitmask: interior points the halo rewrites
   int renorm = -1;                // Y renormalisation: -1 = by precision (mixed on, FP64 off)
+  bool use_tma = false;           // TMA-staged stage kernel (mixed precision, 0 or 9 species)
+  bool tma_ok = false;            // tensor maps built (the TMA variant can run)
+  int kz = 1;                     // k-chunk of the stage tiles
+  double tuned_ms = 0;            // stage-kernel time of the chosen configuration
+  CUtensorMap *d_tmaps = nullptr; // [2][n_blocks]: primitive arenas P[0], P[1] per block
   int n_partials = 296;
 
   cudaStream_t stream = nullptr;
@@ -208,40 +214,46 @@ int from64(cc_ctx *c, const double *src, void *dst, int64_t count) {
 }
 
 // Stage-kernel work list: kTX x kTY columns, k split into chunks of kz.
-void build_tiles(cc_ctx *c) {
-  int slots_per_sm = c->precision == CC_FP64 ? 1 : 2;
-  int n_sm = 148;
-  int dev = 0;
+void build_tiles_kz(cc_ctx *c, int kz) {
+  c->htiles.clear();
+  for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
+    const auto &b = c->blocks[bi];
+    for (int k0 = 0; k0 < b.mz; k0 += kz)
+      for (int j0 = 0; j0 < b.my; j0 += kTY)
+        for (int i0 = 0; i0 < b.mx; i0 += kTX) {
+          Tile t{};
+          t.blk = bi, t.i0 = i0, t.j0 = j0, t.k0 = k0, t.k1 = std::min(b.mz, k0 + kz);
+          c->htiles.push_back(t);
+        }
+  }
+  c->kz = kz;
+}
+
+// Initial chunk size (before autotuning): fewest waves times the per-chunk
+// cost (kz planes plus the prologue plane).
+int heuristic_kz(cc_ctx *c) {
+  const int slots_per_sm = c->precision == CC_FP64 ? 1 : 2;
+  int n_sm = 148, dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
   const int slots = n_sm * slots_per_sm;
   int max_mz = 1;
   for (const auto &b : c->blocks) max_mz = std::max(max_mz, b.mz);
   int best_kz = max_mz;
   double best_cost = 1e300;
-  const char *env = std::getenv("CC_KZ");
-  if (env && std::atoi(env) > 0) {
-    best_kz = std::atoi(env);
-  } else {
-    for (int kz = 1; kz <= max_mz; ++kz) {
-      int64_t tiles = 0;
-      for (const auto &b : c->blocks)
-        tiles += (int64_t)((b.mx + kTX - 1) / kTX) * ((b.my + kTY - 1) / kTY) * ((b.mz + kz - 1) / kz);
-      const double waves = std::ceil((double)tiles / slots);
-      const double cost = waves * (kz + 1.0);
-      if (cost < best_cost - 1e-9) best_cost = cost, best_kz = kz;
-    }
+  for (int kz = 1; kz <= max_mz; ++kz) {
+    int64_t tiles = 0;
+    for (const auto &b : c->blocks)
+      tiles += (int64_t)((b.mx + kTX - 1) / kTX) * ((b.my + kTY - 1) / kTY) * ((b.mz + kz - 1) / kz);
+    const double cost = std::ceil((double)tiles / slots) * (kz + 1.0);
+    if (cost < best_cost - 1e-9) best_cost = cost, best_kz = kz;
   }
-  c->htiles.clear();
-  for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
-    const auto &b = c->blocks[bi];
-    for (int k0 = 0; k0 < b.mz; k0 += best_kz)
-      for (int j0 = 0; j0 < b.my; j0 += kTY)
-        for (int i0 = 0; i0 < b.mx; i0 += kTX) {
-          Tile t{};
-          t.blk = bi, t.i0 = i0, t.j0 = j0, t.k0 = k0, t.k1 = std::min(b.mz, k0 + best_kz);
-          c->htiles.push_back(t);
-        }
-  }
+  return best_kz;
+}
+
+int max_tiles(cc_ctx *c) {
+  int64_t n = 0;
+  for (const auto &b : c->blocks) n += (int64_t)((b.mx + kTX - 1) / kTX) * ((b.my + kTY - 1) / kTY) * b.mz;
+  return (int)n;
 }
 
 int upload_bcs(cc_ctx *c) {
@@ -258,12 +270,48 @@ int upload_bcs(cc_ctx *c) {
   return 0;
 }
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// One 4D tensor map (i, j, k, field) per block and primitive arena; box =
+// the tile plane plus its 2-point halo in i and j, all fields.
+int build_tensor_maps(cc_ctx *c) {
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (!fn || q != cudaDriverEntryPointSuccess) return fail(CC_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  auto encode = reinterpret_cast<EncodeTiledFn>(fn);
+  const int nb = (int)c->blocks.size();
+  std::vector<CUtensorMap> maps(2 * (size_t)nb);
+  const size_t E = c->elem;
+  for (int buf = 0; buf < 2; ++buf)
+    for (int b = 0; b < nb; ++b) {
+      const HostBlock &h = c->blocks[b];
+      const cuuint64_t dims[4] = {(cuuint64_t)h.nx, (cuuint64_t)h.ny, (cuuint64_t)h.nz, (cuuint64_t)np_of(c)};
+      const cuuint64_t strides[3] = {(cuuint64_t)h.nx * E, (cuuint64_t)h.nx * h.ny * E, (cuuint64_t)c->N * E};
+      const cuuint32_t box[4] = {(cuuint32_t)(kTX + 4), (cuuint32_t)(kTY + 4), 1u, (cuuint32_t)np_of(c)};
+      const cuuint32_t estr[4] = {1, 1, 1, 1};
+      void *base = (char *)c->P[buf] + (size_t)h.off * E;
+      CUresult r = encode(&maps[(size_t)buf * nb + b],
+                          E == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
+                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return fail(CC_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    }
+  void *p;
+  if (dev_alloc(c, &p, sizeof(CUtensorMap) * maps.size())) return CC_ERR_CUDA;
+  c->d_tmaps = (CUtensorMap *)p;
+  CK(cudaMemcpy(c->d_tmaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
 // Layout, device allocation, halo program, geometry.  Runs once.
 int setup_device(cc_ctx *c) {
   const int ns = c->chem.ns;
   c->elem = c->precision == CC_FP64 ? 8 : 4;
   c->ns_key = ns == 0 ? 0 : (ns == 9 ? 9 : -1);
-  // arena layout: rows padded to 32 points, interior i=0 on a 32-point boundary
+  // arena layout: rows padded to 32 points, every block starts on a 32-point boundary
   int64_t end = 0, n_int = 0;
   c->hblocks.clear();
   for (auto &b : c->blocks) {
@@ -271,7 +319,7 @@ int setup_device(cc_ctx *c) {
     b.nx = ((b.mx + 2 * b.g + 31) / 32) * 32;
     b.ny = b.my + 2 * b.g;
     b.nz = b.mz + 2 * b.g;
-    int64_t off = ((end + b.g + 31) / 32) * 32 - b.g;
+    int64_t off = ((end + 31) / 32) * 32;  // 128-B aligned block start (TMA tensor-map base)
     b.off = off;
     b.base = off + b.g + (int64_t)b.nx * b.g + (int64_t)b.nx * b.ny * b.g;
     end = off + (int64_t)b.nx * b.ny * b.nz;
@@ -283,17 +331,22 @@ int setup_device(cc_ctx *c) {
   }
   c->N = ((end + 31) / 32) * 32;
   c->n_int = n_int;
+  if ((double)c->N * (6 + kMaxSpec) >= 2147483647.0)
+    return fail(CC_ERR_ARG, "grid too large for one context (32-bit field offsets); split it over contexts");
 
   std::vector<HostBc> bcs = c->bcs;
   if (!build_halo_plan(c->blocks, bcs, c->plan)) return fail(CC_ERR_TOPOLOGY, "halo program: " + c->plan.error);
-  build_tiles(c);
+  {
+    const char *env = std::getenv("CC_KZ");
+    build_tiles_kz(c, env && std::atoi(env) > 0 ? std::atoi(env) : heuristic_kz(c));
+  }
 
   const size_t E = c->elem;
   const int64_t N = c->N;
   void *p;
   if (dev_alloc(c, &p, sizeof(BlockInfo) * c->hblocks.size())) return CC_ERR_CUDA;
   c->d_blocks = (BlockInfo *)p;
-  if (dev_alloc(c, &p, sizeof(Tile) * std::max<size_t>(1, c->htiles.size()))) return CC_ERR_CUDA;
+  if (dev_alloc(c, &p, sizeof(Tile) * (size_t)std::max(1, max_tiles(c)))) return CC_ERR_CUDA;
   c->d_tiles = (Tile *)p;
   for (int b = 0; b < 2; ++b) {
     if (dev_alloc(c, &c->P[b], E * N * np_of(c))) return CC_ERR_CUDA;
@@ -302,6 +355,13 @@ int setup_device(cc_ctx *c) {
     c->Q[b] = (double *)p;
   }
   if (dev_alloc(c, &c->G, E * N * 10)) return CC_ERR_CUDA;
+  {
+    const char *no_tma = std::getenv("CC_NO_TMA");
+    c->tma_ok = c->precision == CC_MIXED && (c->ns_key == 0 || c->ns_key == 9) && !(no_tma && no_tma[0] == '1');
+    if (c->tma_ok)
+      if (int r = build_tensor_maps(c)) return r;
+    c->use_tma = false;
+  }
   if (dev_alloc(c, &p, sizeof(double) * N * std::max(np_of(c), 10))) return CC_ERR_CUDA;
   c->stage64 = (double *)p;
   if (dev_alloc(c, &p, sizeof(double) * N)) return CC_ERR_CUDA;
@@ -497,12 +557,82 @@ template <typename T, int NS>
 int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin) {
   const int nt = (int)c->htiles.size();
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
-  CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
+  if (c->use_tma)
+    CK((Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
+  else
+    CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
   if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next)) return r;
   if (a.vel) CK(launch_zero_points(c->d_vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream));
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
+  return 0;
+}
+
+// Times the stage kernel of each candidate (kernel variant x k-chunk) on the
+// actual problem and keeps the fastest.  The candidates write only the
+// scratch halves of the ping-pong buffers, so the state is unchanged.
+template <typename T, int NS>
+int autotune(cc_ctx *c) {
+  const char *env = std::getenv("CC_AUTOTUNE");
+  if (env && env[0] == '0') return 0;
+  StageArgs<T> a{};
+  a.blocks = c->d_blocks;
+  a.tiles = c->d_tiles;
+  a.N = c->N;
+  a.G = (const T *)c->G;
+  a.dt = c->d_dt;
+  a.status = c->d_status;
+  a.skip_dt = c->d_skip_dt;
+  const int pc = c->cur, pn = 1 - c->cur;
+  a.P = (const T *)c->P[pc], a.Pn = (T *)c->P[pn], a.Pr = (const T *)c->Pr[pc], a.Prn = (T *)c->Pr[pn];
+  a.Qin = c->Q[c->qcur], a.Qn = c->Q[c->qcur], a.Qout = c->Q[1 - c->qcur];
+  a.a = 0.0, a.b = 1.0;
+  int max_mz = 1;
+  for (const auto &b : c->blocks) max_mz = std::max(max_mz, b.mz);
+  std::vector<int> kzs;
+  for (int kz : {4, 8, 16, 32, 64, 128})
+    if (kz <= max_mz) kzs.push_back(kz);
+  kzs.push_back(max_mz);
+  kzs.push_back(heuristic_kz(c));
+  std::sort(kzs.begin(), kzs.end());
+  kzs.erase(std::unique(kzs.begin(), kzs.end()), kzs.end());
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double best = 1e300;
+  int best_kz = c->kz;
+  bool best_tma = false;
+  for (int variant = 0; variant < (c->tma_ok ? 2 : 1); ++variant) {
+    for (int kz : kzs) {
+      build_tiles_kz(c, kz);
+      CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
+                         c->stream));
+      const int nt = (int)c->htiles.size();
+      auto launch = [&]() -> cudaError_t {
+        return variant ? Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt,
+                                                  c->stream)
+                       : Launch<T, NS>::stage(a, c->chem, nt, c->stream);
+      };
+      CK(launch());
+      CK(cudaEventRecord(e0, c->stream));
+      for (int r = 0; r < 3; ++r) CK(launch());
+      CK(cudaEventRecord(e1, c->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms / 3 < best) best = ms / 3, best_kz = kz, best_tma = variant == 1;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  build_tiles_kz(c, best_kz);
+  CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
+                     c->stream));
+  c->use_tma = best_tma;
+  c->tuned_ms = best;
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
@@ -747,6 +877,7 @@ int cc_init(cc_ctx *c, int precision) {
   if (int r = check_ctx(c)) return r;
   if (precision != CC_FP64 && precision != CC_MIXED) return fail(CC_ERR_ARG, "precision must be 0 or 1");
   if (c->blocks.empty()) return fail(CC_ERR_STATE, "no blocks");
+  const bool first_init = !c->initialized;
   if (!c->initialized) {
     for (size_t b = 0; b < c->blocks.size(); ++b)
       if (!c->pend[b]) return fail(CC_ERR_STATE, "block " + std::to_string(b) + " has no state (cc_set_state)");
@@ -779,6 +910,10 @@ int cc_init(cc_ctx *c, int precision) {
   destroy_graphs(c);
   int r = dispatch(c, [&](auto tt, auto nn) { return derive_state<typename decltype(tt)::type, decltype(nn)::value>(c); });
   if (r) return r;
+  if (first_init) {
+    r = dispatch(c, [&](auto tt, auto nn) { return autotune<typename decltype(tt)::type, decltype(nn)::value>(c); });
+    if (r) return r;
+  }
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
@@ -957,6 +1092,14 @@ int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[4]) {
   out_ms[1] = n_launch > 0 ? ha / n_launch : 0;
   out_ms[2] = n_launch;
   out_ms[3] = (st + ha) / n_steps;
+  return 0;
+}
+
+int cc_tuning(cc_ctx *c, int *use_tma, int *kz, double *stage_ms) {
+  if (int r = check_ctx(c)) return r;
+  if (use_tma) *use_tma = c->use_tma ? 1 : 0;
+  if (kz) *kz = c->kz;
+  if (stage_ms) *stage_ms = c->tuned_ms;
   return 0;
 }
 

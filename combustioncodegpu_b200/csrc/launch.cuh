@@ -2,6 +2,7 @@
 #pragma once
 #include "launch.h"
 #include "stage.cuh"
+#include "stage_tma.cuh"
 
 namespace ccb {
 
@@ -12,8 +13,26 @@ size_t Launch<T, NS>::stage_smem() {
 }
 
 template <typename T, int NS>
+size_t Launch<T, NS>::stage_tma_smem() {
+  return TmaLayout<T, NS>::kBytes;
+}
+
+template <typename T, int NS>
 cudaError_t Launch<T, NS>::configure() {
-  return cudaFuncSetAttribute(k_stage<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem());
+  cudaError_t e = cudaFuncSetAttribute(k_stage<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem());
+  if (e != cudaSuccess) return e;
+  if (stage_tma_smem() <= 227 * 1024)
+    e = cudaFuncSetAttribute(k_stage_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_tma_smem());
+  return e;
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::stage_tma(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
+                                     cudaStream_t s) {
+  if (n_tiles <= 0) return cudaSuccess;
+  if (stage_tma_smem() > 227 * 1024) return cudaErrorInvalidConfiguration;
+  k_stage_tma<T, NS><<<n_tiles, dim3(kTX, kTY), stage_tma_smem(), s>>>(a, (const CUtensorMap *)maps, C);
+  return cudaGetLastError();
 }
 
 template <typename T, int NS>

@@ -13,6 +13,10 @@ struct Launch {
   static size_t stage_smem();
   static cudaError_t configure();  // kernel attributes; call outside stream capture
   static cudaError_t stage(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s);
+  // TMA-staged variant (stage_tma.cuh); maps = one CUtensorMap per block for a.P
+  static size_t stage_tma_smem();
+  static cudaError_t stage_tma(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
+                               cudaStream_t s);
   static cudaError_t halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   static cudaError_t halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   static cudaError_t cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, double *vel,

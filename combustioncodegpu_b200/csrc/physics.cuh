@@ -36,10 +36,15 @@ struct SpecCount {
   __device__ __forceinline__ static int n(const ChemParams &C) { return NS >= 0 ? NS : C.ns; }
 };
 
-template <typename T>
-__device__ __forceinline__ T ld(const T *p) {
-  return __ldg(p);
-}
+// Division, reciprocal, square root and x^-0.145 of the bulk precision: IEEE
+// in FP64 (the plain path), hardware approximations in FP32 (the mixed path;
+// relative error of a few ulp, far below the path's 1e-5 error budget).
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double frcp(double a) { return 1.0 / a; }
+__device__ __forceinline__ float frcp(float a) { return __fdividef(1.0f, a); }
+__device__ __forceinline__ double fsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ float fsqrt(float a) { return a * rsqrtf(a); }
 
 // NASA-7 enthalpy and cp of species k at temperature t (per unit mass).
 template <typename T>
@@ -87,7 +92,7 @@ __device__ __forceinline__ double pow_m0145<double>(double x) {
 }
 template <>
 __device__ __forceinline__ float pow_m0145<float>(float x) {
-  return powf(x, -0.145f);
+  return __powf(x, -0.145f);
 }
 
 // Wilke mixture viscosity, modified-Wilke conductivity and constant-Schmidt
@@ -99,17 +104,17 @@ __device__ __forceinline__ void transport(const ChemParams &C, T temp, const T *
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   T X[A], vis[A], svis[A], isvis[A];
-  const T sqt = sqrt(temp);
+  const T sqt = fsqrt(temp);
 #pragma unroll
   for (int l = 0; l < A; ++l) {
     if (l < ns) {
       X[l] = Y[l] * mw_total * S.inv_mw[l];
       const T t_dl = temp * S.lj_inv[l];
       const T tp = t_dl + T(0.5);
-      const T omega = T(1.147) * pow_m0145<T>(t_dl) + T(1) / (tp * tp);
-      vis[l] = S.vis_coeff[l] * sqt / omega;
-      svis[l] = sqrt(vis[l]);
-      isvis[l] = T(1) / svis[l];
+      const T omega = T(1.147) * pow_m0145<T>(t_dl) + frcp(tp * tp);
+      vis[l] = fdiv(S.vis_coeff[l] * sqt, omega);
+      svis[l] = fsqrt(vis[l]);
+      isvis[l] = frcp(svis[l]);
     }
   }
   T viscosity = 0, conductivity = 0;
@@ -131,8 +136,8 @@ __device__ __forceinline__ void transport(const ChemParams &C, T temp, const T *
         }
       }
       const T lam_m = vis[m] * (cp[m] + S.lam_shift[m]);
-      viscosity += vis[m] * X[m] / vt;
-      conductivity += lam_m * X[m] / (T(1.065) * vt - T(0.065) * X[m]);
+      viscosity += fdiv(vis[m] * X[m], vt);
+      conductivity += fdiv(lam_m * X[m], T(1.065) * vt - T(0.065) * X[m]);
     }
   }
   mu_out = viscosity;
@@ -142,7 +147,7 @@ __device__ __forceinline__ void transport(const ChemParams &C, T temp, const T *
   for (int l = 0; l < A; ++l) {
     if (l < ns) {
       const T d = X[l] - T(1);
-      rhod[l] = (fabs(d) < T(1e-3)) ? viscosity * inv_sc : (T(1) - Y[l]) * viscosity / ((T(1) - X[l]) * T(C.Sc));
+      rhod[l] = (fabs(d) < T(1e-3)) ? viscosity * inv_sc : fdiv((T(1) - Y[l]) * viscosity, (T(1) - X[l]) * T(C.Sc));
     }
   }
 }
@@ -174,9 +179,9 @@ __device__ __forceinline__ void point_props(const ChemParams &C, T temp, const T
       cvv += Y[l] * (cp[l] - S.cv_shift[l]);
     }
   }
-  const T mw = T(1) / mwi;
-  gamma = cp_tot / cvv;
-  c = sqrt(gamma * T(kRu) * temp / mw);
+  const T mw = frcp(mwi);
+  gamma = fdiv(cp_tot, cvv);
+  c = fsqrt(gamma * T(kRu) * temp * mwi);
   transport<T, NS>(C, temp, Y, mw, cp, mu, lam, rhod);
 }
 
@@ -216,9 +221,11 @@ __device__ __forceinline__ T sgn1(T a) {
   return T((T(0) < a) - (a < T(0)));
 }
 
+// 0.5 (sgn a + sgn b) min(|a|, |b|), written as a sign test
 template <typename T>
 __device__ __forceinline__ T minmod(T a, T b) {
-  return T(0.5) * (sgn1(a) + sgn1(b)) * fmin(fabs(a), fabs(b));
+  const T m = fmin(fabs(a), fabs(b));
+  return (a > T(0) && b > T(0)) ? m : ((a < T(0) && b < T(0)) ? -m : T(0));
 }
 
 // MUSCL (kappa = 1/3, minmod) or first-order states at the face between
@@ -266,8 +273,8 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T (&v)[
 #pragma unroll
     for (int l = 0; l < A; ++l)
       if (l < ns) mwl += L[5 + l] * S.inv_mw[l], mwr += R[5 + l] * S.inv_mw[l];
-    const T t_l = L[4] / (L[0] * T(kRu) * mwl);
-    const T t_r = R[4] / (R[0] * T(kRu) * mwr);
+    const T t_l = fdiv(L[4], L[0] * T(kRu) * mwl);
+    const T t_r = fdiv(R[4], R[0] * T(kRu) * mwr);
     T cpl = 0, cpr = 0, cvl = 0, cvr = 0;
 #pragma unroll
     for (int l = 0; l < A; ++l) {
@@ -285,23 +292,23 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T (&v)[
     }
     El = L[0] * el - L[4];
     Er = R[0] * er - R[4];
-    gam_l = cpl / cvl;
-    gam_r = cpr / cvr;
+    gam_l = fdiv(cpl, cvl);
+    gam_r = fdiv(cpr, cvr);
   }
   const T alpha = T(3.0 / 16.0);
   const T k1 = k[0], k2 = k[1], k3 = k[2];
-  const T gk = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
-  const T igk = T(1) / gk;
+  const T gk = fsqrt(k1 * k1 + k2 * k2 + k3 * k3);
+  const T igk = frcp(gk);
   const T ul = (k1 * L[1] + k2 * L[2] + k3 * L[3]) * igk;
   const T ur = (k1 * R[1] + k2 * R[2] + k3 * R[3]) * igk;
   const T pl = L[4], pr = R[4], rho_l = L[0], rho_r = R[0];
-  const T c = T(0.5) * (sqrt(gam_l * pl / rho_l) + sqrt(gam_r * pr / rho_r));
-  const T ic = T(1) / c;
+  const T c = T(0.5) * (fsqrt(fdiv(gam_l * pl, rho_l)) + fsqrt(fdiv(gam_r * pr, rho_r)));
+  const T ic = frcp(c);
   const T mach_l = ul * ic, mach_r = ur * ic;
   T mlp, mrn, plp, prn;
   if (fabs(mach_l) > T(1)) {
     mlp = T(0.5) * (mach_l + fabs(mach_l));
-    plp = mlp / mach_l;
+    plp = fdiv(mlp, mach_l);
   } else {
     const T a = (mach_l + T(1)) * (mach_l + T(1)) * T(0.25);
     const T b = (mach_l * mach_l - T(1)) * (mach_l * mach_l - T(1));
@@ -310,7 +317,7 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T (&v)[
   }
   if (fabs(mach_r) > T(1)) {
     mrn = T(0.5) * (mach_r - fabs(mach_r));
-    prn = mrn / mach_r;
+    prn = fdiv(mrn, mach_r);
   } else {
     const T a = (mach_r - T(1)) * (mach_r - T(1)) * T(0.25);
     const T b = (mach_r * mach_r - T(1)) * (mach_r * mach_r - T(1));
@@ -328,7 +335,7 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T (&v)[
   F[1] = coeff * (up ? L[1] : R[1]) + p_coeff * k1;
   F[2] = coeff * (up ? L[2] : R[2]) + p_coeff * k2;
   F[3] = coeff * (up ? L[3] : R[3]) + p_coeff * k3;
-  F[4] = up ? coeff * (El + pl) / rho_l : coeff * (Er + pr) / rho_r;
+  F[4] = up ? fdiv(coeff * (El + pl), rho_l) : fdiv(coeff * (Er + pr), rho_r);
 #pragma unroll
   for (int l = 0; l < A; ++l)
     if (l < ns) F[5 + l] = coeff * (up ? L[5 + l] : R[5 + l]);

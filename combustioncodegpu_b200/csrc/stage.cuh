@@ -52,24 +52,35 @@ __device__ __forceinline__ double local_time_step(const ChemParams &C, const T *
   return C.cfl / (sri + srv);
 }
 
-// Face flux (inviscid minus viscous) of the face between p and p + e_d.
-template <typename T, int NS>
-__device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restrict__ P, const T *__restrict__ Pr,
-                                          const T *__restrict__ G, int64_t N, int64_t p, int d, const int64_t s[3],
-                                          T *F) {
+// Stencil access of the primitives around one face (point p0 and its
+// neighbour p1 = p0 + e_d):  at(f, t) is field f at p0 + t e_d (t = -1..2);
+// cross(f, c, sg, t) is field f at p0 + t e_d + sg e_c.
+template <typename T>
+struct GlobalStencil {
+  const T *__restrict__ P;
+  int N, p, d;
+  const int *s;
+  __device__ __forceinline__ T at(int f, int t) const { return P[f * N + p + t * s[d]]; }
+  __device__ __forceinline__ T cross(int f, int c, int sg, int t) const { return P[f * N + p + t * s[d] + sg * s[c]]; }
+};
+
+// Face flux (inviscid minus viscous) of the face between p0 and p0 + e_d;
+// transport properties and geometry are read from the arenas at the global
+// point gp (and gp + gsd).
+template <typename T, int NS, typename Stencil>
+__device__ __forceinline__ void face_flux_gen(const ChemParams &C, const Stencil &S, const T *__restrict__ Pr,
+                                              const T *__restrict__ G, int N, int gp, int gsd, int d, T *F) {
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
-  const int64_t sd = s[d];
-  const int64_t p1 = p + sd;
+  const int p = gp, p1 = gp + gsd;
   T v[4][5 + A];
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
-    const int64_t q = p + (t - 1) * sd;
 #pragma unroll
-    for (int f = 0; f < 5; ++f) v[t][f] = P[f * N + q];
+    for (int f = 0; f < 5; ++f) v[t][f] = S.at(f, t - 1);
 #pragma unroll
     for (int l = 0; l < A; ++l)
-      if (l < ns) v[t][5 + l] = P[(6 + l) * N + q];
+      if (l < ns) v[t][5 + l] = S.at(6 + l, t - 1);
   }
   T k[3];
   const T J0 = G[p], J1 = G[p1];
@@ -84,15 +95,13 @@ __device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restri
   for (int r = 0; r < 3; ++r)
 #pragma unroll
     for (int c = 0; c < 3; ++c) met[r][c] = T(0.5) * (G[(1 + 3 * r + c) * N + p] + G[(1 + 3 * r + c) * N + p1]);
-  auto deriv = [&](const T *__restrict__ f, T out[3]) {
+  auto deriv = [&](int f, T out[3]) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      if (c == d) {
-        out[c] = f[p1] - f[p];
-      } else {
-        const int64_t sc = s[c];
-        out[c] = T(0.25) * (f[p + sc] - f[p - sc] + f[p1 + sc] - f[p1 - sc]);
-      }
+      if (c == d)
+        out[c] = S.at(f, 1) - S.at(f, 0);
+      else
+        out[c] = T(0.25) * (S.cross(f, c, 1, 0) - S.cross(f, c, -1, 0) + S.cross(f, c, 1, 1) - S.cross(f, c, -1, 1));
     }
   };
   auto grad = [&](const T dd[3], T g[3]) {
@@ -100,18 +109,19 @@ __device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restri
     for (int c = 0; c < 3; ++c) g[c] = dd[0] * met[0][c] + dd[1] * met[1][c] + dd[2] * met[2][c];
   };
   T du[3], dv[3], dw[3], dT[3], gu[3], gv[3], gw[3], gT[3];
-  deriv(P + 1 * N, du);
-  deriv(P + 2 * N, dv);
-  deriv(P + 3 * N, dw);
-  deriv(P + 5 * N, dT);
+  deriv(1, du);
+  deriv(2, dv);
+  deriv(3, dw);
+  deriv(5, dT);
   grad(du, gu);
   grad(dv, gv);
   grad(dw, gw);
   grad(dT, gT);
   const T mu = T(0.5) * (Pr[p] + Pr[p1]);
-  const T txx = mu * (T(4) * gu[0] - T(2) * gv[1] - T(2) * gw[2]) / T(3);
-  const T tyy = mu * (T(4) * gv[1] - T(2) * gu[0] - T(2) * gw[2]) / T(3);
-  const T tzz = mu * (T(4) * gw[2] - T(2) * gu[0] - T(2) * gv[1]) / T(3);
+  const T third = T(1.0 / 3.0);
+  const T txx = mu * (T(4) * gu[0] - T(2) * gv[1] - T(2) * gw[2]) * third;
+  const T tyy = mu * (T(4) * gv[1] - T(2) * gu[0] - T(2) * gw[2]) * third;
+  const T tzz = mu * (T(4) * gw[2] - T(2) * gu[0] - T(2) * gv[1]) * third;
   const T txy = mu * (gu[1] + gv[0]);
   const T txz = mu * (gu[2] + gw[0]);
   const T tyz = mu * (gv[2] + gw[1]);
@@ -119,9 +129,9 @@ __device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restri
   const T f1 = kx * txx + ky * txy + kz * txz;
   const T f2 = kx * txy + ky * tyy + kz * tyz;
   const T f3 = kx * txz + ky * tyz + kz * tzz;
-  const T um = T(0.5) * (P[1 * N + p] + P[1 * N + p1]);
-  const T vm = T(0.5) * (P[2 * N + p] + P[2 * N + p1]);
-  const T wm = T(0.5) * (P[3 * N + p] + P[3 * N + p1]);
+  const T um = T(0.5) * (S.at(1, 0) + S.at(1, 1));
+  const T vm = T(0.5) * (S.at(2, 0) + S.at(2, 1));
+  const T wm = T(0.5) * (S.at(3, 0) + S.at(3, 1));
   const T lam = T(0.5) * (Pr[N + p] + Pr[N + p1]);
   T f4 = um * f1 + vm * f2 + wm * f3 + lam * (kx * gT[0] + ky * gT[1] + kz * gT[2]);
   F[1] -= f1;
@@ -131,8 +141,8 @@ __device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restri
     F[4] -= f4;
     return;
   }
-  const SpecTables<T> &S = tab<T>(C);
-  const T tm = T(0.5) * (P[5 * N + p] + P[5 * N + p1]);
+  const SpecTables<T> &ST = tab<T>(C);
+  const T tm = T(0.5) * (S.at(5, 0) + S.at(5, 1));
   T D[A], gy[A][3];
   T rho_uc = 0, rho_vc = 0, rho_wc = 0;
 #pragma unroll
@@ -140,9 +150,9 @@ __device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restri
     if (l < ns) {
       D[l] = T(0.5) * (Pr[(2 + l) * N + p] + Pr[(2 + l) * N + p1]);
       T dy[3];
-      deriv(P + (6 + l) * N, dy);
+      deriv(6 + l, dy);
       grad(dy, gy[l]);
-      const T DMulH = D[l] * nasa_h<T>(S, l, tm);
+      const T DMulH = D[l] * nasa_h<T>(ST, l, tm);
       f4 += kx * DMulH * gy[l][0];
       f4 += ky * DMulH * gy[l][1];
       f4 += kz * DMulH * gy[l][2];
@@ -156,10 +166,17 @@ __device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restri
 #pragma unroll
   for (int l = 0; l < A; ++l) {
     if (l < ns) {
-      const T ym = T(0.5) * (P[(6 + l) * N + p] + P[(6 + l) * N + p1]);
+      const T ym = T(0.5) * (S.at(6 + l, 0) + S.at(6 + l, 1));
       F[5 + l] -= D[l] * (kx * gy[l][0] + ky * gy[l][1] + kz * gy[l][2]) - ym * corr;
     }
   }
+}
+
+template <typename T, int NS>
+__device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restrict__ P, const T *__restrict__ Pr,
+                                          const T *__restrict__ G, int N, int p, int d, const int s[3], T *F) {
+  GlobalStencil<T> S{P, N, p, d, s};
+  face_flux_gen<T, NS>(C, S, Pr, G, N, p, s[d], d, F);
 }
 
 // gamma and acoustic speed of a point (Field.cu:187-200)
@@ -187,6 +204,89 @@ __device__ __forceinline__ void gamma_and_c(const ChemParams &C, T temp, const T
   c = sqrt(gamma * T(kRu) * temp * mwi);
 }
 
+// RK update of one interior point (TimeAdvanceFunc.cu:255-290 with the
+// Shu-Osher combination), FP64 primitives and Newton, transport properties of
+// the new state (Field.cu:178-210), |V| for the residual and the point's
+// contribution to the next global time step.
+template <typename T, int NS>
+__device__ __forceinline__ void point_update(const ChemParams &C, const StageArgs<T> &a, int p, int N,
+                                             const double *dq, double dt, double t_warm, bool three_d,
+                                             unsigned &flags, double &dt_min) {
+  constexpr int A = SpecCount<NS>::kArr;
+  constexpr int NV = 5 + A;
+  const int ns = SpecCount<NS>::n(C);
+  const int nv = 5 + ns;
+  const T *__restrict__ G = a.G;
+  const double dtj = dt / (double)G[p];
+  double q[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) {
+    if (l < nv) {
+      double qs = a.Qin[l * N + p] + dq[l] * dtj;
+      if (l == 3 && !three_d) qs = 0;
+      q[l] = (a.a != 0.0) ? a.a * a.Qn[l * N + p] + a.b * qs : qs;
+      a.Qout[l * N + p] = q[l];
+    }
+  }
+  // primitives (TimeAdvanceFunc.cu:266-289), FP64
+  const double rho = q[0];
+  const double inv = 1.0 / rho;
+  const double u = q[1] * inv, v = q[2] * inv, w = q[3] * inv;
+  const double vel2 = u * u + v * v + w * w;
+  double pres, temp;
+  double Yd[A];
+  if (NS == 0 || (NS < 0 && ns == 0)) {
+    pres = (kGammaAir - 1) * (q[4] - 0.5 * rho * vel2);
+    temp = pres * kMwAir * inv / kRu;
+  } else {
+    double ysum = 0;
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) Yd[l] = q[5 + l] * inv, ysum += Yd[l];
+    if (a.renorm_y) {
+      const double r = 1.0 / ysum;
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) Yd[l] *= r;
+    }
+    double mwi = 0;
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) mwi += Yd[l] * C.d.inv_mw[l];
+    const double gas_const = kRu * mwi;
+    const double e = q[4] * inv - 0.5 * vel2;
+    bool capped;
+    temp = newton_temperature<NS>(C, e, Yd, gas_const, t_warm, capped);
+    if (capped) flags |= kStatusNewtonCap;
+    pres = rho * temp * gas_const;
+  }
+  if (!(rho > 0) || !(pres > 0) || !(temp > 0) || !isfinite(q[4])) flags |= kStatusNonFinite;
+  if (a.vel) a.vel[p] = sqrt(vel2);
+  T* Pn = a.Pn;
+  Pn[p] = T(rho);
+  Pn[N + p] = T(u);
+  Pn[2 * N + p] = T(v);
+  Pn[3 * N + p] = T(w);
+  Pn[4 * N + p] = T(pres);
+  Pn[5 * N + p] = T(temp);
+  T Yt[A];
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) Yt[l] = T(Yd[l]), Pn[(6 + l) * N + p] = Yt[l];
+  T mu, lam, rd[A], gam, c;
+  point_props<T, NS>(C, T(temp), Yt, mu, lam, rd, gam, c);
+  T* Prn = a.Prn;
+  Prn[p] = mu;
+  Prn[N + p] = lam;
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) Prn[(2 + l) * N + p] = rd[l];
+  if (a.dt_next && !((a.skip_dt[p >> 5] >> (p & 31)) & 1u)) {
+    const double dtl = local_time_step<T>(C, G, N, p, rho, u, v, w, (double)c, (double)gam, (double)mu, three_d);
+    dt_min = fmin(dt_min, dtl);
+  }
+    }
+
 template <typename T, int NS>
 __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
     k_stage(const StageArgs<T> a, const __grid_constant__ ChemParams C) {
@@ -206,9 +306,9 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i = t.i0 + tx, j = t.j0 + ty;
   const bool act = (i < B.mx) && (j < B.my);
-  const int64_t N = a.N;
-  const int64_t s[3] = {1, (int64_t)B.nx, (int64_t)B.nx * B.ny};
-  const int64_t col = B.base + i + s[1] * j;
+  const int N = (int)a.N;
+  const int s[3] = {1, B.nx, B.nx * B.ny};
+  const int col = (int)B.base + i + s[1] * j;
   const T *__restrict__ P = a.P;
   const T *__restrict__ Pr = a.Pr;
   const T *__restrict__ G = a.G;
@@ -225,13 +325,13 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   // goes through the single call site below, so a face shared by two tiles
   // or two blocks is computed by identical instructions.
   for (int k = t.k0 - 1; k < t.k1; ++k) {
-    const int64_t p = col + s[2] * k;
+    const int p = col + s[2] * k;
     const bool first = (k < t.k0);
 #pragma unroll 1
     for (int it = 0; it < 5; ++it) {
       bool doit;
       int d;
-      int64_t pf = p;
+      int pf = p;
       T *dst;
       int ds;
       if (it == 0) {
@@ -246,7 +346,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
       } else if (it == 3) {
         doit = ex_x && !first;
         d = 0, dst = sFx + tx * (kTX + 1), ds = XS;
-        pf = B.base + (t.i0 - 1) + s[1] * (t.j0 + tx) + s[2] * k;
+        pf = (int)B.base + (t.i0 - 1) + s[1] * (t.j0 + tx) + s[2] * k;
       } else {
         doit = ex_y && !first;
         d = 1, dst = sFy + tx, ds = YS;
@@ -292,74 +392,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
       } else {
         dt = *a.dt;
       }
-      const double dtj = dt / (double)G[p];
-      double q[NV];
-#pragma unroll
-      for (int l = 0; l < NV; ++l) {
-        if (l < nv) {
-          double qs = a.Qin[l * N + p] + dq[l] * dtj;
-          if (l == 3 && !three_d) qs = 0;
-          q[l] = (a.a != 0.0) ? a.a * a.Qn[l * N + p] + a.b * qs : qs;
-          a.Qout[l * N + p] = q[l];
-        }
-      }
-      // primitives (TimeAdvanceFunc.cu:266-289), FP64
-      const double rho = q[0];
-      const double inv = 1.0 / rho;
-      const double u = q[1] * inv, v = q[2] * inv, w = q[3] * inv;
-      const double vel2 = u * u + v * v + w * w;
-      double pres, temp;
-      double Yd[A];
-      if (NS == 0 || (NS < 0 && ns == 0)) {
-        pres = (kGammaAir - 1) * (q[4] - 0.5 * rho * vel2);
-        temp = pres * kMwAir * inv / kRu;
-      } else {
-        double ysum = 0;
-#pragma unroll
-        for (int l = 0; l < A; ++l)
-          if (l < ns) Yd[l] = q[5 + l] * inv, ysum += Yd[l];
-        if (a.renorm_y) {
-          const double r = 1.0 / ysum;
-#pragma unroll
-          for (int l = 0; l < A; ++l)
-            if (l < ns) Yd[l] *= r;
-        }
-        double mwi = 0;
-#pragma unroll
-        for (int l = 0; l < A; ++l)
-          if (l < ns) mwi += Yd[l] * C.d.inv_mw[l];
-        const double gas_const = kRu * mwi;
-        const double e = q[4] * inv - 0.5 * vel2;
-        bool capped;
-        temp = newton_temperature<NS>(C, e, Yd, gas_const, (double)P[5 * N + p], capped);
-        if (capped) flags |= kStatusNewtonCap;
-        pres = rho * temp * gas_const;
-      }
-      if (!(rho > 0) || !(pres > 0) || !(temp > 0) || !isfinite(q[4])) flags |= kStatusNonFinite;
-      if (a.vel) a.vel[p] = sqrt(vel2);
-      T* Pn = a.Pn;
-      Pn[p] = T(rho);
-      Pn[N + p] = T(u);
-      Pn[2 * N + p] = T(v);
-      Pn[3 * N + p] = T(w);
-      Pn[4 * N + p] = T(pres);
-      Pn[5 * N + p] = T(temp);
-      T Yt[A];
-#pragma unroll
-      for (int l = 0; l < A; ++l)
-        if (l < ns) Yt[l] = T(Yd[l]), Pn[(6 + l) * N + p] = Yt[l];
-      T mu, lam, rd[A], gam, c;
-      point_props<T, NS>(C, T(temp), Yt, mu, lam, rd, gam, c);
-      T* Prn = a.Prn;
-      Prn[p] = mu;
-      Prn[N + p] = lam;
-#pragma unroll
-      for (int l = 0; l < A; ++l)
-        if (l < ns) Prn[(2 + l) * N + p] = rd[l];
-      if (a.dt_next && !((a.skip_dt[p >> 5] >> (p & 31)) & 1u)) {
-        const double dtl = local_time_step<T>(C, G, N, p, rho, u, v, w, (double)c, (double)gam, (double)mu, three_d);
-        dt_min = fmin(dt_min, dtl);
-      }
+      point_update<T, NS>(C, a, p, N, dq, dt, (double)P[5 * N + p], three_d, flags, dt_min);
     }
     T *tmp = zprev;
     zprev = zcur;

@@ -1,0 +1,306 @@
+// Stage kernel with the primitive planes of each tile staged in shared memory
+// by the Tensor Memory Accelerator (sm_100a), used by the mixed-precision path.
+//
+// Same work decomposition as k_stage (a kTX x kTY column of points swept
+// along k, faces exchanged through shared memory, fused RK update), but every
+// stencil read of the primitives hits shared memory: a ring of kSlots planes,
+// each the tile plus a 2-point halo in i and j (kHX x kHY points) for all
+// 6+ns primitive fields, filled by one cp.async.bulk.tensor (4D tensor map:
+// i, j, k, field) per plane and completed on an mbarrier.  Plane k+4 is
+// requested into the slot of plane k-1 as soon as the faces of plane k are
+// done, so copies run two planes ahead of the sweep and overlap the point
+// updates.  Transport properties and geometry are read through L1.
+//
+// Waits are bounded: a CTA whose plane does not arrive within kMaxSpins
+// polls sets kStatusTmaTimeout in the status word and leaves the sweep.
+#pragma once
+#include <cuda.h>
+
+#include "stage.cuh"
+
+namespace ccb {
+
+constexpr int kHX = kTX + 4;               // staged points along i (i0-2 .. i0+kTX+1)
+constexpr int kHY = kTY + 4;               // staged points along j
+constexpr int kPlaneVals = kHX * kHY;      // values per field and plane
+constexpr int kSlots = 5;                  // planes in flight: k-1 .. k+3
+constexpr unsigned kStatusTmaTimeout = 8u;
+constexpr long kMaxSpins = 1L << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// One plane: box {kHX, kHY, 1, nf} at (x, y, z, 0) of the block's tensor map.
+__device__ __forceinline__ void tma_load_plane(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                               uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Primitives around one face from the plane ring: pl[0..3] = planes k-1..k+2,
+// p0 at (plane 1 + zs, in-plane index q).
+template <typename T>
+struct SmemStencil {
+  const T *pl[4];
+  int q, d, zs;
+  __device__ __forceinline__ const T *loc(int t, int &idx) const {
+    if (d == 2) {
+      idx = q;
+      return pl[1 + zs + t];
+    }
+    idx = q + t * (d == 0 ? 1 : kHX);
+    return pl[1 + zs];
+  }
+  __device__ __forceinline__ T at(int f, int t) const {
+    int idx;
+    const T *b = loc(t, idx);
+    return b[f * kPlaneVals + idx];
+  }
+  __device__ __forceinline__ T cross(int f, int c, int sg, int t) const {
+    int idx;
+    const T *b = loc(t, idx);
+    if (c == 2) {
+      // plane index of the base point +- 1
+      const int base_plane = (d == 2) ? 1 + zs + t : 1 + zs;
+      return pl[base_plane + sg][f * kPlaneVals + idx];
+    }
+    return b[f * kPlaneVals + idx + sg * (c == 0 ? 1 : kHX)];
+  }
+};
+
+template <typename T, int NS>
+struct TmaLayout {
+  static constexpr int kNP = 6 + SpecCount<NS>::kArr;  // primitive fields
+  static constexpr int kNV = 5 + SpecCount<NS>::kArr;  // conserved / flux components
+  static constexpr size_t kPlaneBytes = ((sizeof(T) * kNP * kPlaneVals + 127) / 128) * 128;
+  static constexpr int XS = kTY * (kTX + 1), YS = (kTY + 1) * kTX, ZS = kTY * kTX;
+  static constexpr size_t kFluxBytes = sizeof(T) * kNV * (XS + YS + 2 * ZS);
+  // alignment slack + barriers + ring + fluxes
+  static constexpr size_t kBytes = 128 + 128 + kSlots * kPlaneBytes + kFluxBytes;
+};
+
+template <typename T, int NS>
+__global__ void __launch_bounds__(kTX *kTY, 1)
+    k_stage_tma(const StageArgs<T> a, const CUtensorMap *__restrict__ maps, const __grid_constant__ ChemParams C) {
+  using L = TmaLayout<T, NS>;
+  constexpr int A = SpecCount<NS>::kArr;
+  constexpr int NV = L::kNV;
+  const int ns = SpecCount<NS>::n(C);
+  const int nv = 5 + ns;
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  // TMA destinations must be 128-byte aligned: align the carve-up explicitly
+  unsigned char *smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  unsigned char *ring = smem_raw + 128;
+  T *sFx = reinterpret_cast<T *>(ring + kSlots * L::kPlaneBytes);
+  T *sFy = sFx + NV * L::XS;
+  T *sFz0 = sFy + NV * L::YS;
+  T *sFz1 = sFz0 + NV * L::ZS;
+  constexpr int XS = L::XS, YS = L::YS, ZS = L::ZS;
+
+  const Tile t = a.tiles[blockIdx.x];
+  const BlockInfo B = a.blocks[t.blk];
+  const CUtensorMap *map = maps + t.blk;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * kTX + tx;
+  const int i = t.i0 + tx, j = t.j0 + ty;
+  const bool act = (i < B.mx) && (j < B.my);
+  const int N = (int)a.N;
+  const int s[3] = {1, B.nx, B.nx * B.ny};
+  const int col = (int)B.base + i + s[1] * j;
+  const T *__restrict__ P = a.P;
+  const T *__restrict__ Pr = a.Pr;
+  const T *__restrict__ G = a.G;
+  const bool three_d = B.mz > 1;
+  const unsigned plane_bytes = (unsigned)(sizeof(T) * (6 + ns) * kPlaneVals);
+  // tensor coordinates of plane kp: x = i0 - 2 + g, y = j0 - 2 + g, z = kp + g
+  const int tx0 = t.i0 - 2 + B.g, ty0 = t.j0 - 2 + B.g;
+  const int kfirst = t.k0 - 2, klast = t.k1 + 1;  // planes the sweep reads
+
+  if (tid == 0) {
+    for (int b = 0; b < kSlots; ++b) mbar_init(&bars[b], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+                 : "memory");
+  }
+  __syncthreads();
+  // plane kp lives in slot (kp - kfirst) % kSlots; it is that slot's n-th
+  // load with n = (kp - kfirst) / kSlots, completed when phase n ends
+  auto slot_of = [&](int kp) { return (kp - kfirst) % kSlots; };
+  auto parity_of = [&](int kp) { return (unsigned)(((kp - kfirst) / kSlots) & 1); };
+  int k_issued = kfirst - 1;
+  if (tid == 0) {
+    for (int kp = kfirst; kp <= klast && kp < kfirst + kSlots; ++kp) {
+      const int sl = slot_of(kp);
+      mbar_arrive_expect_tx(&bars[sl], plane_bytes);
+      tma_load_plane(ring + sl * L::kPlaneBytes, map, tx0, ty0, kp + B.g, &bars[sl]);
+    }
+  }
+  k_issued = min(klast, kfirst + kSlots - 1);
+
+  const int q = (ty + 2) * kHX + (tx + 2);  // in-plane index of this thread's point
+  const bool ex_x = (ty == 1) && (tx < kTY) && (t.j0 + tx < B.my);
+  const bool ex_y = (ty == 0) && act;
+  unsigned flags = 0;
+  double dt_min = 1e300;
+  T *zprev = sFz1, *zcur = sFz0;
+  T F[NV];
+  bool aborted = false;
+
+  for (int k = t.k0 - 1; k < t.k1; ++k) {
+    // planes k-1 .. k+2 must be resident
+    bool late = false;
+    for (int kp = k - 1; kp <= k + 2; ++kp) {
+      long spins = 0;
+      while (!mbar_try_wait(&bars[slot_of(kp)], parity_of(kp))) {
+        if (++spins > kMaxSpins) {
+          late = true;
+          break;
+        }
+      }
+    }
+    if (__syncthreads_or(late)) {
+      if (tid == 0) atomicOr(a.status, kStatusTmaTimeout);
+      aborted = true;
+      break;
+    }
+    const T *pl[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      pl[r] = reinterpret_cast<const T *>(ring + slot_of(k - 1 + r) * L::kPlaneBytes);
+    const int p = col + s[2] * k;
+    const bool first = (k < t.k0);
+#pragma unroll 1
+    for (int it = 0; it < 5; ++it) {
+      bool doit;
+      int d, qq = q, gp = p;
+      T *dst;
+      int ds;
+      if (it == 0) {
+        doit = act && three_d;
+        d = 2, dst = zcur + ty * kTX + tx, ds = ZS;
+      } else if (it == 1) {
+        doit = act && !first;
+        d = 0, dst = sFx + ty * (kTX + 1) + tx + 1, ds = XS;
+      } else if (it == 2) {
+        doit = act && !first;
+        d = 1, dst = sFy + (ty + 1) * kTX + tx, ds = YS;
+      } else if (it == 3) {
+        doit = ex_x && !first;
+        d = 0, dst = sFx + tx * (kTX + 1), ds = XS;
+        qq = (tx + 2) * kHX + 1;  // row tx of the tile, i = i0 - 1
+        gp = (int)B.base + (t.i0 - 1) + s[1] * (t.j0 + tx) + s[2] * k;
+      } else {
+        doit = ex_y && !first;
+        d = 1, dst = sFy + tx, ds = YS;
+        qq = q - kHX;
+        gp = p - s[1];
+      }
+      if (doit) {
+        SmemStencil<T> S{{pl[0], pl[1], pl[2], pl[3]}, qq, d, 0};
+        face_flux_gen<T, NS>(C, S, Pr, G, N, gp, s[d], d, F);
+#pragma unroll
+        for (int l = 0; l < NV; ++l)
+          if (l < nv) dst[l * ds] = F[l];
+      }
+    }
+    __syncthreads();  // faces of plane k written; plane k-1 no longer read
+    {
+      const int kp = k + 4;  // reuses the slot of plane k-1
+      if (kp <= klast) {
+        if (tid == 0) {
+          const int sl = slot_of(kp);
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive_expect_tx(&bars[sl], plane_bytes);
+          tma_load_plane(ring + sl * L::kPlaneBytes, map, tx0, ty0, kp + B.g, &bars[sl]);
+        }
+        k_issued = kp;
+      }
+    }
+    if (first) {
+      T *tmp = zprev;
+      zprev = zcur;
+      zcur = tmp;
+      continue;
+    }
+    if (act) {
+      double dq[NV];
+#pragma unroll
+      for (int l = 0; l < NV; ++l) {
+        if (l < nv) {
+          T acc = (sFx[l * XS + ty * (kTX + 1) + tx + 1] - sFx[l * XS + ty * (kTX + 1) + tx]);
+          acc += (sFy[l * YS + (ty + 1) * kTX + tx] - sFy[l * YS + ty * kTX + tx]);
+          if (three_d) acc += (zcur[l * ZS + ty * kTX + tx] - zprev[l * ZS + ty * kTX + tx]);
+          dq[l] = -(double)acc;
+        }
+      }
+      const T *own = pl[1];
+      double dt;
+      if (a.local_dt) {
+        T Y[A];
+#pragma unroll
+        for (int l = 0; l < A; ++l)
+          if (l < ns) Y[l] = own[(6 + l) * kPlaneVals + q];
+        T gam, c;
+        gamma_and_c<T, NS>(C, own[5 * kPlaneVals + q], Y, gam, c);
+        dt = local_time_step<T>(C, G, N, p, (double)own[q], (double)own[kPlaneVals + q],
+                                (double)own[2 * kPlaneVals + q], (double)own[3 * kPlaneVals + q], (double)c,
+                                (double)gam, (double)Pr[p], three_d);
+      } else {
+        dt = *a.dt;
+      }
+      point_update<T, NS>(C, a, p, N, dq, dt, (double)own[5 * kPlaneVals + q], three_d, flags, dt_min);
+      (void)P;
+    }
+    T *tmp = zprev;
+    zprev = zcur;
+    zcur = tmp;
+    __syncthreads();
+  }
+  if (aborted) {
+    // let this CTA's copies in flight land before the CTA exits (bounded)
+    if (tid == 0) {
+      for (int kp = max(kfirst, k_issued - kSlots + 1); kp <= k_issued; ++kp) {
+        long spins = 0;
+        while (!mbar_try_wait(&bars[slot_of(kp)], parity_of(kp)) && ++spins < kMaxSpins) {
+        }
+      }
+    }
+    __syncthreads();
+    return;
+  }
+  if (a.dt_next) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dt_min = fmin(dt_min, __shfl_xor_sync(0xffffffffu, dt_min, o));
+    if (tx == 0) atomic_min_pos_double(a.dt_next, dt_min);
+  }
+  const unsigned any = __reduce_or_sync(0xffffffffu, flags);
+  if (any && tx == 0) atomicOr(a.status, any);
+}
+
+}  // namespace ccb

@@ -169,6 +169,10 @@ int cc_info(cc_ctx *ctx, int64_t *n_points, int64_t *device_bytes, int *n_tiles,
  * out_ms = {mean stage-kernel ms per launch, mean halo ms per stage,
  *           number of stage launches, mean stage+halo ms per step}. */
 int cc_time_kernels(cc_ctx *ctx, int n_steps, int scheme, double out_ms[4]);
+/* The stage-kernel configuration the autotuner chose at the first cc_init
+ * (use_tma: TMA-staged planes or L1 stencil reads; kz: k-planes per tile)
+ * and its measured time per launch.  CC_AUTOTUNE=0 keeps the heuristic. */
+int cc_tuning(cc_ctx *ctx, int *use_tma, int *kz, double *stage_ms);
 /* Synchronises the context's stream. */
 int cc_sync(cc_ctx *ctx);
 

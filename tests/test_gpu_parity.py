@@ -129,12 +129,12 @@ def test_graph_replay_equals_launches():
 
 
 def test_status_flags_nonfinite_state():
-    """A non-physical point (negative pressure) is reported through the
-    status word; the context stays usable."""
+    """A NaN seeded into the host state (one interior temperature) is reported
+    through the status word; the context stays usable."""
     case = cases.case_box(10, species=cases.synthetic_species(), seed=4)
     bv = case["blocks"][0]["bv"].copy()
-    ng = bv.shape[1]
-    bv[4, ng // 2] = -1.0e5
+    n = 10 + 4
+    bv[5, 5 + n * (5 + n * 5)] = np.nan  # interior point (3, 3, 3)
     case["blocks"][0]["bv"] = bv
     d = cc.Driver.from_case(case, "fp64")
     d.initialize_computation()
@@ -151,6 +151,7 @@ def test_full_size_conservation_and_mass_fractions(precision):
     n = 128
     case = cases.case_box(n, species=cases.synthetic_species(), seed=1234)
     d = cc.Driver.from_case(case, precision)
+    d.set_renormalize(True)
     d.initialize_computation()
     sl = (slice(None), slice(2, -3), slice(2, -3), slice(2, -3))
     cv0 = d.field[0].get_state()[2].reshape(14, n + 4, n + 4, n + 4)[sl].sum(axis=(1, 2, 3))
