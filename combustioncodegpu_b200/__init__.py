@@ -97,6 +97,8 @@ EXPORTS = {
     "cc_time_kernels": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp], ctypes.c_int),
     "cc_tuning": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
     "cc_sync": ([ctypes.c_void_p], ctypes.c_int),
+    "cc_residual_rms_noalloc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
+                                ctypes.c_int),
 }
 
 _lib = None

@@ -49,6 +49,8 @@ struct IntC {
 
 }  // namespace
 
+void ccb_set_last_error(const std::string &msg) { g_err = msg; }
+
 struct cc_ctx {
   ChemParams chem{};
   int ngg = 2;

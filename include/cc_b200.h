@@ -176,6 +176,19 @@ int cc_tuning(cc_ctx *ctx, int *use_tma, int *kz, double *stage_ms);
 /* Synchronises the context's stream. */
 int cc_sync(cc_ctx *ctx);
 
+/* No counterpart in the reference.  Residual norms without any allocation,
+ * for callers that cannot call cudaMalloc where they need them (an
+ * allocation-free loop, a host application that owns the device allocator):
+ * out[l] = sqrt(sum_g (cur[l*n+g] - last[l*n+g])^2 / n), l = 0..3, with cur,
+ * last ([4][n]) and out ([4]) in device memory, enqueued on `stream`.  Its
+ * scratch is a fixed 64 KiB array inside the library (held by every device
+ * that loads it), so n is limited to CC_NOALLOC_MAX_POINTS; larger n is
+ * rejected with CC_ERR_ARG.  The first call on a device looks up that
+ * array's device address, so make it before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race. */
+#define CC_NOALLOC_MAX_POINTS 8388608
+int cc_residual_rms_noalloc(const double *cur, const double *last, int64_t n, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
