@@ -158,11 +158,15 @@ void fill_tables(SpecTables<T> &S, const cc_params *p) {
     S.t_low[k] = (T)p->t_low[k];
     S.t_mid[k] = (T)p->t_mid[k];
     const double *lo = p->low_temp_coeff + 7 * k, *hi = p->high_temp_coeff + 7 * k;
-    for (int c = 0; c < 5; ++c) S.cp_lo[k][c] = (T)lo[c], S.cp_hi[k][c] = (T)hi[c];
     const double sc[5] = {1.0, 0.5, 1.0 / 3.0, 0.25, 0.2};
-    for (int c = 0; c < 5; ++c) S.h_lo[k][c] = (T)(lo[c] * sc[c]), S.h_hi[k][c] = (T)(hi[c] * sc[c]);
-    S.h_lo[k][2] = (T)(lo[2] / 3), S.h_hi[k][2] = (T)(hi[2] / 3);
-    S.h_lo[k][5] = (T)lo[5], S.h_hi[k][5] = (T)hi[5];
+    for (int r = 0; r < 2; ++r) {
+      const double *a = r == 0 ? lo : hi;
+      T *rec = S.rec[k][r];
+      for (int c = 0; c < 5; ++c) rec[c] = (T)a[c], rec[5 + c] = (T)(a[c] * sc[c]);
+      rec[7] = (T)(a[2] / 3);
+      rec[10] = (T)a[5];
+      rec[11] = 0;
+    }
     S.lj_inv[k] = (T)p->LJ_potent_inv[k];
     S.vis_coeff[k] = (T)p->vis_coeff[k];
     S.lam_shift[k] = (T)(1.25 * kRu / mw);

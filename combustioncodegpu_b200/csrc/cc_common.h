@@ -11,6 +11,7 @@ constexpr double kMwAir = 28.9647;     // Constants.h:28
 constexpr int kMaxSpec = 16;           // species supported by one context
 constexpr int kTX = 32;                // stage tile: points along i (one warp)
 constexpr int kTY = 8;                 // stage tile: points along j (warps)
+constexpr int kRecLen = 12;            // values per NASA-7 record (cp, h, pad)
 
 // Per-precision species tables, passed to every kernel by value (constant
 // bank).  Horner-form NASA-7 coefficients: for T >= t_mid the `hi` set.
@@ -21,8 +22,11 @@ struct SpecTables {
   T r_over_mw[kMaxSpec];      // R_u / W_k
   T cv_shift[kMaxSpec];       // R_u / W_k (cp - cv per species)
   T t_low[kMaxSpec], t_mid[kMaxSpec];
-  T cp_lo[kMaxSpec][5], cp_hi[kMaxSpec][5];   // cp/R   = a0 + a1 T + ... + a4 T^4
-  T h_lo[kMaxSpec][6], h_hi[kMaxSpec][6];     // h/R    = a5 + T(a0 + T(a1/2 + T(a2/3 + T(a3/4 + T a4/5))))
+  // NASA-7 record of species k, range r (0: T < t_mid, 1: T >= t_mid):
+  //   [0..4]  cp/R = a0 + a1 T + ... + a4 T^4
+  //   [5..10] h/R  = a5 + T(a0 + T(a1/2 + T(a2/3 + T(a3/4 + T a4/5)))) as b0..b4 = a0, a1/2, .., a4/5; b5 = a5
+  //   [11]    padding (records are 16-byte aligned for vector loads)
+  alignas(16) T rec[kMaxSpec][2][kRecLen];
   T lj_inv[kMaxSpec];
   T vis_coeff[kMaxSpec];
   T lam_shift[kMaxSpec];      // 1.25 R_u / W_k

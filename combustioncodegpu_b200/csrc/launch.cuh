@@ -8,8 +8,7 @@ namespace ccb {
 
 template <typename T, int NS>
 size_t Launch<T, NS>::stage_smem() {
-  constexpr int NV = 5 + SpecCount<NS>::kArr;
-  return sizeof(T) * NV * (kTY * (kTX + 1) + (kTY + 1) * kTX + 2 * kTY * kTX);
+  return StageSmem<T, NS>::kBytes;
 }
 
 template <typename T, int NS>

@@ -46,35 +46,70 @@ __device__ __forceinline__ float frcp(float a) { return __fdividef(1.0f, a); }
 __device__ __forceinline__ double fsqrt(double a) { return sqrt(a); }
 __device__ __forceinline__ float fsqrt(float a) { return a * rsqrtf(a); }
 
-// NASA-7 enthalpy and cp of species k at temperature t (per unit mass).
+// NASA-7 records (SpecTables::rec) are read through a pointer `rec` to the
+// [kMaxSpec][2][kRecLen] array: the stage kernel points it at a copy in
+// shared memory, other kernels at the constant bank (param_rec).  The range
+// is chosen per thread by the record address, so a warp whose points
+// straddle t_mid reads two records in one vector load instead of serialising
+// on divergent constant addresses, and the coefficients cannot be hoisted
+// out of the surrounding loops into registers.
 template <typename T>
-__device__ __forceinline__ void nasa_h_cp(const SpecTables<T> &S, int k, T t, T &h, T &cp) {
+__device__ __forceinline__ const T *param_rec(const ChemParams &C) {
+  return &tab<T>(C).rec[0][0][0];
+}
+
+template <typename T>
+__device__ __forceinline__ void load_rec(const T *r, T (&x)[kRecLen]);
+template <>
+__device__ __forceinline__ void load_rec<float>(const float *r, float (&x)[kRecLen]) {
+  const float4 *v = reinterpret_cast<const float4 *>(r);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const float4 w = v[q];
+    x[4 * q] = w.x, x[4 * q + 1] = w.y, x[4 * q + 2] = w.z, x[4 * q + 3] = w.w;
+  }
+}
+template <>
+__device__ __forceinline__ void load_rec<double>(const double *r, double (&x)[kRecLen]) {
+  const double2 *v = reinterpret_cast<const double2 *>(r);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const double2 w = v[q];
+    x[2 * q] = w.x, x[2 * q + 1] = w.y;
+  }
+}
+
+// Enthalpy and cp of species k at temperature t (per unit mass); below
+// t_low, h continues linearly with cp(t_low) (Thermo.cu:7-63).
+template <typename T>
+__device__ __forceinline__ void nasa_h_cp(const SpecTables<T> &S, const T *rec, int k, T t, T &h, T &cp) {
   const T tl = S.t_low[k];
   const bool below = t < tl;
   const T te = below ? tl : t;
   const bool lo = below || t < S.t_mid[k];
-  const T *a = lo ? S.cp_lo[k] : S.cp_hi[k];
-  const T *b = lo ? S.h_lo[k] : S.h_hi[k];
-  T c = a[0] + te * (a[1] + te * (a[2] + te * (a[3] + te * a[4])));
-  T hh = b[5] + te * (b[0] + te * (b[1] + te * (b[2] + te * (b[3] + te * b[4]))));
+  T x[kRecLen];
+  load_rec<T>(rec + (2 * k + (lo ? 0 : 1)) * kRecLen, x);
+  const T c = x[0] + te * (x[1] + te * (x[2] + te * (x[3] + te * x[4])));
+  T hh = x[10] + te * (x[5] + te * (x[6] + te * (x[7] + te * (x[8] + te * x[9]))));
   if (below) hh += c * (t - te);
   h = hh * S.r_over_mw[k];
   cp = c * S.r_over_mw[k];
 }
 
 template <typename T>
-__device__ __forceinline__ T nasa_h(const SpecTables<T> &S, int k, T t) {
+__device__ __forceinline__ T nasa_h(const SpecTables<T> &S, const T *rec, int k, T t) {
   T h, cp;
-  nasa_h_cp(S, k, t, h, cp);
+  nasa_h_cp(S, rec, k, t, h, cp);
   return h;
 }
 
 template <typename T>
-__device__ __forceinline__ T nasa_cp(const SpecTables<T> &S, int k, T t) {
+__device__ __forceinline__ T nasa_cp(const SpecTables<T> &S, const T *rec, int k, T t) {
   const T tl = S.t_low[k];
   const T te = t < tl ? tl : t;
-  const T *a = (t < S.t_mid[k]) ? S.cp_lo[k] : S.cp_hi[k];
-  return (a[0] + te * (a[1] + te * (a[2] + te * (a[3] + te * a[4])))) * S.r_over_mw[k];
+  T x[kRecLen];
+  load_rec<T>(rec + (2 * k + (t < S.t_mid[k] ? 0 : 1)) * kRecLen, x);
+  return (x[0] + te * (x[1] + te * (x[2] + te * (x[3] + te * x[4])))) * S.r_over_mw[k];
 }
 
 template <typename T>
@@ -155,8 +190,8 @@ __device__ __forceinline__ void transport(const ChemParams &C, T temp, const T *
 // Point properties used by the stage update and the time step:
 // mu, lambda, rho*D_k (stored) and gamma, acoustic speed (for dt).
 template <typename T, int NS>
-__device__ __forceinline__ void point_props(const ChemParams &C, T temp, const T *Y, T &mu, T &lam, T *rhod, T &gamma,
-                                            T &c) {
+__device__ __forceinline__ void point_props(const ChemParams &C, const T *rec, T temp, const T *Y, T &mu, T &lam,
+                                            T *rhod, T &gamma, T &c) {
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   if (NS == 0 || (NS < 0 && ns == 0)) {
@@ -173,7 +208,7 @@ __device__ __forceinline__ void point_props(const ChemParams &C, T temp, const T
 #pragma unroll
   for (int l = 0; l < A; ++l) {
     if (l < ns) {
-      cp[l] = nasa_cp<T>(S, l, temp);
+      cp[l] = nasa_cp<T>(S, rec, l, temp);
       mwi += Y[l] * S.inv_mw[l];
       cp_tot += Y[l] * cp[l];
       cvv += Y[l] * (cp[l] - S.cv_shift[l]);
@@ -188,8 +223,8 @@ __device__ __forceinline__ void point_props(const ChemParams &C, T temp, const T
 // Temperature from internal energy by Newton iteration, always in FP64
 // (tolerance 1e-3 on |1 - T1/T|, at most 1000 iterations, warm start t).
 template <int NS>
-__device__ __forceinline__ double newton_temperature(const ChemParams &C, double e, const double *Y, double gas_const,
-                                                     double t, bool &capped) {
+__device__ __forceinline__ double newton_temperature(const ChemParams &C, const double *rec, double e, const double *Y,
+                                                     double gas_const, double t, bool &capped) {
   const SpecTables<double> &S = C.d;
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
@@ -201,7 +236,7 @@ __device__ __forceinline__ double newton_temperature(const ChemParams &C, double
     for (int l = 0; l < A; ++l) {
       if (l < ns) {
         double hl, cpl;
-        nasa_h_cp<double>(S, l, t, hl, cpl);
+        nasa_h_cp<double>(S, rec, l, t, hl, cpl);
         cp_tot += cpl * Y[l];
         h += hl * Y[l];
       }
@@ -232,7 +267,7 @@ __device__ __forceinline__ T minmod(T a, T b) {
 // points 1 and 2 of v[0..3], face thermodynamics, then AUSM+.
 // v[t][0..4] = rho,u,v,w,p ; v[t][5+l] = Y_l.  F receives n_var values.
 template <typename T, int NS>
-__device__ __forceinline__ void face_inviscid(const ChemParams &C, const T (&v)[4][5 + SpecCount<NS>::kArr],
+__device__ __forceinline__ void face_inviscid(const ChemParams &C, const T *rec, const T (&v)[4][5 + SpecCount<NS>::kArr],
                                               const T k[3], T *F) {
   constexpr int A = SpecCount<NS>::kArr;
   constexpr int NV = 5 + A;
@@ -280,8 +315,8 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T (&v)[
     for (int l = 0; l < A; ++l) {
       if (l < ns) {
         T hl, cl, hr, cr;
-        nasa_h_cp<T>(S, l, t_l, hl, cl);
-        nasa_h_cp<T>(S, l, t_r, hr, cr);
+        nasa_h_cp<T>(S, rec, l, t_l, hl, cl);
+        nasa_h_cp<T>(S, rec, l, t_r, hr, cr);
         cpl += cl * L[5 + l];
         cpr += cr * R[5 + l];
         cvl += L[5 + l] * (cl - S.cv_shift[l]);

@@ -55,21 +55,27 @@ __device__ __forceinline__ double local_time_step(const ChemParams &C, const T *
 // Stencil access of the primitives around one face (point p0 and its
 // neighbour p1 = p0 + e_d):  at(f, t) is field f at p0 + t e_d (t = -1..2);
 // cross(f, c, sg, t) is field f at p0 + t e_d + sg e_c.
+// The strides are scalars, not an array: an array indexed by the runtime
+// face direction would live in local memory and put a local load in front of
+// every stencil address.  c is a compile-time index after unrolling.
 template <typename T>
 struct GlobalStencil {
   const T *__restrict__ P;
-  int N, p, d;
-  const int *s;
-  __device__ __forceinline__ T at(int f, int t) const { return P[f * N + p + t * s[d]]; }
-  __device__ __forceinline__ T cross(int f, int c, int sg, int t) const { return P[f * N + p + t * s[d] + sg * s[c]]; }
+  int N, p, sd, sj, sk;  // sd: stride along the face normal; sj, sk: strides of j and k
+  __device__ __forceinline__ int stride(int c) const { return c == 0 ? 1 : (c == 1 ? sj : sk); }
+  __device__ __forceinline__ T at(int f, int t) const { return P[f * N + p + t * sd]; }
+  __device__ __forceinline__ T cross(int f, int c, int sg, int t) const {
+    return P[f * N + p + t * sd + sg * stride(c)];
+  }
 };
 
 // Face flux (inviscid minus viscous) of the face between p0 and p0 + e_d;
 // transport properties and geometry are read from the arenas at the global
 // point gp (and gp + gsd).
 template <typename T, int NS, typename Stencil>
-__device__ __forceinline__ void face_flux_gen(const ChemParams &C, const Stencil &S, const T *__restrict__ Pr,
-                                              const T *__restrict__ G, int N, int gp, int gsd, int d, T *F) {
+__device__ __forceinline__ void face_flux_gen(const ChemParams &C, const T *rec, const Stencil &S,
+                                              const T *__restrict__ Pr, const T *__restrict__ G, int N, int gp, int gsd,
+                                              int d, T *F) {
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   const int p = gp, p1 = gp + gsd;
@@ -86,7 +92,7 @@ __device__ __forceinline__ void face_flux_gen(const ChemParams &C, const Stencil
   const T J0 = G[p], J1 = G[p1];
 #pragma unroll
   for (int c = 0; c < 3; ++c) k[c] = T(0.5) * (J0 * G[(1 + 3 * d + c) * N + p] + J1 * G[(1 + 3 * d + c) * N + p1]);
-  face_inviscid<T, NS>(C, v, k, F);
+  face_inviscid<T, NS>(C, rec, v, k, F);
   if (!C.viscous) return;
 
   // ViscousScheme.cu:11-342, metrics averaged over both points (m and m1)
@@ -152,7 +158,7 @@ __device__ __forceinline__ void face_flux_gen(const ChemParams &C, const Stencil
       T dy[3];
       deriv(6 + l, dy);
       grad(dy, gy[l]);
-      const T DMulH = D[l] * nasa_h<T>(ST, l, tm);
+      const T DMulH = D[l] * nasa_h<T>(ST, rec, l, tm);
       f4 += kx * DMulH * gy[l][0];
       f4 += ky * DMulH * gy[l][1];
       f4 += kz * DMulH * gy[l][2];
@@ -173,15 +179,16 @@ __device__ __forceinline__ void face_flux_gen(const ChemParams &C, const Stencil
 }
 
 template <typename T, int NS>
-__device__ __forceinline__ void face_flux(const ChemParams &C, const T *__restrict__ P, const T *__restrict__ Pr,
-                                          const T *__restrict__ G, int N, int p, int d, const int s[3], T *F) {
-  GlobalStencil<T> S{P, N, p, d, s};
-  face_flux_gen<T, NS>(C, S, Pr, G, N, p, s[d], d, F);
+__device__ __forceinline__ void face_flux(const ChemParams &C, const T *rec, const T *__restrict__ P,
+                                          const T *__restrict__ Pr, const T *__restrict__ G, int N, int p, int d,
+                                          int sd, int sj, int sk, T *F) {
+  GlobalStencil<T> S{P, N, p, sd, sj, sk};
+  face_flux_gen<T, NS>(C, rec, S, Pr, G, N, p, sd, d, F);
 }
 
 // gamma and acoustic speed of a point (Field.cu:187-200)
 template <typename T, int NS>
-__device__ __forceinline__ void gamma_and_c(const ChemParams &C, T temp, const T *Y, T &gamma, T &c) {
+__device__ __forceinline__ void gamma_and_c(const ChemParams &C, const T *rec, T temp, const T *Y, T &gamma, T &c) {
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   if (NS == 0 || (NS < 0 && ns == 0)) {
@@ -194,7 +201,7 @@ __device__ __forceinline__ void gamma_and_c(const ChemParams &C, T temp, const T
 #pragma unroll
   for (int l = 0; l < A; ++l) {
     if (l < ns) {
-      const T cp = nasa_cp<T>(S, l, temp);
+      const T cp = nasa_cp<T>(S, rec, l, temp);
       mwi += Y[l] * S.inv_mw[l];
       cp_tot += Y[l] * cp;
       cvv += Y[l] * (cp - S.cv_shift[l]);
@@ -209,7 +216,8 @@ __device__ __forceinline__ void gamma_and_c(const ChemParams &C, T temp, const T
 // the new state (Field.cu:178-210), |V| for the residual and the point's
 // contribution to the next global time step.
 template <typename T, int NS>
-__device__ __forceinline__ void point_update(const ChemParams &C, const StageArgs<T> &a, int p, int N,
+__device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, const double *rec_d,
+                                             const StageArgs<T> &a, int p, int N,
                                              const double *dq, double dt, double t_warm, bool three_d,
                                              unsigned &flags, double &dt_min) {
   constexpr int A = SpecCount<NS>::kArr;
@@ -256,7 +264,7 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const StageArg
     const double gas_const = kRu * mwi;
     const double e = q[4] * inv - 0.5 * vel2;
     bool capped;
-    temp = newton_temperature<NS>(C, e, Yd, gas_const, t_warm, capped);
+    temp = newton_temperature<NS>(C, rec_d, e, Yd, gas_const, t_warm, capped);
     if (capped) flags |= kStatusNewtonCap;
     pres = rho * temp * gas_const;
   }
@@ -274,7 +282,7 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const StageArg
   for (int l = 0; l < A; ++l)
     if (l < ns) Yt[l] = T(Yd[l]), Pn[(6 + l) * N + p] = Yt[l];
   T mu, lam, rd[A], gam, c;
-  point_props<T, NS>(C, T(temp), Yt, mu, lam, rd, gam, c);
+  point_props<T, NS>(C, rec, T(temp), Yt, mu, lam, rd, gam, c);
   T* Prn = a.Prn;
   Prn[p] = mu;
   Prn[N + p] = lam;
@@ -287,6 +295,19 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const StageArg
   }
     }
 
+// Dynamic shared memory of k_stage: FP64 NASA records, bulk-precision
+// records (aliasing the FP64 ones when T is double), face flux planes.
+template <typename T, int NS>
+struct StageSmem {
+  static constexpr int A = SpecCount<NS>::kArr;
+  static constexpr int NV = 5 + A;
+  static constexpr size_t kRecD = sizeof(double) * A * 2 * kRecLen;
+  static constexpr size_t kRecBytes = kRecD + (sizeof(T) == sizeof(double) ? 0 : sizeof(T) * A * 2 * kRecLen);
+  static constexpr size_t kBytes =
+      kRecBytes + sizeof(T) * NV * (kTY * (kTX + 1) + (kTY + 1) * kTX + 2 * kTY * kTX);
+  static_assert(kRecD % 16 == 0 && kRecBytes % 16 == 0, "records must stay 16-byte aligned");
+};
+
 template <typename T, int NS>
 __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
     k_stage(const StageArgs<T> a, const __grid_constant__ ChemParams C) {
@@ -295,7 +316,11 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   const int ns = SpecCount<NS>::n(C);
   const int nv = 5 + ns;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *sFx = reinterpret_cast<T *>(smem_raw);              // [NV][kTY][kTX+1]
+  // NASA-7 records of both precisions (the bulk one for the face and point
+  // thermodynamics, FP64 for the temperature Newton), then the face fluxes.
+  double *sRecD = reinterpret_cast<double *>(smem_raw);  // [A][2][kRecLen]
+  T *sRec = reinterpret_cast<T *>(smem_raw + (sizeof(T) == sizeof(double) ? 0 : StageSmem<T, NS>::kRecD));
+  T *sFx = reinterpret_cast<T *>(smem_raw + StageSmem<T, NS>::kRecBytes);  // [NV][kTY][kTX+1]
   T *sFy = sFx + NV * kTY * (kTX + 1);                   // [NV][kTY+1][kTX]
   T *sFz0 = sFy + NV * (kTY + 1) * kTX;                  // [NV][kTY][kTX]
   T *sFz1 = sFz0 + NV * kTY * kTX;
@@ -307,14 +332,24 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   const int i = t.i0 + tx, j = t.j0 + ty;
   const bool act = (i < B.mx) && (j < B.my);
   const int N = (int)a.N;
-  const int s[3] = {1, B.nx, B.nx * B.ny};
-  const int col = (int)B.base + i + s[1] * j;
+  const int sj = B.nx, sk = B.nx * B.ny;
+  const int col = (int)B.base + i + sj * j;
   const T *__restrict__ P = a.P;
   const T *__restrict__ Pr = a.Pr;
   const T *__restrict__ G = a.G;
   const bool three_d = B.mz > 1;
   T F[NV];
 
+  {
+    const int tid = ty * kTX + tx, nrec = ns * 2 * kRecLen;
+    const double *gd = param_rec<double>(C);
+    const T *gt = param_rec<T>(C);
+    for (int e = tid; e < nrec; e += kTX * kTY) {
+      sRecD[e] = gd[e];
+      if (sizeof(T) != sizeof(double)) sRec[e] = gt[e];
+    }
+    __syncthreads();
+  }
   const bool ex_x = (ty == 1) && (tx < kTY) && (t.j0 + tx < B.my);  // -x boundary face of row tx
   const bool ex_y = (ty == 0) && act;                               // -y boundary face of column tx
   unsigned flags = 0;
@@ -325,35 +360,35 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   // goes through the single call site below, so a face shared by two tiles
   // or two blocks is computed by identical instructions.
   for (int k = t.k0 - 1; k < t.k1; ++k) {
-    const int p = col + s[2] * k;
+    const int p = col + sk * k;
     const bool first = (k < t.k0);
 #pragma unroll 1
     for (int it = 0; it < 5; ++it) {
       bool doit;
-      int d;
+      int d, sd;
       int pf = p;
       T *dst;
       int ds;
       if (it == 0) {
         doit = act && three_d;
-        d = 2, dst = zcur + ty * kTX + tx, ds = ZS;
+        d = 2, sd = sk, dst = zcur + ty * kTX + tx, ds = ZS;
       } else if (it == 1) {
         doit = act && !first;
-        d = 0, dst = sFx + ty * (kTX + 1) + tx + 1, ds = XS;
+        d = 0, sd = 1, dst = sFx + ty * (kTX + 1) + tx + 1, ds = XS;
       } else if (it == 2) {
         doit = act && !first;
-        d = 1, dst = sFy + (ty + 1) * kTX + tx, ds = YS;
+        d = 1, sd = sj, dst = sFy + (ty + 1) * kTX + tx, ds = YS;
       } else if (it == 3) {
         doit = ex_x && !first;
-        d = 0, dst = sFx + tx * (kTX + 1), ds = XS;
-        pf = (int)B.base + (t.i0 - 1) + s[1] * (t.j0 + tx) + s[2] * k;
+        d = 0, sd = 1, dst = sFx + tx * (kTX + 1), ds = XS;
+        pf = (int)B.base + (t.i0 - 1) + sj * (t.j0 + tx) + sk * k;
       } else {
         doit = ex_y && !first;
-        d = 1, dst = sFy + tx, ds = YS;
-        pf = p - s[1];
+        d = 1, sd = sj, dst = sFy + tx, ds = YS;
+        pf = p - sj;
       }
       if (doit) {
-        face_flux<T, NS>(C, P, Pr, G, N, pf, d, s, F);
+        face_flux<T, NS>(C, sRec, P, Pr, G, N, pf, d, sd, sj, sk, F);
 #pragma unroll
         for (int l = 0; l < NV; ++l)
           if (l < nv) dst[l * ds] = F[l];
@@ -386,13 +421,13 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
         for (int l = 0; l < A; ++l)
           if (l < ns) Y[l] = P[(6 + l) * N + p];
         T gam, c;
-        gamma_and_c<T, NS>(C, P[5 * N + p], Y, gam, c);
+        gamma_and_c<T, NS>(C, sRec, P[5 * N + p], Y, gam, c);
         dt = local_time_step<T>(C, G, N, p, (double)P[p], (double)P[N + p], (double)P[2 * N + p],
                                 (double)P[3 * N + p], (double)c, (double)gam, (double)Pr[p], three_d);
       } else {
         dt = *a.dt;
       }
-      point_update<T, NS>(C, a, p, N, dq, dt, (double)P[5 * N + p], three_d, flags, dt_min);
+      point_update<T, NS>(C, sRec, sRecD, a, p, N, dq, dt, (double)P[5 * N + p], three_d, flags, dt_min);
     }
     T *tmp = zprev;
     zprev = zcur;
@@ -430,13 +465,14 @@ __device__ __forceinline__ RefPtrs<T> resolve(const HaloArgs<T> &a, const HaloRe
 template <int NS>
 __device__ __forceinline__ double total_energy(const ChemParams &C, double rho, double u, double v, double w, double p,
                                                double t, const double *Y) {
+  const double *rec = param_rec<double>(C);
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   double e = 0.5 * rho * (u * u + v * v + w * w);
   if (NS == 0 || (NS < 0 && ns == 0)) return e + p / (kGammaAir - 1);
 #pragma unroll
   for (int l = 0; l < A; ++l)
-    if (l < ns) e += nasa_h<double>(C.d, l, t) * (rho * Y[l]);
+    if (l < ns) e += nasa_h<double>(C.d, rec, l, t) * (rho * Y[l]);
   return e - p;
 }
 
@@ -555,7 +591,7 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
 #pragma unroll
     for (int l = 0; l < A; ++l)
       if (l < ns) Yt[l] = T(Y[l]);
-    point_props<T, NS>(C, T(pr[5]), Yt, mu, lam, rd, gam, c);
+    point_props<T, NS>(C, param_rec<T>(C), T(pr[5]), Yt, mu, lam, rd, gam, c);
     a.sPr[o] = mu;
     a.sPr[S + o] = lam;
 #pragma unroll
@@ -587,7 +623,7 @@ __global__ void k_halo_copies(const HaloArgs<T> a, const __grid_constant__ ChemP
 #pragma unroll
       for (int l = 0; l < A; ++l)
         if (l < ns) Y[l] = a.P[(6 + l) * N + p];
-      gamma_and_c<T, NS>(C, a.P[5 * N + p], Y, gam, cs);
+      gamma_and_c<T, NS>(C, param_rec<T>(C), a.P[5 * N + p], Y, gam, cs);
       dt_min = local_time_step<T>(C, a.G, N, p, (double)a.P[p], (double)a.P[N + p], (double)a.P[2 * N + p],
                                   (double)a.P[3 * N + p], (double)cs, (double)gam, (double)a.Pr[p],
                                   (c.src.pad & 2) != 0);
@@ -639,7 +675,7 @@ __global__ void k_props_all(const __grid_constant__ ChemParams C, const T *P, T 
 #pragma unroll
   for (int l = 0; l < A; ++l)
     if (l < ns) Y[l] = P[(6 + l) * N + p];
-  point_props<T, NS>(C, P[5 * N + p], Y, mu, lam, rd, gam, c);
+  point_props<T, NS>(C, param_rec<T>(C), P[5 * N + p], Y, mu, lam, rd, gam, c);
   Pr[p] = mu;
   Pr[N + p] = lam;
 #pragma unroll
@@ -669,7 +705,7 @@ __global__ void k_dt_reduce(const __grid_constant__ ChemParams C, const BlockInf
 #pragma unroll
     for (int l = 0; l < A; ++l)
       if (l < ns) Y[l] = P[(6 + l) * N + p];
-    gamma_and_c<T, NS>(C, P[5 * N + p], Y, gam, c);
+    gamma_and_c<T, NS>(C, param_rec<T>(C), P[5 * N + p], Y, gam, c);
     const double dtl = local_time_step<T>(C, G, N, p, (double)P[p], (double)P[N + p], (double)P[2 * N + p],
                                           (double)P[3 * N + p], (double)c, (double)gam, (double)Pr[p], B.mz > 1);
     m = fmin(m, dtl);

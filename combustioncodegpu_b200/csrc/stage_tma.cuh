@@ -131,8 +131,8 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
   const int i = t.i0 + tx, j = t.j0 + ty;
   const bool act = (i < B.mx) && (j < B.my);
   const int N = (int)a.N;
-  const int s[3] = {1, B.nx, B.nx * B.ny};
-  const int col = (int)B.base + i + s[1] * j;
+  const int sj = B.nx, sk = B.nx * B.ny;
+  const int col = (int)B.base + i + sj * j;
   const T *__restrict__ P = a.P;
   const T *__restrict__ Pr = a.Pr;
   const T *__restrict__ G = a.G;
@@ -193,37 +193,37 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
 #pragma unroll
     for (int r = 0; r < 4; ++r)
       pl[r] = reinterpret_cast<const T *>(ring + slot_of(k - 1 + r) * L::kPlaneBytes);
-    const int p = col + s[2] * k;
+    const int p = col + sk * k;
     const bool first = (k < t.k0);
 #pragma unroll 1
     for (int it = 0; it < 5; ++it) {
       bool doit;
-      int d, qq = q, gp = p;
+      int d, sd, qq = q, gp = p;
       T *dst;
       int ds;
       if (it == 0) {
         doit = act && three_d;
-        d = 2, dst = zcur + ty * kTX + tx, ds = ZS;
+        d = 2, sd = sk, dst = zcur + ty * kTX + tx, ds = ZS;
       } else if (it == 1) {
         doit = act && !first;
-        d = 0, dst = sFx + ty * (kTX + 1) + tx + 1, ds = XS;
+        d = 0, sd = 1, dst = sFx + ty * (kTX + 1) + tx + 1, ds = XS;
       } else if (it == 2) {
         doit = act && !first;
-        d = 1, dst = sFy + (ty + 1) * kTX + tx, ds = YS;
+        d = 1, sd = sj, dst = sFy + (ty + 1) * kTX + tx, ds = YS;
       } else if (it == 3) {
         doit = ex_x && !first;
-        d = 0, dst = sFx + tx * (kTX + 1), ds = XS;
+        d = 0, sd = 1, dst = sFx + tx * (kTX + 1), ds = XS;
         qq = (tx + 2) * kHX + 1;  // row tx of the tile, i = i0 - 1
-        gp = (int)B.base + (t.i0 - 1) + s[1] * (t.j0 + tx) + s[2] * k;
+        gp = (int)B.base + (t.i0 - 1) + sj * (t.j0 + tx) + sk * k;
       } else {
         doit = ex_y && !first;
-        d = 1, dst = sFy + tx, ds = YS;
+        d = 1, sd = sj, dst = sFy + tx, ds = YS;
         qq = q - kHX;
-        gp = p - s[1];
+        gp = p - sj;
       }
       if (doit) {
         SmemStencil<T> S{{pl[0], pl[1], pl[2], pl[3]}, qq, d, 0};
-        face_flux_gen<T, NS>(C, S, Pr, G, N, gp, s[d], d, F);
+        face_flux_gen<T, NS>(C, param_rec<T>(C), S, Pr, G, N, gp, sd, d, F);
 #pragma unroll
         for (int l = 0; l < NV; ++l)
           if (l < nv) dst[l * ds] = F[l];
@@ -267,14 +267,15 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
         for (int l = 0; l < A; ++l)
           if (l < ns) Y[l] = own[(6 + l) * kPlaneVals + q];
         T gam, c;
-        gamma_and_c<T, NS>(C, own[5 * kPlaneVals + q], Y, gam, c);
+        gamma_and_c<T, NS>(C, param_rec<T>(C), own[5 * kPlaneVals + q], Y, gam, c);
         dt = local_time_step<T>(C, G, N, p, (double)own[q], (double)own[kPlaneVals + q],
                                 (double)own[2 * kPlaneVals + q], (double)own[3 * kPlaneVals + q], (double)c,
                                 (double)gam, (double)Pr[p], three_d);
       } else {
         dt = *a.dt;
       }
-      point_update<T, NS>(C, a, p, N, dq, dt, (double)own[5 * kPlaneVals + q], three_d, flags, dt_min);
+      point_update<T, NS>(C, param_rec<T>(C), param_rec<double>(C), a, p, N, dq, dt, (double)own[5 * kPlaneVals + q],
+                          three_d, flags, dt_min);
       (void)P;
     }
     T *tmp = zprev;
