@@ -96,6 +96,7 @@ EXPORTS = {
                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "cc_time_kernels": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp], ctypes.c_int),
     "cc_tuning": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
+    "cc_set_tuning": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "cc_sync": ([ctypes.c_void_p], ctypes.c_int),
     "cc_residual_rms_noalloc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
                                 ctypes.c_int),
@@ -389,6 +390,12 @@ class Driver:
         tma, kz, ms = ctypes.c_int(), ctypes.c_int(), np.zeros(1)
         _check(self.lib.cc_tuning(self.ctx, ctypes.byref(tma), ctypes.byref(kz), _ptr(ms)))
         return {"tma": bool(tma.value), "kz": kz.value, "stage_ms": float(ms[0])}
+
+    def set_tuning(self, variant="auto", kz=0):
+        """Pin the stage-kernel configuration: variant "auto", "l1" or "tma";
+        kz k-planes per tile (0 = autotune)."""
+        v = {"auto": -1, "l1": 0, "tma": 1}[variant] if isinstance(variant, str) else int(variant)
+        _check(self.lib.cc_set_tuning(self.ctx, v, int(kz)))
 
     def close(self):
         if getattr(self, "ctx", None):

@@ -100,6 +100,8 @@ struct cc_ctx {
   int renorm = -1;                // Y renormalisation: -1 = by precision (mixed on, FP64 off)
   bool use_tma = false;           // TMA-staged stage kernel (mixed precision, 0 or 9 species)
   bool tma_ok = false;            // tensor maps built (the TMA variant can run)
+  int force_variant = -1;         // cc_set_tuning: -1 autotune, 0 L1 stencil reads, 1 TMA planes
+  int force_kz = 0;               // cc_set_tuning: k-planes per tile, 0 = autotune
   int kz = 1;                     // k-chunk of the stage tiles
   double tuned_ms = 0;            // stage-kernel time of the chosen configuration
   CUtensorMap *d_tmaps = nullptr; // [2][n_blocks]: primitive arenas P[0], P[1] per block
@@ -581,7 +583,9 @@ int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qou
 template <typename T, int NS>
 int autotune(cc_ctx *c) {
   const char *env = std::getenv("CC_AUTOTUNE");
-  if (env && env[0] == '0') return 0;
+  if (env && env[0] == '0' && c->force_variant < 0 && c->force_kz <= 0) return 0;
+  const char *venv = std::getenv("CC_AUTOTUNE_VERBOSE");  // print every candidate's time to stderr
+  const bool verbose = venv && venv[0] == '1';
   StageArgs<T> a{};
   a.blocks = c->d_blocks;
   a.tiles = c->d_tiles;
@@ -609,7 +613,13 @@ int autotune(cc_ctx *c) {
   double best = 1e300;
   int best_kz = c->kz;
   bool best_tma = false;
-  for (int variant = 0; variant < (c->tma_ok ? 2 : 1); ++variant) {
+  if (c->force_kz > 0) kzs.assign(1, c->force_kz);
+  std::vector<int> variants;
+  if (c->force_variant >= 0)
+    variants.push_back(c->force_variant);
+  else
+    for (int v = 0; v < (c->tma_ok ? 2 : 1); ++v) variants.push_back(v);
+  for (int variant : variants) {
     for (int kz : kzs) {
       build_tiles_kz(c, kz);
       CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
@@ -627,6 +637,8 @@ int autotune(cc_ctx *c) {
       CK(cudaEventSynchronize(e1));
       float ms = 0;
       CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (verbose)
+        std::fprintf(stderr, "cc autotune: %s kz=%d tiles=%d %.4f ms\n", variant ? "tma" : "l1", kz, nt, ms / 3);
       if (ms / 3 < best) best = ms / 3, best_kz = kz, best_tma = variant == 1;
     }
   }
@@ -1106,6 +1118,22 @@ int cc_tuning(cc_ctx *c, int *use_tma, int *kz, double *stage_ms) {
   if (use_tma) *use_tma = c->use_tma ? 1 : 0;
   if (kz) *kz = c->kz;
   if (stage_ms) *stage_ms = c->tuned_ms;
+  return 0;
+}
+
+int cc_set_tuning(cc_ctx *c, int variant, int kz) {
+  if (int r = check_ctx(c)) return r;
+  if (variant < -1 || variant > 1) return fail(CC_ERR_ARG, "variant must be -1 (autotune), 0 (L1) or 1 (TMA)");
+  if (kz < 0) return fail(CC_ERR_ARG, "kz must be >= 0");
+  c->force_variant = variant;
+  c->force_kz = kz;
+  if (!c->initialized) return 0;
+  if (variant == 1 && !c->tma_ok)
+    return fail(CC_ERR_ARG, "the TMA variant needs CC_MIXED with 0 or 9 species");
+  destroy_graphs(c);
+  int r = dispatch(c, [&](auto tt, auto nn) { return autotune<typename decltype(tt)::type, decltype(nn)::value>(c); });
+  if (r) return r;
+  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 

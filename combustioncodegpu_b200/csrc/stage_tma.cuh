@@ -62,34 +62,30 @@ __device__ __forceinline__ void tma_load_plane(void *dst, const CUtensorMap *map
       : "memory");
 }
 
-// Primitives around one face from the plane ring: pl[0..3] = planes k-1..k+2,
-// p0 at (plane 1 + zs, in-plane index q).
+// Primitives around one face from the plane ring: planes k-1 .. k+2 at
+// pm, p0, p1, p2; the face's first point at in-plane index q of plane k.
+// Scalar plane pointers (not an array): a runtime-indexed array would be
+// placed in local memory.  t and c are compile-time after unrolling; d is
+// the runtime face direction.
 template <typename T>
 struct SmemStencil {
-  const T *pl[4];
-  int q, d, zs;
-  __device__ __forceinline__ const T *loc(int t, int &idx) const {
-    if (d == 2) {
-      idx = q;
-      return pl[1 + zs + t];
-    }
-    idx = q + t * (d == 0 ? 1 : kHX);
-    return pl[1 + zs];
+  const T *pm, *p0, *p1, *p2;
+  int q, d;
+  __device__ __forceinline__ const T *plane(int r) const {  // r = 0..3 -> k-1 .. k+2
+    return r == 0 ? pm : (r == 1 ? p0 : (r == 2 ? p1 : p2));
   }
   __device__ __forceinline__ T at(int f, int t) const {
-    int idx;
-    const T *b = loc(t, idx);
-    return b[f * kPlaneVals + idx];
+    if (d == 2) return plane(1 + t)[f * kPlaneVals + q];
+    return p0[f * kPlaneVals + q + t * (d == 0 ? 1 : kHX)];
   }
   __device__ __forceinline__ T cross(int f, int c, int sg, int t) const {
-    int idx;
-    const T *b = loc(t, idx);
-    if (c == 2) {
-      // plane index of the base point +- 1
-      const int base_plane = (d == 2) ? 1 + zs + t : 1 + zs;
-      return pl[base_plane + sg][f * kPlaneVals + idx];
+    if (c == 2) {  // neighbour plane of the base point (k or k+t along z)
+      if (d == 2) return plane(1 + t + sg)[f * kPlaneVals + q];
+      return plane(1 + sg)[f * kPlaneVals + q + t * (d == 0 ? 1 : kHX)];
     }
-    return b[f * kPlaneVals + idx + sg * (c == 0 ? 1 : kHX)];
+    const int cs = sg * (c == 0 ? 1 : kHX);
+    if (d == 2) return plane(1 + t)[f * kPlaneVals + q + cs];
+    return p0[f * kPlaneVals + q + t * (d == 0 ? 1 : kHX) + cs];
   }
 };
 
@@ -99,9 +95,11 @@ struct TmaLayout {
   static constexpr int kNV = 5 + SpecCount<NS>::kArr;  // conserved / flux components
   static constexpr size_t kPlaneBytes = ((sizeof(T) * kNP * kPlaneVals + 127) / 128) * 128;
   static constexpr int XS = kTY * (kTX + 1), YS = (kTY + 1) * kTX, ZS = kTY * kTX;
-  static constexpr size_t kFluxBytes = sizeof(T) * kNV * (XS + YS + 2 * ZS);
-  // alignment slack + barriers + ring + fluxes
-  static constexpr size_t kBytes = 128 + 128 + kSlots * kPlaneBytes + kFluxBytes;
+  static constexpr size_t kFluxBytes = ((sizeof(T) * kNV * (XS + YS + 2 * ZS) + 15) / 16) * 16;
+  static constexpr size_t kRecD = sizeof(double) * SpecCount<NS>::kArr * 2 * kRecLen;
+  static constexpr size_t kRecBytes = kRecD + (sizeof(T) == sizeof(double) ? 0 : sizeof(T) * SpecCount<NS>::kArr * 2 * kRecLen);
+  // alignment slack + barriers + ring + fluxes + NASA records (FP64, bulk)
+  static constexpr size_t kBytes = 128 + 128 + kSlots * kPlaneBytes + kFluxBytes + kRecBytes;
 };
 
 template <typename T, int NS>
@@ -121,6 +119,9 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
   T *sFy = sFx + NV * L::XS;
   T *sFz0 = sFy + NV * L::YS;
   T *sFz1 = sFz0 + NV * L::ZS;
+  double *sRecD = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(sFx) + L::kFluxBytes);
+  T *sRec = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(sRecD) +
+                                  (sizeof(T) == sizeof(double) ? 0 : L::kRecD));
   constexpr int XS = L::XS, YS = L::YS, ZS = L::ZS;
 
   const Tile t = a.tiles[blockIdx.x];
@@ -142,6 +143,10 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
   const int tx0 = t.i0 - 2 + B.g, ty0 = t.j0 - 2 + B.g;
   const int kfirst = t.k0 - 2, klast = t.k1 + 1;  // planes the sweep reads
 
+  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * kTY) {
+    sRecD[e] = param_rec<double>(C)[e];
+    if (sizeof(T) != sizeof(double)) sRec[e] = param_rec<T>(C)[e];
+  }
   if (tid == 0) {
     for (int b = 0; b < kSlots; ++b) mbar_init(&bars[b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -189,10 +194,10 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
       aborted = true;
       break;
     }
-    const T *pl[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-      pl[r] = reinterpret_cast<const T *>(ring + slot_of(k - 1 + r) * L::kPlaneBytes);
+    const T *plm = reinterpret_cast<const T *>(ring + slot_of(k - 1) * L::kPlaneBytes);
+    const T *pl0 = reinterpret_cast<const T *>(ring + slot_of(k) * L::kPlaneBytes);
+    const T *pl1 = reinterpret_cast<const T *>(ring + slot_of(k + 1) * L::kPlaneBytes);
+    const T *pl2 = reinterpret_cast<const T *>(ring + slot_of(k + 2) * L::kPlaneBytes);
     const int p = col + sk * k;
     const bool first = (k < t.k0);
 #pragma unroll 1
@@ -222,8 +227,8 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
         gp = p - sj;
       }
       if (doit) {
-        SmemStencil<T> S{{pl[0], pl[1], pl[2], pl[3]}, qq, d, 0};
-        face_flux_gen<T, NS>(C, param_rec<T>(C), S, Pr, G, N, gp, sd, d, F);
+        SmemStencil<T> S{plm, pl0, pl1, pl2, qq, d};
+        face_flux_gen<T, NS>(C, sRec, S, Pr, G, N, gp, sd, d, F);
 #pragma unroll
         for (int l = 0; l < NV; ++l)
           if (l < nv) dst[l * ds] = F[l];
@@ -259,7 +264,7 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
           dq[l] = -(double)acc;
         }
       }
-      const T *own = pl[1];
+      const T *own = pl0;
       double dt;
       if (a.local_dt) {
         T Y[A];
@@ -267,15 +272,14 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
         for (int l = 0; l < A; ++l)
           if (l < ns) Y[l] = own[(6 + l) * kPlaneVals + q];
         T gam, c;
-        gamma_and_c<T, NS>(C, param_rec<T>(C), own[5 * kPlaneVals + q], Y, gam, c);
+        gamma_and_c<T, NS>(C, sRec, own[5 * kPlaneVals + q], Y, gam, c);
         dt = local_time_step<T>(C, G, N, p, (double)own[q], (double)own[kPlaneVals + q],
                                 (double)own[2 * kPlaneVals + q], (double)own[3 * kPlaneVals + q], (double)c,
                                 (double)gam, (double)Pr[p], three_d);
       } else {
         dt = *a.dt;
       }
-      point_update<T, NS>(C, param_rec<T>(C), param_rec<double>(C), a, p, N, dq, dt, (double)own[5 * kPlaneVals + q],
-                          three_d, flags, dt_min);
+      point_update<T, NS>(C, sRec, sRecD, a, p, N, dq, dt, (double)own[5 * kPlaneVals + q], three_d, flags, dt_min);
       (void)P;
     }
     T *tmp = zprev;

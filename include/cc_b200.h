@@ -173,6 +173,13 @@ int cc_time_kernels(cc_ctx *ctx, int n_steps, int scheme, double out_ms[4]);
  * (use_tma: TMA-staged planes or L1 stencil reads; kz: k-planes per tile)
  * and its measured time per launch.  CC_AUTOTUNE=0 keeps the heuristic. */
 int cc_tuning(cc_ctx *ctx, int *use_tma, int *kz, double *stage_ms);
+/* No counterpart in the reference (its launch shapes are fixed).  Pins the
+ * stage-kernel configuration instead of autotuning it: variant -1 = autotune,
+ * 0 = L1 stencil reads, 1 = TMA-staged planes (CC_MIXED with 0 or 9 species
+ * only); kz = k-planes per tile, 0 = autotune.  Before cc_init it applies to
+ * the first cc_init; after it, the new configuration is timed and used from
+ * the next cc_step on. */
+int cc_set_tuning(cc_ctx *ctx, int variant, int kz);
 /* Synchronises the context's stream. */
 int cc_sync(cc_ctx *ctx);
 

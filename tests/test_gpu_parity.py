@@ -38,12 +38,15 @@ def _cases():
 CASES = _cases()
 
 
-def compare(case, scheme, n, precision):
+def compare(case, scheme, n, precision, variant="auto", kz=0):
     renorm = precision == "mixed" and case["params"].get("species") is not None
     o = Oracle(case)
     o.init()
     d = cc.Driver.from_case(case, precision)
+    d.set_tuning(variant, kz)
     d.initialize_computation()
+    if variant != "auto":
+        assert d.tuning()["tma"] == (variant == "tma")
     if scheme == "rk3":
         o.rk3_step(n, renorm_y=renorm)
     else:
@@ -90,6 +93,37 @@ def test_mixed_close_to_oracle(name, scheme):
     tol = {"res": 5e-3, "dt": 1e-5}
     bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-4)}
     assert not bad, errs
+
+
+# The TMA-staged variant (mixed precision, 0 or 9 species) on every case,
+# with k-chunks that split the sweep (kz=3) and that do not (kz=64).
+@pytest.mark.parametrize("kz", [3, 64])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tma_variant_close_to_oracle(name, kz):
+    errs, status = compare(CASES[name], "rk3", 2, "mixed", "tma", kz)
+    assert status == 0
+    tol = {"res": 5e-3, "dt": 1e-5}
+    bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-4)}
+    assert not bad, errs
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_k_chunking_is_bit_identical(precision):
+    """A face at a k-chunk boundary is computed by both chunks through the
+    same call site: the state after two steps must not depend on kz."""
+    case = CASES["multiblock"]
+    out = []
+    for kz in (1, 2, 64):
+        d = cc.Driver.from_case(case, precision)
+        d.set_tuning("l1", kz)
+        d.initialize_computation()
+        assert d.tuning()["kz"] == kz
+        d.simulate(2, "rk3")
+        out.append([d.field[b].get_state()[2] for b in range(len(case["blocks"]))])
+        d.close()
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            np.testing.assert_array_equal(a, b)
 
 
 @pytest.mark.parametrize("name", mg.NAMES)
