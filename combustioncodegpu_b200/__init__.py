@@ -29,6 +29,7 @@ MAX_SPECIES = 16
 CC_FP64, CC_MIXED = 0, 1
 CC_RK3, CC_STEADY_EULER = 0, 1
 PRECISIONS = {"fp64": CC_FP64, "mixed": CC_MIXED}
+VARIANTS = ("l1", "tma", "split")  # stage-kernel variants, cc_tuning order
 SCHEMES = {"rk3": CC_RK3, "steady": CC_STEADY_EULER}
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -386,15 +387,17 @@ class Driver:
         return {"n_points": n.value, "device_bytes": nb.value, "n_tiles": nt.value, "halo_levels": nl.value}
 
     def tuning(self):
-        """Stage-kernel configuration chosen by the autotuner."""
-        tma, kz, ms = ctypes.c_int(), ctypes.c_int(), np.zeros(1)
-        _check(self.lib.cc_tuning(self.ctx, ctypes.byref(tma), ctypes.byref(kz), _ptr(ms)))
-        return {"tma": bool(tma.value), "kz": kz.value, "stage_ms": float(ms[0])}
+        """Stage-kernel configuration in use: variant ("l1" fused with L1
+        stencil reads, "tma" fused with TMA-staged planes, "split" face and
+        update kernels), k-planes per tile, measured ms per stage."""
+        v, kz, ms = ctypes.c_int(), ctypes.c_int(), np.zeros(1)
+        _check(self.lib.cc_tuning(self.ctx, ctypes.byref(v), ctypes.byref(kz), _ptr(ms)))
+        return {"variant": VARIANTS[v.value], "kz": kz.value, "stage_ms": float(ms[0])}
 
     def set_tuning(self, variant="auto", kz=0):
-        """Pin the stage-kernel configuration: variant "auto", "l1" or "tma";
-        kz k-planes per tile (0 = autotune)."""
-        v = {"auto": -1, "l1": 0, "tma": 1}[variant] if isinstance(variant, str) else int(variant)
+        """Pin the stage-kernel configuration: variant "auto", "l1", "tma" or
+        "split"; kz k-planes per tile (0 = autotune)."""
+        v = (-1 if variant == "auto" else VARIANTS.index(variant)) if isinstance(variant, str) else int(variant)
         _check(self.lib.cc_set_tuning(self.ctx, v, int(kz)))
 
     def close(self):

@@ -98,9 +98,12 @@ struct cc_ctx {
   int64_t *d_vel_zero = nullptr;  // wall-face points (vel = 0 after the wall condition)
   uint32_t *d_skip_dt = nullptr;  // bitmask: interior points the halo rewrites
   int renorm = -1;                // Y renormalisation: -1 = by precision (mixed on, FP64 off)
-  bool use_tma = false;           // TMA-staged stage kernel (mixed precision, 0 or 9 species)
+  int variant = 0;                // stage kernels: 0 fused (L1 stencil reads), 1 fused TMA planes, 2 split faces/update
+  std::vector<Tile> hedges;       // split variant: tiles of the minus-side face layers
+  Tile *d_edges = nullptr;
+  void *faces = nullptr;          // split variant: face fluxes [3][n_var][N] (bulk precision)
   bool tma_ok = false;            // tensor maps built (the TMA variant can run)
-  int force_variant = -1;         // cc_set_tuning: -1 autotune, 0 L1 stencil reads, 1 TMA planes
+  int force_variant = -1;         // cc_set_tuning: -1 autotune, else the variant
   int force_kz = 0;               // cc_set_tuning: k-planes per tile, 0 = autotune
   int kz = 1;                     // k-chunk of the stage tiles
   double tuned_ms = 0;            // stage-kernel time of the chosen configuration
@@ -125,10 +128,14 @@ int nv_of(const cc_ctx *c) { return 5 + c->chem.ns; }
 int np_of(const cc_ctx *c) { return 6 + c->chem.ns; }
 int npr_of(const cc_ctx *c) { return 2 + c->chem.ns; }
 
+// Allocation zeroed on the context's stream: every later upload to the
+// buffer is issued on the same stream, so it is ordered after the zeroing
+// (the context stream is non-blocking: a cudaMemset on the legacy default
+// stream could land after such an upload).
 int dev_alloc(cc_ctx *c, void **p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   CK(cudaMalloc(p, bytes));
-  CK(cudaMemset(*p, 0, bytes));
+  CK(cudaMemsetAsync(*p, 0, bytes, c->stream));
   c->allocs.push_back(*p);
   c->device_bytes += (int64_t)bytes;
   return 0;
@@ -237,6 +244,23 @@ void build_tiles_kz(cc_ctx *c, int kz) {
   c->kz = kz;
 }
 
+// Tiles of the split variant's minus-side face layers (stage_split.cuh):
+// i = -1 faces with lanes along j and warps along k, j = -1 faces with lanes
+// along i and warps along k, k = -1 faces with lanes along i, warps along j.
+void build_edge_tiles(cc_ctx *c) {
+  c->hedges.clear();
+  for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
+    const auto &b = c->blocks[bi];
+    for (int k0 = 0; k0 < b.mz; k0 += kTY) {
+      for (int j0 = 0; j0 < b.my; j0 += kTX) c->hedges.push_back(Tile{bi, -1, j0, k0, std::min(b.mz, k0 + kTY), 0, 0, 0});
+      for (int i0 = 0; i0 < b.mx; i0 += kTX) c->hedges.push_back(Tile{bi, i0, -1, k0, std::min(b.mz, k0 + kTY), 1, 0, 0});
+    }
+    if (b.mz > 1)
+      for (int j0 = 0; j0 < b.my; j0 += kTY)
+        for (int i0 = 0; i0 < b.mx; i0 += kTX) c->hedges.push_back(Tile{bi, i0, j0, -1, 0, 2, 0, 0});
+  }
+}
+
 // Initial chunk size (before autotuning): fewest waves times the per-chunk
 // cost (kz planes plus the prologue plane).
 int heuristic_kz(cc_ctx *c) {
@@ -310,7 +334,8 @@ int build_tensor_maps(cc_ctx *c) {
   void *p;
   if (dev_alloc(c, &p, sizeof(CUtensorMap) * maps.size())) return CC_ERR_CUDA;
   c->d_tmaps = (CUtensorMap *)p;
-  CK(cudaMemcpy(c->d_tmaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(c->d_tmaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice,
+                     c->stream));
   return 0;
 }
 
@@ -363,12 +388,19 @@ int setup_device(cc_ctx *c) {
     c->Q[b] = (double *)p;
   }
   if (dev_alloc(c, &c->G, E * N * 10)) return CC_ERR_CUDA;
+  if (dev_alloc(c, &c->faces, E * N * 3 * nv_of(c))) return CC_ERR_CUDA;
+  build_edge_tiles(c);
+  if (dev_alloc(c, &p, sizeof(Tile) * std::max<size_t>(1, c->hedges.size()))) return CC_ERR_CUDA;
+  c->d_edges = (Tile *)p;
+  if (!c->hedges.empty())
+    CK(cudaMemcpyAsync(c->d_edges, c->hedges.data(), sizeof(Tile) * c->hedges.size(), cudaMemcpyHostToDevice,
+                       c->stream));
   {
     const char *no_tma = std::getenv("CC_NO_TMA");
     c->tma_ok = c->precision == CC_MIXED && (c->ns_key == 0 || c->ns_key == 9) && !(no_tma && no_tma[0] == '1');
     if (c->tma_ok)
       if (int r = build_tensor_maps(c)) return r;
-    c->use_tma = false;
+    c->variant = 0;
   }
   if (dev_alloc(c, &p, sizeof(double) * N * std::max(np_of(c), 10))) return CC_ERR_CUDA;
   c->stage64 = (double *)p;
@@ -405,7 +437,8 @@ int setup_device(cc_ctx *c) {
       if (cp.src.pad & 1) mask[(size_t)(cp.dst >> 5)] |= 1u << (cp.dst & 31);
     if (dev_alloc(c, &p, sizeof(uint32_t) * mask.size())) return CC_ERR_CUDA;
     c->d_skip_dt = (uint32_t *)p;
-    CK(cudaMemcpy(c->d_skip_dt, mask.data(), sizeof(uint32_t) * mask.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(c->d_skip_dt, mask.data(), sizeof(uint32_t) * mask.size(), cudaMemcpyHostToDevice,
+                       c->stream));
   }
   if (dev_alloc(c, &p, sizeof(int64_t) * std::max<size_t>(1, c->plan.vel_zero.size()))) return CC_ERR_CUDA;
   c->d_vel_zero = (int64_t *)p;
@@ -561,14 +594,29 @@ int prof_event(cc_ctx *c, std::vector<cudaEvent_t> &pool, size_t &next) {
   return 0;
 }
 
+const char *const kVariantName[3] = {"fused-l1", "fused-tma", "split"};
+
+// One stage's kernels of the given variant over the current tile list.
+template <typename T, int NS>
+int launch_stage(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt) {
+  if (variant == 1) {
+    CK((Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
+  } else if (variant == 2) {
+    a.faces = (T *)c->faces;
+    a.edge_tiles = c->d_edges;
+    CK((Launch<T, NS>::faces(a, c->chem, nt, (int)c->hedges.size(), c->stream)));
+    CK((Launch<T, NS>::update(a, c->chem, nt, c->stream)));
+  } else {
+    CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
+  }
+  return 0;
+}
+
 template <typename T, int NS>
 int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin) {
   const int nt = (int)c->htiles.size();
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
-  if (c->use_tma)
-    CK((Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
-  else
-    CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
+  if (int r = launch_stage<T, NS>(c, a, pc, c->variant, nt)) return r;
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
   if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next)) return r;
@@ -612,34 +660,31 @@ int autotune(cc_ctx *c) {
   CK(cudaEventCreate(&e1));
   double best = 1e300;
   int best_kz = c->kz;
-  bool best_tma = false;
+  int best_variant = 0;
   if (c->force_kz > 0) kzs.assign(1, c->force_kz);
   std::vector<int> variants;
   if (c->force_variant >= 0)
     variants.push_back(c->force_variant);
   else
-    for (int v = 0; v < (c->tma_ok ? 2 : 1); ++v) variants.push_back(v);
+    for (int v : {0, 1, 2})
+      if (v != 1 || c->tma_ok) variants.push_back(v);
   for (int variant : variants) {
     for (int kz : kzs) {
       build_tiles_kz(c, kz);
       CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
                          c->stream));
       const int nt = (int)c->htiles.size();
-      auto launch = [&]() -> cudaError_t {
-        return variant ? Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt,
-                                                  c->stream)
-                       : Launch<T, NS>::stage(a, c->chem, nt, c->stream);
-      };
-      CK(launch());
+      if (int r = launch_stage<T, NS>(c, a, pc, variant, nt)) return r;
       CK(cudaEventRecord(e0, c->stream));
-      for (int r = 0; r < 3; ++r) CK(launch());
+      for (int r = 0; r < 3; ++r)
+        if (int rr = launch_stage<T, NS>(c, a, pc, variant, nt)) return rr;
       CK(cudaEventRecord(e1, c->stream));
       CK(cudaEventSynchronize(e1));
       float ms = 0;
       CK(cudaEventElapsedTime(&ms, e0, e1));
       if (verbose)
-        std::fprintf(stderr, "cc autotune: %s kz=%d tiles=%d %.4f ms\n", variant ? "tma" : "l1", kz, nt, ms / 3);
-      if (ms / 3 < best) best = ms / 3, best_kz = kz, best_tma = variant == 1;
+        std::fprintf(stderr, "cc autotune: %s kz=%d tiles=%d %.4f ms\n", kVariantName[variant], kz, nt, ms / 3);
+      if (ms / 3 < best) best = ms / 3, best_kz = kz, best_variant = variant;
     }
   }
   cudaEventDestroy(e0);
@@ -647,7 +692,7 @@ int autotune(cc_ctx *c) {
   build_tiles_kz(c, best_kz);
   CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
                      c->stream));
-  c->use_tma = best_tma;
+  c->variant = best_variant;
   c->tuned_ms = best;
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1113,9 +1158,9 @@ int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[4]) {
   return 0;
 }
 
-int cc_tuning(cc_ctx *c, int *use_tma, int *kz, double *stage_ms) {
+int cc_tuning(cc_ctx *c, int *variant, int *kz, double *stage_ms) {
   if (int r = check_ctx(c)) return r;
-  if (use_tma) *use_tma = c->use_tma ? 1 : 0;
+  if (variant) *variant = c->variant;
   if (kz) *kz = c->kz;
   if (stage_ms) *stage_ms = c->tuned_ms;
   return 0;
@@ -1123,7 +1168,8 @@ int cc_tuning(cc_ctx *c, int *use_tma, int *kz, double *stage_ms) {
 
 int cc_set_tuning(cc_ctx *c, int variant, int kz) {
   if (int r = check_ctx(c)) return r;
-  if (variant < -1 || variant > 1) return fail(CC_ERR_ARG, "variant must be -1 (autotune), 0 (L1) or 1 (TMA)");
+  if (variant < -1 || variant > 2)
+    return fail(CC_ERR_ARG, "variant must be -1 (autotune), 0 (fused, L1), 1 (fused, TMA) or 2 (split)");
   if (kz < 0) return fail(CC_ERR_ARG, "kz must be >= 0");
   c->force_variant = variant;
   c->force_kz = kz;

@@ -3,6 +3,7 @@
 #include "launch.h"
 #include "stage.cuh"
 #include "stage_tma.cuh"
+#include "stage_split.cuh"
 
 namespace ccb {
 
@@ -14,6 +15,33 @@ size_t Launch<T, NS>::stage_smem() {
 template <typename T, int NS>
 size_t Launch<T, NS>::stage_tma_smem() {
   return TmaLayout<T, NS>::kBytes;
+}
+
+template <typename T, int NS>
+size_t Launch<T, NS>::faces_smem() {
+  return sizeof(T) * SpecCount<NS>::kArr * 2 * kRecLen;
+}
+
+template <typename T, int NS>
+size_t Launch<T, NS>::update_smem() {
+  return StageSmem<T, NS>::kRecBytes;
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::faces(const StageArgs<T> &a, const ChemParams &C, int n_regular, int n_edge,
+                                 cudaStream_t s) {
+  if (n_regular + n_edge <= 0) return cudaSuccess;
+  StageArgs<T> b = a;
+  b.n_regular = n_regular;
+  k_faces<T, NS><<<n_regular + n_edge, dim3(kTX, kTY), faces_smem(), s>>>(b, C);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s) {
+  if (n_tiles <= 0) return cudaSuccess;
+  k_update<T, NS><<<n_tiles, dim3(kTX, kTY), update_smem(), s>>>(a, C);
+  return cudaGetLastError();
 }
 
 template <typename T, int NS>

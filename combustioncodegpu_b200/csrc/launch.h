@@ -17,6 +17,11 @@ struct Launch {
   static size_t stage_tma_smem();
   static cudaError_t stage_tma(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
                                cudaStream_t s);
+  // split variant (stage_split.cuh): faces of n_regular tiles + n_edge edge tiles, then the update
+  static size_t faces_smem();
+  static size_t update_smem();
+  static cudaError_t faces(const StageArgs<T> &a, const ChemParams &C, int n_regular, int n_edge, cudaStream_t s);
+  static cudaError_t update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s);
   static cudaError_t halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   static cudaError_t halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   static cudaError_t cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, double *vel,

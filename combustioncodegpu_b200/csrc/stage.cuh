@@ -295,6 +295,53 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
   }
     }
 
+// L2 prefetch of elements [s, e) of one field row through the bulk copy
+// engine: a hint that nothing waits on.  The range is clamped to the field's
+// [0, N) (N is a multiple of 32 points) and widened to 16-byte boundaries.
+template <typename E>
+__device__ __forceinline__ void l2_prefetch(const E *field, int N, int s, int e) {
+  constexpr int kPer16 = 16 / (int)sizeof(E);
+  s = max(s, 0) & ~(kPer16 - 1);
+  e = (min(e, N) + kPer16 - 1) & ~(kPer16 - 1);
+  if (e <= s) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(field + s), "r"((unsigned)((e - s) * sizeof(E)))
+               : "memory");
+}
+
+// While plane k is processed, bring into L2 what plane k+1 will read for
+// the first time: primitives of plane k+3 (tile + 2-point halo in i and j),
+// transport and geometry of plane k+2 (1-point halo), conserved variables of
+// plane k+1 (tile).  Rows are spread over the CTA's threads.
+template <typename T>
+__device__ __forceinline__ void prefetch_planes(const StageArgs<T> &a, const BlockInfo &B, const Tile &t, int k,
+                                                int np, int npr, int nv, int tid) {
+  const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
+  const int i_lo = t.i0 - 4, i_hi = t.i0 + kTX + 4;
+  auto rows = [&](auto *base, int nf, int kp, int j_lo, int j_hi, int ilo, int ihi, int &e0) {
+    const int nr = j_hi - j_lo;
+    const int n = nf * nr;
+    for (int e = tid - e0; e < n; e += kTX * kTY) {
+      if (e < 0) continue;
+      const int f = e / nr, j = j_lo + e % nr;
+      const int row = (int)B.base + sk * kp + sj * j;
+      l2_prefetch(base + (size_t)f * N, N, row + ilo, row + ihi);
+    }
+    e0 = (e0 + n) % (kTX * kTY);  // next group starts on the next free thread
+  };
+  int e0 = 0;
+  const int kmax = B.mz - 1 + B.g;
+  if (k + 3 <= kmax)
+    rows(a.P, np, k + 3, max(t.j0 - 2, -B.g), min(t.j0 + kTY + 2, B.my + B.g), i_lo, i_hi, e0);
+  if (k + 2 <= kmax) {
+    rows(a.Pr, npr, k + 2, max(t.j0 - 1, -B.g), min(t.j0 + kTY + 1, B.my + B.g), i_lo, i_hi, e0);
+    rows(a.G, 10, k + 2, max(t.j0 - 1, -B.g), min(t.j0 + kTY + 1, B.my + B.g), i_lo, i_hi, e0);
+  }
+  if (k + 1 < t.k1) {
+    rows(a.Qin, nv, k + 1, t.j0, min(t.j0 + kTY, B.my), t.i0, t.i0 + kTX, e0);
+    if (a.a != 0.0 && a.Qn != a.Qin) rows(a.Qn, nv, k + 1, t.j0, min(t.j0 + kTY, B.my), t.i0, t.i0 + kTX, e0);
+  }
+}
+
 // Dynamic shared memory of k_stage: FP64 NASA records, bulk-precision
 // records (aliasing the FP64 ones when T is double), face flux planes.
 template <typename T, int NS>
@@ -362,6 +409,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   for (int k = t.k0 - 1; k < t.k1; ++k) {
     const int p = col + sk * k;
     const bool first = (k < t.k0);
+    prefetch_planes<T>(a, B, t, k, 6 + ns, 2 + ns, nv, ty * kTX + tx);
 #pragma unroll 1
     for (int it = 0; it < 5; ++it) {
       bool doit;

@@ -169,14 +169,17 @@ int cc_info(cc_ctx *ctx, int64_t *n_points, int64_t *device_bytes, int *n_tiles,
  * out_ms = {mean stage-kernel ms per launch, mean halo ms per stage,
  *           number of stage launches, mean stage+halo ms per step}. */
 int cc_time_kernels(cc_ctx *ctx, int n_steps, int scheme, double out_ms[4]);
-/* The stage-kernel configuration the autotuner chose at the first cc_init
- * (use_tma: TMA-staged planes or L1 stencil reads; kz: k-planes per tile)
- * and its measured time per launch.  CC_AUTOTUNE=0 keeps the heuristic. */
-int cc_tuning(cc_ctx *ctx, int *use_tma, int *kz, double *stage_ms);
+/* The stage-kernel configuration in use (chosen by the autotuner at the
+ * first cc_init, or pinned by cc_set_tuning) and its measured time per
+ * stage: variant 0 = fused stage kernel with L1 stencil reads, 1 = fused
+ * with TMA-staged primitive planes, 2 = split (face kernel, then update
+ * kernel); kz = k-planes per tile.  CC_AUTOTUNE=0 keeps the heuristic. */
+int cc_tuning(cc_ctx *ctx, int *variant, int *kz, double *stage_ms);
 /* No counterpart in the reference (its launch shapes are fixed).  Pins the
  * stage-kernel configuration instead of autotuning it: variant -1 = autotune,
- * 0 = L1 stencil reads, 1 = TMA-staged planes (CC_MIXED with 0 or 9 species
- * only); kz = k-planes per tile, 0 = autotune.  Before cc_init it applies to
+ * 0 = fused with L1 stencil reads, 1 = fused with TMA-staged planes (CC_MIXED
+ * with 0 or 9 species only), 2 = split faces / update; kz = k-planes per
+ * tile, 0 = autotune.  Before cc_init it applies to
  * the first cc_init; after it, the new configuration is timed and used from
  * the next cc_step on. */
 int cc_set_tuning(cc_ctx *ctx, int variant, int kz);

@@ -46,7 +46,7 @@ def compare(case, scheme, n, precision, variant="auto", kz=0):
     d.set_tuning(variant, kz)
     d.initialize_computation()
     if variant != "auto":
-        assert d.tuning()["tma"] == (variant == "tma")
+        assert d.tuning()["variant"] == variant
     if scheme == "rk3":
         o.rk3_step(n, renorm_y=renorm)
     else:
@@ -95,8 +95,9 @@ def test_mixed_close_to_oracle(name, scheme):
     assert not bad, errs
 
 
-# The TMA-staged variant (mixed precision, 0 or 9 species) on every case,
-# with k-chunks that split the sweep (kz=3) and that do not (kz=64).
+# Every stage-kernel variant on every case, with k-chunks that split the
+# sweep (kz=3) and that do not (kz=64).  The TMA variant exists for the
+# mixed path with 0 or 9 species.
 @pytest.mark.parametrize("kz", [3, 64])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_tma_variant_close_to_oracle(name, kz):
@@ -107,15 +108,35 @@ def test_tma_variant_close_to_oracle(name, kz):
     assert not bad, errs
 
 
+@pytest.mark.parametrize("scheme", ["steady", "rk3"])
+@pytest.mark.parametrize("kz", [3, 64])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_split_variant_fp64_matches_oracle(name, kz, scheme):
+    errs, status = compare(CASES[name], scheme, 2, "fp64", "split", kz)
+    assert status == 0
+    bad = {k: v for k, v in errs.items() if not v < 1e-10}
+    assert not bad, errs
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_split_variant_mixed_close_to_oracle(name):
+    errs, status = compare(CASES[name], "rk3", 2, "mixed", "split", 3)
+    assert status == 0
+    tol = {"res": 5e-3, "dt": 1e-5}
+    bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-4)}
+    assert not bad, errs
+
+
+@pytest.mark.parametrize("variant", ["l1", "split"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_k_chunking_is_bit_identical(precision):
+def test_k_chunking_is_bit_identical(precision, variant):
     """A face at a k-chunk boundary is computed by both chunks through the
     same call site: the state after two steps must not depend on kz."""
     case = CASES["multiblock"]
     out = []
     for kz in (1, 2, 64):
         d = cc.Driver.from_case(case, precision)
-        d.set_tuning("l1", kz)
+        d.set_tuning(variant, kz)
         d.initialize_computation()
         assert d.tuning()["kz"] == kz
         d.simulate(2, "rk3")
@@ -124,6 +145,30 @@ def test_k_chunking_is_bit_identical(precision):
     for other in out[1:]:
         for a, b in zip(out[0], other):
             np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_variants_agree_at_64(precision):
+    """All stage-kernel variants give the same state at 64^3 (a size whose
+    split-variant edge tiles span several CTAs per face layer) after two
+    RK3 steps: FP64 to 1e-13, mixed to 1e-6 relative per field."""
+    case = cases.case_box(64, species=cases.synthetic_species(), seed=5)
+    variants = ["l1", "split"] + (["tma"] if precision == "mixed" else [])
+    out = {}
+    for v in variants:
+        d = cc.Driver.from_case(case, precision)
+        d.set_tuning(v, 4)
+        d.initialize_computation()
+        d.simulate(2, "rk3")
+        assert d.status() == 0
+        out[v] = d.field[0].get_state()[2].reshape(14, -1)
+        d.close()
+    tol = 1e-13 if precision == "fp64" else 1e-6
+    ref = out["l1"]
+    scale = np.abs(ref).max(axis=1)
+    for v in variants[1:]:
+        rel = np.abs(out[v] - ref).max(axis=1) / scale
+        assert rel.max() < tol, (v, rel)
 
 
 @pytest.mark.parametrize("name", mg.NAMES)
