@@ -35,7 +35,7 @@ METRIC = "Mcell-updates/s per RK stage, mixed vs FP64 plain, at stated L2 err vs
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128)
@@ -113,6 +113,14 @@ def algorithmic_bytes(ns, precision):
     if precision == "fp64":
         return nv * 24 + 2 * 8 + 10 * 8
     return nv * 24 + 2 * 4 + 10 * 4
+
+
+def face_kernel_bytes(ns, precision):
+    """Bytes per point of the split variant's face kernel: it reads the
+    primitives (6+ns), transport (2+ns) and geometry (10) once and writes three
+    faces of n_var fluxes, all at the bulk width."""
+    w = 8 if precision == "fp64" else 4
+    return ((6 + ns) + (2 + ns) + 10 + 3 * (5 + ns)) * w
 
 
 def ncu_traffic(kernel_tag):
@@ -285,12 +293,20 @@ def main():
     value = world * mixed["npts"] * stages / (mixed["ms_total"] / 1e3) / 1e6
     value_plain = world * plain["npts"] * stages / (plain["ms_total"] / 1e3) / 1e6
     bpp = algorithmic_bytes(9, "mixed")
-    stage_ms = mixed["kernels"]["stage_ms"]
-    achieved = bpp * mixed["npts"] / (stage_ms / 1e3) / 1e9
-    traffic = ncu_traffic("stage_kernel_box128_mixed")
+    kt = mixed["kernels"]
+    stage_ms = kt["stage_ms"]
+    split = mixed["tuning"]["variant"] == "split"
+    stage_achieved = bpp * mixed["npts"] / (stage_ms / 1e3) / 1e9
+    if split:  # dominant kernel: the face kernel
+        kname, kbpp, kms = "k_faces<float,9>", face_kernel_bytes(9, "mixed"), kt["faces_ms"]
+        traffic = ncu_traffic("faces_kernel_box128_mixed")
+    else:
+        kname, kbpp, kms = "k_stage<float,9>", bpp, stage_ms
+        traffic = ncu_traffic("stage_kernel_box128_mixed")
+    achieved = kbpp * mixed["npts"] / (kms / 1e3) / 1e9
     cpu = cpu_baseline(args, os.cpu_count() or 1, steps=2, n=96)
     levels = mixed["info"]["halo_levels"]
-    launches_per_step = 3 * (1 + levels + 1) + 1
+    launches_per_step = 3 * ((2 if split else 1) + levels + 1) + 1
     line = {
         "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -304,8 +320,11 @@ def main():
         "error_mixed_vs_fp64": errs,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                     "kernel": "k_stage<float,9>", "algorithmic_bytes_per_point": bpp,
-                     "stage_ms_per_launch": stage_ms, "peak_kind": peak_kind},
+                     "kernel": kname, "algorithmic_bytes_per_point": kbpp, "kernel_ms_per_launch": kms,
+                     "peak_kind": peak_kind,
+                     "stage": {"ms": stage_ms, "faces_ms": kt["faces_ms"], "update_ms": kt["update_ms"],
+                               "algorithmic_bytes_per_point": bpp, "achieved_gbs": stage_achieved,
+                               "frac": stage_achieved / peaks["hbm_gbs"]}},
         "cpu_baseline": {"value": cpu["value"], "unit": cpu["unit"], "cores": cpu["cores"], "kind": cpu["kind"],
                          "sample": cpu["sample"]},
         "e2e": e2e,

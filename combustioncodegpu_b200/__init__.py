@@ -373,10 +373,11 @@ class Driver:
     def time_kernels(self, n_steps, scheme="rk3"):
         """Event-timed run without graph replay: dict of mean stage-kernel ms
         per launch, mean halo ms per stage, launches, stage+halo ms per step."""
-        out = np.zeros(4)
+        out = np.zeros(6)
         sch = SCHEMES[scheme] if isinstance(scheme, str) else int(scheme)
         _check(self.lib.cc_time_kernels(self.ctx, int(n_steps), sch, _ptr(out)))
-        return {"stage_ms": out[0], "halo_ms": out[1], "stage_launches": int(out[2]), "step_ms": out[3]}
+        return {"stage_ms": out[0], "halo_ms": out[1], "stage_launches": int(out[2]), "step_ms": out[3],
+                "faces_ms": out[4], "update_ms": out[5]}
 
     def sync(self):
         _check(self.lib.cc_sync(self.ctx))

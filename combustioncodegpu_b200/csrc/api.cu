@@ -118,8 +118,8 @@ struct cc_ctx {
   std::vector<void *> allocs;
   // kernel timing (cc_time_kernels): events around every stage and halo launch
   bool profiling = false;
-  std::vector<cudaEvent_t> ev_stage, ev_halo;
-  size_t ev_next_stage = 0, ev_next_halo = 0;
+  std::vector<cudaEvent_t> ev_stage, ev_halo, ev_mid;  // ev_mid: between the split variant's two kernels
+  size_t ev_next_stage = 0, ev_next_halo = 0, ev_next_mid = 0;
 };
 
 namespace {
@@ -605,6 +605,7 @@ int launch_stage(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt) {
     a.faces = (T *)c->faces;
     a.edge_tiles = c->d_edges;
     CK((Launch<T, NS>::faces(a, c->chem, nt, (int)c->hedges.size(), c->stream)));
+    if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
     CK((Launch<T, NS>::update(a, c->chem, nt, c->stream)));
   } else {
     CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
@@ -831,6 +832,7 @@ int cc_destroy(cc_ctx *c) {
   destroy_graphs(c);
   for (auto e : c->ev_stage) cudaEventDestroy(e);
   for (auto e : c->ev_halo) cudaEventDestroy(e);
+  for (auto e : c->ev_mid) cudaEventDestroy(e);
   for (void *p : c->allocs) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -1120,7 +1122,7 @@ int cc_info(cc_ctx *c, int64_t *n_points, int64_t *device_bytes, int *n_tiles, i
   return 0;
 }
 
-int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[4]) {
+int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[6]) {
   if (int r = check_ctx(c)) return r;
   if (!c->initialized) return fail(CC_ERR_STATE, "cc_time_kernels before cc_init");
   if (!out_ms || n_steps < 1) return fail(CC_ERR_ARG, "bad arguments");
@@ -1130,7 +1132,7 @@ int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[4]) {
     if (r) return r;
   }
   c->profiling = true;
-  c->ev_next_stage = c->ev_next_halo = 0;
+  c->ev_next_stage = c->ev_next_halo = c->ev_next_mid = 0;
   int r = dispatch(c, [&](auto tt, auto nn) -> int {
     for (int s = 0; s < n_steps; ++s)
       if (int e = enqueue_step<typename decltype(tt)::type, decltype(nn)::value>(c, scheme)) return e;
@@ -1150,11 +1152,21 @@ int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[4]) {
     CK(cudaEventElapsedTime(&ms, c->ev_halo[i], c->ev_halo[i + 1]));
     ha += ms;
   }
+  double fa = 0, up = 0;
+  if (c->ev_next_mid * 2 == c->ev_next_stage)  // split variant: one mid event per stage
+    for (size_t i = 0; i < c->ev_next_mid; ++i) {
+      float m1 = 0, m2 = 0;
+      CK(cudaEventElapsedTime(&m1, c->ev_stage[2 * i], c->ev_mid[i]));
+      CK(cudaEventElapsedTime(&m2, c->ev_mid[i], c->ev_stage[2 * i + 1]));
+      fa += m1, up += m2;
+    }
   const double n_launch = (double)(c->ev_next_stage / 2);
   out_ms[0] = n_launch > 0 ? st / n_launch : 0;
   out_ms[1] = n_launch > 0 ? ha / n_launch : 0;
   out_ms[2] = n_launch;
   out_ms[3] = (st + ha) / n_steps;
+  out_ms[4] = n_launch > 0 ? fa / n_launch : 0;
+  out_ms[5] = n_launch > 0 ? up / n_launch : 0;
   return 0;
 }
 

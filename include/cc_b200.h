@@ -166,9 +166,11 @@ int cc_use_graph(cc_ctx *ctx, int enable);
 int cc_info(cc_ctx *ctx, int64_t *n_points, int64_t *device_bytes, int *n_tiles, int *n_halo_levels);
 /* Runs n_steps steps without graph replay, timing every stage-kernel launch
  * and every halo program with CUDA events on the context's stream:
- * out_ms = {mean stage-kernel ms per launch, mean halo ms per stage,
- *           number of stage launches, mean stage+halo ms per step}. */
-int cc_time_kernels(cc_ctx *ctx, int n_steps, int scheme, double out_ms[4]);
+ * out_ms = {mean stage-kernel ms per stage, mean halo ms per stage,
+ *           number of stages, mean stage+halo ms per step,
+ *           mean face-kernel ms and mean update-kernel ms per stage (split
+ *           variant; 0 for the fused variants)}. */
+int cc_time_kernels(cc_ctx *ctx, int n_steps, int scheme, double out_ms[6]);
 /* The stage-kernel configuration in use (chosen by the autotuner at the
  * first cc_init, or pinned by cc_set_tuning) and its measured time per
  * stage: variant 0 = fused stage kernel with L1 stencil reads, 1 = fused
