@@ -40,6 +40,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--err-steps", type=int, default=100, help="steps of the mixed-vs-FP64 error check")
+    ap.add_argument("--workload", default="box128", choices=["box128", "multiblock64", "mixing_layer"],
+                    help="box128: the headline 128^3 box; multiblock64: 64 uneven blocks, batched vs "
+                         "per-block; mixing_layer: 1024x512x4 precision study (FP64 / mixed / FP32)")
+    ap.add_argument("--study-steps", default="100,1000,2000", help="mixing_layer: error snapshot steps")
     return ap.parse_args()
 
 
@@ -230,6 +234,116 @@ def run_ours(args, rank, world, dist):
     return out, errs, e2e
 
 
+def run_multiblock(args):
+    """64 uneven blocks (4x4x4 periodic layout, 16..96 points per side): the
+    batched launch (one launch per stage kernel over all blocks, one CUDA
+    graph per step) against one launch per block per kernel, both precisions."""
+    import torch
+    import combustioncodegpu_b200 as cc
+    from combustioncodegpu_b200 import cases
+
+    case = cases.case_multiblock64(seed=2024, species=cases.synthetic_species())
+    res = {}
+    for prec in ("mixed", "fp64"):
+        for mode in ("batched", "per_block"):
+            d = cc.Driver.from_case(case, prec)
+            d.set_launch_mode(mode)
+            d.initialize_computation()
+            s = torch.cuda.ExternalStream(d.stream())
+            npts = d.info()["n_points"]
+            d.simulate(args.warmup)
+            d.sync()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            with ClockSampler(torch.cuda.current_device()) as clk:
+                e0.record(s)
+                d.simulate(args.steps)
+                e1.record(s)
+                e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            res[(prec, mode)] = {"value": npts * 3 * args.steps / (ms / 1e3) / 1e6, "ms_per_step": ms / args.steps,
+                                 "npts": npts, "clocks": clk.summary(), "tuning": d.tuning(), "status": d.status()}
+            d.close()
+    b = res[("mixed", "batched")]
+    peaks, peak_kind = load_peaks()
+    line = {"metric": METRIC, "value": b["value"], "unit": "Mcell-updates/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": b["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 fluxes/transport + f64 conserved/Newton/reductions",
+            "data": "synthetic",
+            "config": {"workload": "multiblock64_9sp_viscous_rk3", "blocks": len(case["blocks"]),
+                       "block_sizes_per_axis": cases.multiblock_sizes(2024), "points": b["npts"],
+                       "precision": "mixed", "parallelism": "single GPU", "l2": "inputs larger than L2 (no flush)",
+                       "graph": "one CUDA graph per step"},
+            "per_block_launches": {k[0]: {"batched": res[(k[0], "batched")]["value"],
+                                          "per_block": res[(k[0], "per_block")]["value"],
+                                          "batched_over_per_block": res[(k[0], "batched")]["value"]
+                                          / res[(k[0], "per_block")]["value"]} for k in res},
+            "plain_fp64": {"value": res[("fp64", "batched")]["value"], "unit": "Mcell-updates/s"},
+            "mixed_over_fp64": b["value"] / res[("fp64", "batched")]["value"],
+            "clocks": b["clocks"], "autotune": {"mixed": b["tuning"], "fp64": res[("fp64", "batched")]["tuning"]},
+            "status": {"%s/%s" % k: v["status"] for k, v in res.items()}}
+    print(json.dumps(line), flush=True)
+
+
+def run_mixing_layer(args):
+    """Precision study on the 1024x512x4 H2/air temporal mixing layer: FP64,
+    mixed and full-FP32 runs from the same state (Y renormalised in all
+    three), relative L2 / Linf errors of the primitives against FP64 at the
+    snapshot steps, and each precision's throughput over the last segment."""
+    import torch
+    import combustioncodegpu_b200 as cc
+    from combustioncodegpu_b200 import cases
+
+    case = cases.case_mixing_layer(1024, 512, 4, species=cases.synthetic_species())
+    snaps = [int(x) for x in args.study_steps.split(",")]
+    nx, ny, nz = case["blocks"][0]["dims"]
+    sl = lambda a: a.reshape(a.shape[0], nz + 4, ny + 4, nx + 4)[:, 2:-2, 2:-2, 2:-2].reshape(a.shape[0], -1)
+    states, perf, status = {}, {}, {}
+    for prec in ("fp64", "mixed", "fp32"):
+        d = cc.Driver.from_case(case, prec)
+        d.set_renormalize(True)
+        d.initialize_computation()
+        s = torch.cuda.ExternalStream(d.stream())
+        npts = d.info()["n_points"]
+        done, states[prec] = 0, {}
+        for k in snaps:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            d.simulate(k - done)
+            e1.record(s)
+            e1.synchronize()
+            perf[prec] = {"value": npts * 3 * (k - done) / (e0.elapsed_time(e1) / 1e3) / 1e6,
+                          "steps_timed": "%d-%d" % (done, k)}
+            done = k
+            bv, yk, _ = d.field[0].get_state()
+            states[prec][k] = (sl(bv), sl(yk))
+        status[prec] = d.status()
+        d.close()
+    names = ["rho", "u", "v", "w", "p", "T"]
+    l2 = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    li = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())
+    errors = {}
+    for prec in ("mixed", "fp32"):
+        errors[prec] = {}
+        for k in snaps:
+            (b, y), (b0, y0) = states[prec][k], states["fp64"][k]
+            e = {}
+            for i, nm in enumerate(names):
+                e["l2_" + nm], e["linf_" + nm] = l2(b[i], b0[i]), li(b[i], b0[i])
+            e["l2_Y"], e["linf_Y"] = l2(y, y0), li(y, y0)
+            errors[prec][str(k)] = e
+    m = perf["mixed"]
+    line = {"metric": METRIC, "value": m["value"], "unit": "Mcell-updates/s", "n_gpus": 1, "steps": snaps[-1],
+            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 fluxes/transport + f64 conserved/Newton/reductions", "data": "synthetic",
+            "config": {"workload": "mixing_layer_1024x512x4_9sp_viscous_rk3", "streams": case["streams"],
+                       "bc": "periodic x and z, zero-gradient outflow in y", "precision": "mixed",
+                       "l2": "inputs larger than L2 (no flush)", "graph": "one CUDA graph per step"},
+            "throughput": perf, "mixed_over_fp64": m["value"] / perf["fp64"]["value"],
+            "errors_vs_fp64": errors, "status": status}
+    print(json.dumps(line), flush=True)
+
+
 def cpu_baseline(args, n_threads, steps=1, n=64):
     """The oracle on the host cores: bounded sample of the workload (an
     n^3-point box with the same per-point work, `steps` RK3 steps)."""
@@ -282,6 +396,12 @@ def main():
             dist.destroy_process_group()
         return
 
+    if args.workload in ("multiblock64", "mixing_layer"):
+        if rank == 0:
+            (run_multiblock if args.workload == "multiblock64" else run_mixing_layer)(args)
+        if dist:
+            dist.destroy_process_group()
+        return
     out, errs, e2e = run_ours(args, rank, world, dist)
     if rank != 0:
         if dist:

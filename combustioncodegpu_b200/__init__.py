@@ -26,9 +26,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcc_b200.so")
 MAX_SPECIES = 16
 
-CC_FP64, CC_MIXED = 0, 1
+CC_FP64, CC_MIXED, CC_FP32 = 0, 1, 2
 CC_RK3, CC_STEADY_EULER = 0, 1
-PRECISIONS = {"fp64": CC_FP64, "mixed": CC_MIXED}
+PRECISIONS = {"fp64": CC_FP64, "mixed": CC_MIXED, "fp32": CC_FP32}
 VARIANTS = ("l1", "tma", "split")  # stage-kernel variants, cc_tuning order
 SCHEMES = {"rk3": CC_RK3, "steady": CC_STEADY_EULER}
 
@@ -98,6 +98,7 @@ EXPORTS = {
     "cc_time_kernels": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp], ctypes.c_int),
     "cc_tuning": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
     "cc_set_tuning": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "cc_set_launch_mode": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_sync": ([ctypes.c_void_p], ctypes.c_int),
     "cc_residual_rms_noalloc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
                                 ctypes.c_int),
@@ -400,6 +401,11 @@ class Driver:
         "split"; kz k-planes per tile (0 = autotune)."""
         v = (-1 if variant == "auto" else VARIANTS.index(variant)) if isinstance(variant, str) else int(variant)
         _check(self.lib.cc_set_tuning(self.ctx, v, int(kz)))
+
+    def set_launch_mode(self, mode="batched"):
+        """"batched": one launch per stage kernel over all blocks;
+        "per_block": one launch per block per kernel (the reference's way)."""
+        _check(self.lib.cc_set_launch_mode(self.ctx, {"batched": 0, "per_block": 1}[mode]))
 
     def close(self):
         if getattr(self, "ctx", None):

@@ -456,6 +456,68 @@ def case_multiblock(sizes_per_axis, L_cell=2e-3 / 127, species=None, seed=7):
             "bcs": [], "global_dims": gdims}
 
 
+def multiblock_sizes(seed=2024, n_per_axis=4, lo=16, hi=96):
+    """Block sizes of the uneven multiblock workload: n_per_axis sizes per
+    axis drawn from U[lo, hi] (PCG64, seed); block (a, b, c) of the periodic
+    layout is (nx_a, ny_b, nz_c), so every interface is conforming."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return tuple([int(v) for v in rng.integers(lo, hi + 1, size=n_per_axis)] for _ in range(3))
+
+
+def case_multiblock64(seed=2024, species=None):
+    """64 blocks (4 x 4 x 4 periodic layout) of 16..96 points per side."""
+    return case_multiblock(multiblock_sizes(seed), species=species, seed=seed)
+
+
+def mole_to_mass(X, mw):
+    """Mass fractions of mole fractions X (any shape [ns, ...])."""
+    X = np.asarray(X, dtype=np.float64)
+    w = X * mw.reshape((-1,) + (1,) * (X.ndim - 1))
+    return w / w.sum(axis=0, keepdims=True)
+
+
+def case_mixing_layer(nx=1024, ny=512, nz=4, h=4e-3 / 1023, delta=1e-4, seed=11, species=None):
+    """Temporal H2/air mixing layer (the precision-study workload).
+
+    Fuel stream above the mid-plane: X(H2) = 0.3, X(N2) = 0.7, 300 K, u = 50
+    m/s; oxidiser below: air as X(O2) = 0.21, X(N2) = 0.79, 600 K, u = 10 m/s;
+    p = 101325 Pa.  The streams are blended with s = (1 + tanh((y - y_mid) /
+    delta)) / 2 (u, T and the mass fractions linearly in s) and u, v carry
+    seeded uniform perturbations of 1% of the velocity difference.  Uniform
+    spacing h in all directions; periodic in x and z, zero-gradient outflow
+    at both y ends."""
+    species = species or synthetic_species()
+    names = list(species["names"])
+    mw = np.asarray(species["mw"])
+    ns = len(names)
+    x_fuel, x_ox = np.zeros(ns), np.zeros(ns)
+    x_fuel[names.index("H2")], x_fuel[names.index("N2")] = 0.3, 0.7
+    x_ox[names.index("O2")], x_ox[names.index("N2")] = 0.21, 0.79
+    y_fuel, y_ox = mole_to_mass(x_fuel, mw), mole_to_mass(x_ox, mw)
+    dims = (nx, ny, nz)
+    lengths = (h * (nx - 1), h * (ny - 1), h * (nz - 1))
+    jac, met = make_block(dims, lengths)
+    _, yc, _ = block_coordinates(dims, lengths)
+    yv = yc[1:-1, 1:-1, 1:-1].ravel()  # y of every ghosted point (i fastest)
+    sfr = 0.5 * (1.0 + np.tanh((yv - 0.5 * lengths[1]) / delta))
+    rng = np.random.Generator(np.random.PCG64(seed))
+    du = 50.0 - 10.0
+    u = 10.0 + du * sfr + 0.01 * du * rng.uniform(-1.0, 1.0, yv.size)
+    v = 0.01 * du * rng.uniform(-1.0, 1.0, yv.size)
+    w = np.zeros_like(u)
+    T = 600.0 - 300.0 * sfr
+    Y = y_ox[:, None] * (1.0 - sfr)[None, :] + y_fuel[:, None] * sfr[None, :]
+    p = np.full_like(u, 101325.0)
+    rho = p / (R_U * T * (Y / mw[:, None]).sum(axis=0))
+    blk = {"dims": dims, "jac": jac, "metric": met, "bv": np.stack([rho, u, v, w, p, T]), "yk": Y,
+           "boundaries": [boundary_raw(dims, "j-", 6), boundary_raw(dims, "j+", 6)],
+           "inner_faces": periodic_raw(dims, 0) + periodic_raw(dims, 2)}
+    return {"name": "mixing_layer%dx%dx%d" % dims, "params": default_params(species), "blocks": [blk],
+            "bcs": [{"label": 6, "kind": 6}],
+            "streams": {"fuel": {"X": x_fuel.tolist(), "T": 300.0, "u": 50.0},
+                        "oxidiser": {"X": x_ox.tolist(), "T": 600.0, "u": 10.0}, "delta": delta}}
+
+
 def case_channel(dims=(12, 9, 6), L=(2e-3, 1.5e-3, 1e-3), species=None, seed=99):
     """Inflow at i-, outflow at i+, isothermal wall at j-, adiabatic wall at
     j+, periodic k: exercises every boundary condition of the reference."""

@@ -100,6 +100,8 @@ struct cc_ctx {
   int renorm = -1;                // Y renormalisation: -1 = by precision (mixed on, FP64 off)
   int variant = 0;                // stage kernels: 0 fused (L1 stencil reads), 1 fused TMA planes, 2 split faces/update
   std::vector<Tile> hedges;       // split variant: tiles of the minus-side face layers
+  std::vector<int> tile_begin, edge_begin;  // per block: first tile / edge tile (lists are block-ordered), + end
+  bool per_block = false;         // cc_set_launch_mode: one launch per block per kernel instead of one per stage
   Tile *d_edges = nullptr;
   void *faces = nullptr;          // split variant: face fluxes [3][n_var][N] (bulk precision)
   bool tma_ok = false;            // tensor maps built (the TMA variant can run)
@@ -231,7 +233,9 @@ int from64(cc_ctx *c, const double *src, void *dst, int64_t count) {
 // Stage-kernel work list: kTX x kTY columns, k split into chunks of kz.
 void build_tiles_kz(cc_ctx *c, int kz) {
   c->htiles.clear();
+  c->tile_begin.clear();
   for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
+    c->tile_begin.push_back((int)c->htiles.size());
     const auto &b = c->blocks[bi];
     for (int k0 = 0; k0 < b.mz; k0 += kz)
       for (int j0 = 0; j0 < b.my; j0 += kTY)
@@ -241,6 +245,7 @@ void build_tiles_kz(cc_ctx *c, int kz) {
           c->htiles.push_back(t);
         }
   }
+  c->tile_begin.push_back((int)c->htiles.size());
   c->kz = kz;
 }
 
@@ -249,7 +254,9 @@ void build_tiles_kz(cc_ctx *c, int kz) {
 // along i and warps along k, k = -1 faces with lanes along i, warps along j.
 void build_edge_tiles(cc_ctx *c) {
   c->hedges.clear();
+  c->edge_begin.clear();
   for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
+    c->edge_begin.push_back((int)c->hedges.size());
     const auto &b = c->blocks[bi];
     for (int k0 = 0; k0 < b.mz; k0 += kTY) {
       for (int j0 = 0; j0 < b.my; j0 += kTX) c->hedges.push_back(Tile{bi, -1, j0, k0, std::min(b.mz, k0 + kTY), 0, 0, 0});
@@ -259,6 +266,7 @@ void build_edge_tiles(cc_ctx *c) {
       for (int j0 = 0; j0 < b.my; j0 += kTY)
         for (int i0 = 0; i0 < b.mx; i0 += kTX) c->hedges.push_back(Tile{bi, i0, j0, -1, 0, 2, 0, 0});
   }
+  c->edge_begin.push_back((int)c->hedges.size());
 }
 
 // Initial chunk size (before autotuning): fewest waves times the per-chunk
@@ -397,7 +405,7 @@ int setup_device(cc_ctx *c) {
                        c->stream));
   {
     const char *no_tma = std::getenv("CC_NO_TMA");
-    c->tma_ok = c->precision == CC_MIXED && (c->ns_key == 0 || c->ns_key == 9) && !(no_tma && no_tma[0] == '1');
+    c->tma_ok = c->precision != CC_FP64 && (c->ns_key == 0 || c->ns_key == 9) && !(no_tma && no_tma[0] == '1');
     if (c->tma_ok)
       if (int r = build_tensor_maps(c)) return r;
     c->variant = 0;
@@ -596,15 +604,34 @@ int prof_event(cc_ctx *c, std::vector<cudaEvent_t> &pool, size_t &next) {
 
 const char *const kVariantName[3] = {"fused-l1", "fused-tma", "split"};
 
-// One stage's kernels of the given variant over the current tile list.
+// One stage's kernels of the given variant over the current tile list:
+// one launch per kernel over all blocks, or (per_block) one per block.
+template <typename T, int NS>
+int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge);
+
 template <typename T, int NS>
 int launch_stage(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt) {
+  if (!c->per_block || c->tile_begin.size() != c->blocks.size() + 1)
+    return launch_stage_range<T, NS>(c, a, pc, variant, nt, (int)c->hedges.size());
+  const Tile *tiles = a.tiles;
+  for (size_t b = 0; b < c->blocks.size(); ++b) {
+    a.tiles = tiles + c->tile_begin[b];
+    a.edge_tiles = c->d_edges + c->edge_begin[b];
+    if (int r = launch_stage_range<T, NS>(c, a, pc, variant, c->tile_begin[b + 1] - c->tile_begin[b],
+                                          c->edge_begin[b + 1] - c->edge_begin[b]))
+      return r;
+  }
+  return 0;
+}
+
+template <typename T, int NS>
+int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge) {
   if (variant == 1) {
     CK((Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
   } else if (variant == 2) {
     a.faces = (T *)c->faces;
-    a.edge_tiles = c->d_edges;
-    CK((Launch<T, NS>::faces(a, c->chem, nt, (int)c->hedges.size(), c->stream)));
+    if (!a.edge_tiles) a.edge_tiles = c->d_edges;
+    CK((Launch<T, NS>::faces(a, c->chem, nt, n_edge, c->stream)));
     if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
     CK((Launch<T, NS>::update(a, c->chem, nt, c->stream)));
   } else {
@@ -711,6 +738,7 @@ int enqueue_step(cc_ctx *c, int scheme) {
   a.status = c->d_status;
   a.skip_dt = c->d_skip_dt;
   a.renorm_y = c->chem.ns > 0 && (c->renorm < 0 ? c->precision != CC_FP64 : c->renorm != 0);
+  a.q32 = c->precision == CC_FP32;
   if (scheme == CC_STEADY_EULER) {
     const int pc = c->cur, pn = 1 - c->cur;
     a.P = (const T *)c->P[pc], a.Pn = (T *)c->P[pn], a.Pr = (const T *)c->Pr[pc], a.Prn = (T *)c->Pr[pn];
@@ -940,7 +968,8 @@ int cc_set_state(cc_ctx *c, int block, const double *bv, const double *yk) {
 
 int cc_init(cc_ctx *c, int precision) {
   if (int r = check_ctx(c)) return r;
-  if (precision != CC_FP64 && precision != CC_MIXED) return fail(CC_ERR_ARG, "precision must be 0 or 1");
+  if (precision != CC_FP64 && precision != CC_MIXED && precision != CC_FP32)
+    return fail(CC_ERR_ARG, "precision must be CC_FP64, CC_MIXED or CC_FP32");
   if (c->blocks.empty()) return fail(CC_ERR_STATE, "no blocks");
   const bool first_init = !c->initialized;
   if (!c->initialized) {
@@ -1192,6 +1221,13 @@ int cc_set_tuning(cc_ctx *c, int variant, int kz) {
   int r = dispatch(c, [&](auto tt, auto nn) { return autotune<typename decltype(tt)::type, decltype(nn)::value>(c); });
   if (r) return r;
   CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int cc_set_launch_mode(cc_ctx *c, int per_block) {
+  if (int r = check_ctx(c)) return r;
+  c->per_block = per_block != 0;
+  destroy_graphs(c);
   return 0;
 }
 

@@ -108,6 +108,7 @@ struct StageArgs {
   const uint32_t *skip_dt;   // bitmask of points the halo rewrites (their dt is reduced there)
   int local_dt;              // 1: per-point time step of the current state
   int renorm_y;              // 1: renormalise Y_k to sum 1
+  int q32;                   // 1: full-FP32 precision (conserved variables rounded to FP32, FP32 Newton)
   // split variant (stage_split.cuh): face fluxes [3][n_var][N] (face d of
   // point p lies between p and p + e_d), the tiles of the minus-side face
   // layers (i, j or k = -1; direction in Tile::pad0), regular tile count

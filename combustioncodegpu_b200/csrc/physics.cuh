@@ -220,35 +220,42 @@ __device__ __forceinline__ void point_props(const ChemParams &C, const T *rec, T
   transport<T, NS>(C, temp, Y, mw, cp, mu, lam, rhod);
 }
 
-// Temperature from internal energy by Newton iteration, always in FP64
-// (tolerance 1e-3 on |1 - T1/T|, at most 1000 iterations, warm start t).
-template <int NS>
-__device__ __forceinline__ double newton_temperature(const ChemParams &C, const double *rec, double e, const double *Y,
-                                                     double gas_const, double t, bool &capped) {
-  const SpecTables<double> &S = C.d;
+// Temperature from internal energy by Newton iteration (tolerance 1e-3 on
+// |1 - T1/T|, at most 1000 iterations, warm start t), in the precision W:
+// FP64 for the plain and mixed paths, FP32 for the full-FP32 study.
+template <typename W, int NS>
+__device__ __forceinline__ W newton_temperature_w(const ChemParams &C, const W *rec, W e, const W *Y, W gas_const,
+                                                  W t, bool &capped) {
+  const SpecTables<W> &S = tab<W>(C);
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
-  double err = 1;
+  W err = 1;
   int iter = 0;
-  while (err > 1e-3 && iter++ < 1000) {
-    double cp_tot = 0, h = 0;
+  while (err > W(1e-3) && iter++ < 1000) {
+    W cp_tot = 0, h = 0;
 #pragma unroll
     for (int l = 0; l < A; ++l) {
       if (l < ns) {
-        double hl, cpl;
-        nasa_h_cp<double>(S, rec, l, t, hl, cpl);
+        W hl, cpl;
+        nasa_h_cp<W>(S, rec, l, t, hl, cpl);
         cp_tot += cpl * Y[l];
         h += hl * Y[l];
       }
     }
-    const double e_t = h - gas_const * t;
-    const double cvv = cp_tot - gas_const;
-    const double t1 = t - (e_t - e) / cvv;
-    err = fabs(1 - t1 / t);
+    const W e_t = h - gas_const * t;
+    const W cvv = cp_tot - gas_const;
+    const W t1 = t - (e_t - e) / cvv;
+    err = fabs(W(1) - t1 / t);
     t = t1;
   }
-  capped = err > 1e-3;
+  capped = err > W(1e-3);
   return t;
+}
+
+template <int NS>
+__device__ __forceinline__ double newton_temperature(const ChemParams &C, const double *rec, double e, const double *Y,
+                                                     double gas_const, double t, bool &capped) {
+  return newton_temperature_w<double, NS>(C, rec, e, Y, gas_const, t, capped);
 }
 
 template <typename T>

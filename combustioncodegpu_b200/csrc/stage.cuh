@@ -233,6 +233,7 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
       double qs = a.Qin[l * N + p] + dq[l] * dtj;
       if (l == 3 && !three_d) qs = 0;
       q[l] = (a.a != 0.0) ? a.a * a.Qn[l * N + p] + a.b * qs : qs;
+      if (a.q32) q[l] = (double)(float)q[l];  // full-FP32 study: FP32 conserved state
       a.Qout[l * N + p] = q[l];
     }
   }
@@ -247,24 +248,51 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
     pres = (kGammaAir - 1) * (q[4] - 0.5 * rho * vel2);
     temp = pres * kMwAir * inv / kRu;
   } else {
-    double ysum = 0;
-#pragma unroll
-    for (int l = 0; l < A; ++l)
-      if (l < ns) Yd[l] = q[5 + l] * inv, ysum += Yd[l];
-    if (a.renorm_y) {
-      const double r = 1.0 / ysum;
+    bool capped;
+    double gas_const;
+    if (!a.q32) {
+      double ysum = 0;
 #pragma unroll
       for (int l = 0; l < A; ++l)
-        if (l < ns) Yd[l] *= r;
-    }
-    double mwi = 0;
+        if (l < ns) Yd[l] = q[5 + l] * inv, ysum += Yd[l];
+      if (a.renorm_y) {
+        const double r = 1.0 / ysum;
 #pragma unroll
-    for (int l = 0; l < A; ++l)
-      if (l < ns) mwi += Yd[l] * C.d.inv_mw[l];
-    const double gas_const = kRu * mwi;
-    const double e = q[4] * inv - 0.5 * vel2;
-    bool capped;
-    temp = newton_temperature<NS>(C, rec_d, e, Yd, gas_const, t_warm, capped);
+        for (int l = 0; l < A; ++l)
+          if (l < ns) Yd[l] *= r;
+      }
+      double mwi = 0;
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) mwi += Yd[l] * C.d.inv_mw[l];
+      gas_const = kRu * mwi;
+      const double e = q[4] * inv - 0.5 * vel2;
+      temp = newton_temperature<NS>(C, rec_d, e, Yd, gas_const, t_warm, capped);
+    } else {
+      // full-FP32 study: Y, its renormalisation, e and the Newton in FP32
+      // (only the FP32 bulk precision runs it; the FP64 instantiation reads
+      // the records from the constant bank)
+      const float *rec_f32 = sizeof(T) == 4 ? reinterpret_cast<const float *>(rec) : param_rec<float>(C);
+      float Yf[A], ysum = 0;
+      const float invf = 1.0f / (float)rho;
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) Yf[l] = (float)q[5 + l] * invf, ysum += Yf[l];
+      if (a.renorm_y) {
+        const float r = 1.0f / ysum;
+#pragma unroll
+        for (int l = 0; l < A; ++l)
+          if (l < ns) Yf[l] *= r;
+      }
+      float mwi = 0;
+#pragma unroll
+      for (int l = 0; l < A; ++l)
+        if (l < ns) mwi += Yf[l] * C.f.inv_mw[l], Yd[l] = Yf[l];
+      const float gcf = float(kRu) * mwi;
+      const float ef = (float)q[4] * invf - 0.5f * (float)vel2;
+      temp = newton_temperature_w<float, NS>(C, rec_f32, ef, Yf, gcf, (float)t_warm, capped);
+      gas_const = gcf;
+    }
     if (capped) flags |= kStatusNewtonCap;
     pres = rho * temp * gas_const;
   }

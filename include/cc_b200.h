@@ -37,9 +37,13 @@ enum cc_status_code {
 
 enum cc_precision {
   CC_FP64 = 0,   /* plain: every field and every operation in FP64 */
-  CC_MIXED = 1   /* reconstruction, fluxes, transport, stored primitives in FP32;
+  CC_MIXED = 1,  /* reconstruction, fluxes, transport, stored primitives in FP32;
                     conserved variables, RK accumulation, Newton, Y renormalisation,
                     dt and residual reductions in FP64 */
+  CC_FP32 = 2    /* full FP32, for precision studies: as CC_MIXED, and the
+                    conserved variables are rounded to FP32 after every update,
+                    the temperature Newton and the Y renormalisation run in FP32
+                    (the residual reduction stays FP64) */
 };
 
 enum cc_time_scheme {
@@ -185,6 +189,11 @@ int cc_tuning(cc_ctx *ctx, int *variant, int *kz, double *stage_ms);
  * the first cc_init; after it, the new configuration is timed and used from
  * the next cc_step on. */
 int cc_set_tuning(cc_ctx *ctx, int variant, int kz);
+/* Launch granularity of the stage kernels: 0 (default) = one launch per
+ * kernel over the tiles of every block; 1 = one launch per block per kernel,
+ * the reference's granularity (Driver.cu:144-177 launches per block), kept for
+ * comparison.  Results are identical; takes effect at the next cc_step. */
+int cc_set_launch_mode(cc_ctx *ctx, int per_block);
 /* Synchronises the context's stream. */
 int cc_sync(cc_ctx *ctx);
 

@@ -32,6 +32,7 @@ def _cases():
         "channel": cases.case_channel((11, 8, 6), species=sp),
         "multiblock": cases.case_multiblock(([6, 7], [6, 5], [5]), species=sp),
         "air_visc": mg.load("air_visc_o1")[0],
+        "mixing": cases.case_mixing_layer(40, 24, 4, h=4e-3 / 39, delta=4e-4, species=sp),
     }
 
 
@@ -39,7 +40,7 @@ CASES = _cases()
 
 
 def compare(case, scheme, n, precision, variant="auto", kz=0):
-    renorm = precision == "mixed" and case["params"].get("species") is not None
+    renorm = precision in ("mixed", "fp32") and case["params"].get("species") is not None
     o = Oracle(case)
     o.init()
     d = cc.Driver.from_case(case, precision)
@@ -169,6 +170,49 @@ def test_variants_agree_at_64(precision):
     for v in variants[1:]:
         rel = np.abs(out[v] - ref).max(axis=1) / scale
         assert rel.max() < tol, (v, rel)
+
+
+# Full-FP32 precision (conserved state rounded to FP32, FP32 Newton): close
+# to the FP64 oracle after two steps, at the FP32 level.
+@pytest.mark.parametrize("name", ["box", "channel", "mixing", "sod"])
+def test_fp32_close_to_oracle(name):
+    errs, status = compare(CASES[name], "rk3", 2, "fp32")
+    assert status == 0
+    tol = {"res": 5e-2, "dt": 1e-4}
+    bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-3)}
+    assert not bad, errs
+
+
+# The uneven 64-block periodic layout at small sizes (5..9 points per side).
+MB64_SMALL = cases.case_multiblock(cases.multiblock_sizes(seed=3, lo=5, hi=9), species=cases.synthetic_species(),
+                                   seed=3)
+
+
+@pytest.mark.parametrize("variant", ["l1", "split"])
+def test_multiblock64_small_fp64_matches_oracle(variant):
+    errs, status = compare(MB64_SMALL, "rk3", 2, "fp64", variant, 4)
+    assert status == 0
+    bad = {k: v for k, v in errs.items() if not v < 1e-10}
+    assert not bad, errs
+
+
+@pytest.mark.parametrize("variant", ["l1", "split"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_per_block_launches_equal_batched(precision, variant):
+    """One launch per block per kernel (the reference's granularity) gives
+    bit-identical states to the batched launch over all blocks."""
+    out = []
+    for mode in ("batched", "per_block"):
+        d = cc.Driver.from_case(MB64_SMALL, precision)
+        d.set_tuning(variant, 4)
+        d.set_launch_mode(mode)
+        d.initialize_computation()
+        d.simulate(2, "rk3", residual=True)
+        out.append(([d.field[b].get_state()[2] for b in range(len(MB64_SMALL["blocks"]))], d.residual()))
+        d.close()
+    for a, b in zip(out[0][0], out[1][0]):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(out[0][1], out[1][1])
 
 
 @pytest.mark.parametrize("name", mg.NAMES)
