@@ -40,9 +40,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--err-steps", type=int, default=100, help="steps of the mixed-vs-FP64 error check")
-    ap.add_argument("--workload", default="box128", choices=["box128", "multiblock64", "mixing_layer"],
+    ap.add_argument("--workload", default="box128",
+                    choices=["box128", "multiblock64", "mixing_layer", "box256_closure"],
                     help="box128: the headline 128^3 box; multiblock64: 64 uneven blocks, batched vs "
-                         "per-block; mixing_layer: 1024x512x4 precision study (FP64 / mixed / FP32)")
+                         "per-block; mixing_layer: 1024x512x4 precision study (FP64 / mixed / FP32); "
+                         "box256_closure: 256^3 box, exact transport vs the learned closure")
     ap.add_argument("--study-steps", default="100,1000,2000", help="mixing_layer: error snapshot steps")
     return ap.parse_args()
 
@@ -353,6 +355,66 @@ def run_mixing_layer(args):
     print(json.dumps(line), flush=True)
 
 
+def run_closure(args):
+    """256^3 box (the 128^3 workload's generator), mixed precision: stages
+    with the exact Wilke / constant-Schmidt transport against stages with the
+    learned closure on the tensor cores (exact fallback outside its hull);
+    throughput, fallback rate, closure accuracy on fresh states and the
+    difference of the two solutions."""
+    import torch
+    import combustioncodegpu_b200 as cc
+    from combustioncodegpu_b200 import cases, closure
+
+    sp = cases.synthetic_species()
+    n = 256
+    case = cases.case_box(n, species=sp, seed=1234)
+    w, report = closure.load()
+    res, states = {}, {}
+    for mode in ("exact", "closure"):
+        d = cc.Driver.from_case(case, "mixed")
+        if mode == "closure":
+            d.set_closure(w)
+            d.use_closure(True)
+        d.initialize_computation()
+        s = torch.cuda.ExternalStream(d.stream())
+        npts = d.info()["n_points"]
+        d.simulate(args.warmup)
+        d.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            e0.record(s)
+            d.simulate(args.steps)
+            e1.record(s)
+            e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        kt = d.time_kernels(1)
+        res[mode] = {"value": npts * 3 * args.steps / (ms / 1e3) / 1e6, "ms_per_step": ms / args.steps,
+                     "kernels": kt, "clocks": clk.summary(), "status": d.status(), "tuning": d.tuning()}
+        if mode == "closure":
+            n_eval, n_fb = d.closure_stats()
+            res[mode]["closure_points"] = n_eval
+            res[mode]["fallback_rate"] = n_fb / max(1, n_eval)
+            res[mode]["closure_accuracy_fresh_states"] = closure.validate(d, sp, n=200_000, seed=31)
+        states[mode] = d.field[0].get_state()[0]
+        d.close()
+    sl = lambda a: a.reshape(6, n + 4, n + 4, n + 4)[:, 2:-2, 2:-2, 2:-2].reshape(6, -1)
+    diff = field_errors(sl(states["closure"]), sl(states["exact"]))
+    c = res["closure"]
+    line = {"metric": METRIC, "value": c["value"], "unit": "Mcell-updates/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": c["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 fluxes + bf16 tensor-core transport closure + f64 conserved/Newton",
+            "data": "synthetic",
+            "config": {"workload": "box256_9sp_viscous_rk3_closure", "grid": "256^3 points, 2 mm periodic cube",
+                       "closure": "MLP (T, X_1..9) -> (mu, lambda, rhoD_1..9), 3x64 SiLU, BF16 tcgen05, "
+                                  "FP32 accumulate", "precision": "mixed",
+                       "l2": "inputs larger than L2 (no flush)", "graph": "one CUDA graph per step"},
+            "exact_transport": res["exact"], "closure": c,
+            "closure_over_exact": c["value"] / res["exact"]["value"],
+            "solution_difference_after_steps": diff,
+            "training": {k: report[k] for k in ("n_samples", "epochs", "seconds_train", "torch_model_rel_err")}}
+    print(json.dumps(line), flush=True)
+
+
 def cpu_baseline(args, n_threads, steps=1, n=64):
     """The oracle on the host cores: bounded sample of the workload (an
     n^3-point box with the same per-point work, `steps` RK3 steps)."""
@@ -405,9 +467,10 @@ def main():
             dist.destroy_process_group()
         return
 
-    if args.workload in ("multiblock64", "mixing_layer"):
+    if args.workload in ("multiblock64", "mixing_layer", "box256_closure"):
         if rank == 0:
-            (run_multiblock if args.workload == "multiblock64" else run_mixing_layer)(args)
+            {"multiblock64": run_multiblock, "mixing_layer": run_mixing_layer,
+             "box256_closure": run_closure}[args.workload](args)
         if dist:
             dist.destroy_process_group()
         return

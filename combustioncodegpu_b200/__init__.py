@@ -58,6 +58,12 @@ class CCInnerFace(ctypes.Structure):
                 ("src_tar", ctypes.c_int * 3), ("loop_dir", ctypes.c_int * 3), ("target_loop_dir", ctypes.c_int * 3)]
 
 
+class CCClosure(ctypes.Structure):
+    _fields_ = [(k, ctypes.POINTER(ctypes.c_float)) for k in
+                ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4", "out_mean", "out_scale")] + \
+               [(k, ctypes.c_double) for k in ("t_center", "t_scale", "t_min", "t_max")]
+
+
 class CCBc(ctypes.Structure):
     _fields_ = [("label", ctypes.c_int), ("kind", ctypes.c_int), ("thermal_type", ctypes.c_int),
                 ("pad", ctypes.c_int), ("t_wall", ctypes.c_double), ("density", ctypes.c_double),
@@ -99,6 +105,10 @@ EXPORTS = {
     "cc_tuning": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
     "cc_set_tuning": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "cc_set_launch_mode": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "cc_set_closure": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "cc_use_closure": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "cc_closure_stats": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+    "cc_eval_transport": ([ctypes.c_void_p, ctypes.c_int64, _dp, _dp, ctypes.c_int, _dp], ctypes.c_int),
     "cc_sync": ([ctypes.c_void_p], ctypes.c_int),
     "cc_residual_rms_noalloc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
                                 ctypes.c_int),
@@ -406,6 +416,38 @@ class Driver:
         """"batched": one launch per stage kernel over all blocks;
         "per_block": one launch per block per kernel (the reference's way)."""
         _check(self.lib.cc_set_launch_mode(self.ctx, {"batched": 0, "per_block": 1}[mode]))
+
+    def set_closure(self, weights):
+        """Upload a learned transport closure: a dict with w1, b1, ..., w4,
+        b4, out_mean, out_scale (float32 arrays) and t_center, t_scale,
+        t_min, t_max (see cc_b200.h, cc_closure)."""
+        keep = {k: np.ascontiguousarray(weights[k], dtype=np.float32)
+                for k in ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4", "out_mean", "out_scale")}
+        fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        m = CCClosure(*(fp(keep[k]) for k in ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4", "out_mean",
+                                              "out_scale")),
+                      float(weights["t_center"]), float(weights["t_scale"]), float(weights["t_min"]),
+                      float(weights["t_max"]))
+        _check(self.lib.cc_set_closure(self.ctx, ctypes.byref(m)))
+
+    def use_closure(self, on=True):
+        _check(self.lib.cc_use_closure(self.ctx, 1 if on else 0))
+
+    def closure_stats(self):
+        """(points evaluated by the closure kernel, exact fallbacks)."""
+        out = (ctypes.c_int64 * 2)()
+        _check(self.lib.cc_closure_stats(self.ctx, out))
+        return int(out[0]), int(out[1])
+
+    def eval_transport(self, T, Y, mode="exact"):
+        """(mu, lambda, rhoD_k) [2 + n_spec][n] of points (T [n], Y [n_spec][n])
+        by the exact FP64 kernel ("exact") or the closure kernel ("closure")."""
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        Y = np.ascontiguousarray(Y, dtype=np.float64)
+        out = np.empty((2 + self.n_spec, T.size))
+        _check(self.lib.cc_eval_transport(self.ctx, T.size, _ptr(T), _ptr(Y), {"exact": 0, "closure": 1}[mode],
+                                          _ptr(out)))
+        return out
 
     def close(self):
         if getattr(self, "ctx", None):

@@ -1,0 +1,199 @@
+"""Learned transport closure: training data, training and validation.
+
+The closure replaces the Wilke / constant-Schmidt transport evaluation
+(Transport.cu:43-96) by an MLP (T, X_1..X_n) -> (log mu, log lambda,
+log rhoD_1..rhoD_n) evaluated on the tensor cores (csrc/closure.cuh); points
+outside the training hull in T take the exact transport.
+
+Training data: T ~ U[t_min, t_max], X ~ Dirichlet(alpha * 1_n), Y from X;
+targets are the library's own exact FP64 transport of those points
+(cc_eval_transport, mode 0).  The network is trained with the arithmetic of
+the kernel: inputs as BF16 (hi, lo) pairs, BF16 weights and BF16 hidden
+activations (rounding with a straight-through gradient), FP32 accumulation,
+FP32 biases; the loss is the mean squared error of the log properties, i.e.
+of the relative error.  Training runs on the GPU with PyTorch (an offline
+step, not the hot path); the result is a dict that Driver.set_closure takes.
+
+  python -m combustioncodegpu_b200.closure --out closure_weights.npz
+"""
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+HIDDEN = 64
+T_MIN, T_MAX = 300.0, 2500.0
+T_CENTER, T_SCALE = 0.5 * (T_MIN + T_MAX), 0.5 * (T_MAX - T_MIN)
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "closure_weights.npz")
+
+
+def sample_states(n, species, seed, alpha=0.5, t_range=(T_MIN, T_MAX)):
+    """n random states: T [n], Y [ns][n], X [ns][n]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ns = species["n_spec"]
+    T = rng.uniform(t_range[0], t_range[1], n)
+    X = rng.dirichlet(np.full(ns, alpha), n).T
+    mw = np.asarray(species["mw"])[:, None]
+    Y = X * mw / (X * mw).sum(axis=0, keepdims=True)
+    return T, Y, X
+
+
+def mole_fractions(Y, mw):
+    x = Y / np.asarray(mw)[:, None]
+    return x / x.sum(axis=0, keepdims=True)
+
+
+def _bf16(x):
+    import torch
+    return x.to(torch.bfloat16).to(torch.float32)
+
+
+def _round_ste(x):
+    """BF16 rounding in the forward pass, identity gradient."""
+    return x + (_bf16(x) - x).detach()
+
+
+def features(T, X, torch_device="cpu"):
+    """Network inputs as the kernel forms them: [t_hi, t_lo, X_hi, X_lo],
+    each BF16, from t = (T - T_CENTER) / T_SCALE and the mole fractions (FP32)."""
+    import torch
+    t = ((torch.as_tensor(T, dtype=torch.float32, device=torch_device) - np.float32(T_CENTER))
+         * np.float32(1.0 / T_SCALE))
+    Xt = torch.as_tensor(X, dtype=torch.float32, device=torch_device)  # [ns][n]
+    t_hi = _bf16(t)
+    x_hi = _bf16(Xt)
+    return torch.cat([t_hi[None], _bf16(t - t_hi)[None], x_hi, _bf16(Xt - x_hi)], dim=0).T.contiguous()
+
+
+class ClosureNet:
+    """The closure MLP with the kernel's rounding points (torch, FP32 master)."""
+
+    def __init__(self, n_in, n_out, device, seed=0):
+        import torch
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        dims = [(n_in, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, n_out)]
+        self.params = []
+        for i, (a, b) in enumerate(dims):
+            w = torch.randn(b, a, generator=g) * (1.0 / np.sqrt(a)) * (0.5 if i == 3 else 1.0)
+            self.params += [w.to(device).requires_grad_(), torch.zeros(b, device=device).requires_grad_()]
+
+    def forward(self, x, quantized=True):
+        import torch
+        r = _round_ste if quantized else (lambda v: v)
+        h = x
+        for i in range(4):
+            w, b = self.params[2 * i], self.params[2 * i + 1]
+            h = r(h) @ r(w).T + b
+            if i < 3:
+                h = torch.nn.functional.silu(h)
+        return h
+
+    def export(self, out_mean, out_scale):
+        names = ["w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4"]
+        d = {k: p.detach().cpu().numpy().astype(np.float32) for k, p in zip(names, self.params)}
+        d.update({"out_mean": np.asarray(out_mean, np.float32), "out_scale": np.asarray(out_scale, np.float32),
+                  "t_center": T_CENTER, "t_scale": T_SCALE, "t_min": T_MIN, "t_max": T_MAX})
+        return d
+
+
+def train(driver, species, n_samples=2_000_000, n_val=200_000, epochs=60, batch=4096, lr=2e-3, seed=7,
+          device="cuda", log=print):
+    """Fit the closure to the exact transport of `driver`'s species tables.
+    Returns (weights dict, report dict)."""
+    import torch
+
+    t0 = time.time()
+    T, Y, X = sample_states(n_samples + n_val, species, seed)
+    tgt = np.log(driver.eval_transport(T, Y, "exact"))  # [2+ns][n]
+    t_data = time.time() - t0
+    ns = species["n_spec"]
+    n_in, n_out = 2 + 2 * ns, 2 + ns
+    mean = tgt[:, :n_samples].mean(axis=1)
+    scale = tgt[:, :n_samples].std(axis=1) + 1e-6
+    x_all = features(T, X, device)
+    y_all = torch.as_tensor(((tgt - mean[:, None]) / scale[:, None]).T, dtype=torch.float32, device=device)
+    sc = torch.as_tensor(scale, dtype=torch.float32, device=device)
+    xtr, ytr = x_all[:n_samples], y_all[:n_samples]
+    net = ClosureNet(n_in, n_out, device, seed)
+    opt = torch.optim.Adam(net.params, lr=lr)
+    steps = epochs * (n_samples // batch)
+    sched = torch.optim.lr_scheduler.OneCycleLR(opt, max_lr=lr, total_steps=steps, pct_start=0.05)
+    gen = torch.Generator(device=device).manual_seed(seed)
+    t1 = time.time()
+    for ep in range(epochs):
+        perm = torch.randperm(n_samples, device=device, generator=gen)
+        tot = 0.0
+        for b in range(n_samples // batch):
+            idx = perm[b * batch:(b + 1) * batch]
+            err = (net.forward(xtr[idx]) - ytr[idx]) * sc  # error of the log properties
+            loss = (err * err).mean()
+            opt.zero_grad(set_to_none=True)
+            loss.backward()
+            opt.step()
+            sched.step()
+            tot += float(loss.detach()) if b % 50 == 0 else 0.0
+        if ep % 10 == 0 or ep == epochs - 1:
+            log("epoch %d  loss(sampled) %.3e" % (ep, tot / max(1, (n_samples // batch) // 50)))
+    t_train = time.time() - t1
+    w = net.export(mean, scale)
+    with torch.no_grad():
+        o = net.forward(x_all[n_samples:]).cpu().numpy() * scale + mean  # torch model, log space
+    rel_torch = np.abs(np.expm1(o.T - tgt[:, n_samples:]))
+    report = {"n_samples": n_samples, "n_val": n_val, "epochs": epochs, "batch": batch, "seed": seed,
+              "seconds_data": t_data, "seconds_train": t_train,
+              "torch_model_rel_err": _err_summary(rel_torch)}
+    return w, report
+
+
+def _err_summary(rel):
+    """rel: [n_out][n] relative errors."""
+    worst = rel.max(axis=0)
+    return {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)), "max": float(rel.max()),
+            "frac_points_above_1e-3": float((worst > 1e-3).mean()),
+            "per_output_p99": [float(v) for v in np.percentile(rel, 99, axis=1)]}
+
+
+def validate(driver, species, n=200_000, seed=99):
+    """Relative error of the closure kernel (as uploaded to driver) against
+    the exact transport on fresh states inside the hull."""
+    T, Y, _ = sample_states(n, species, seed)
+    exact = driver.eval_transport(T, Y, "exact")
+    got = driver.eval_transport(T, Y, "closure")
+    return _err_summary(np.abs(got / exact - 1.0))
+
+
+def save(path, weights, report):
+    np.savez(path, report=json.dumps(report), **{k: np.asarray(v) for k, v in weights.items()})
+
+
+def load(path=DEFAULT_WEIGHTS):
+    z = np.load(path, allow_pickle=False)
+    w = {k: z[k] for k in z.files if k != "report"}
+    for k in ("t_center", "t_scale", "t_min", "t_max"):
+        w[k] = float(w[k])
+    return w, json.loads(str(z["report"]))
+
+
+def main():
+    import combustioncodegpu_b200 as cc
+    from combustioncodegpu_b200 import cases
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--samples", type=int, default=2_000_000)
+    ap.add_argument("--epochs", type=int, default=60)
+    args = ap.parse_args()
+    sp = cases.synthetic_species()
+    d = cc.Driver.from_case(cases.case_box(4, species=sp), "mixed")
+    w, report = train(d, sp, n_samples=args.samples, epochs=args.epochs)
+    d.set_closure(w)
+    report["kernel_rel_err"] = validate(d, sp)
+    d.close()
+    save(args.out, w, report)
+    print(json.dumps(report))
+
+
+if __name__ == "__main__":
+    main()

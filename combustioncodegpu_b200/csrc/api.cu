@@ -107,6 +107,9 @@ struct cc_ctx {
   bool tma_ok = false;            // tensor maps built (the TMA variant can run)
   int force_variant = -1;         // cc_set_tuning: -1 autotune, else the variant
   int force_kz = 0;               // cc_set_tuning: k-planes per tile, 0 = autotune
+  bool closure_set = false;       // cc_set_closure: learned transport closure uploaded
+  bool closure_on = false;        // cc_use_closure: stages take transport from the closure kernel
+  ClosureDev cl{};                // device weights, biases, normalisation, counters
   int kz = 1;                     // k-chunk of the stage tiles
   double tuned_ms = 0;            // stage-kernel time of the chosen configuration
   CUtensorMap *d_tmaps = nullptr; // [2][n_blocks]: primitive arenas P[0], P[1] per block
@@ -645,6 +648,7 @@ int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qou
   const int nt = (int)c->htiles.size();
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
   if (int r = launch_stage<T, NS>(c, a, pc, c->variant, nt)) return r;
+  if (c->closure_on) CK((Launch<T, NS>::props_mlp(a.Pn, a.Prn, c->N, &c->cl, c->d_status, c->chem, c->stream)));
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
   if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next)) return r;
@@ -739,6 +743,8 @@ int enqueue_step(cc_ctx *c, int scheme) {
   a.skip_dt = c->d_skip_dt;
   a.renorm_y = c->chem.ns > 0 && (c->renorm < 0 ? c->precision != CC_FP64 : c->renorm != 0);
   a.q32 = c->precision == CC_FP32;
+  a.closure = c->closure_on ? 1 : 0;
+  const bool dt_after = c->plan.has_wall || c->closure_on;  // global dt reduced after the halo
   if (scheme == CC_STEADY_EULER) {
     const int pc = c->cur, pn = 1 - c->cur;
     a.P = (const T *)c->P[pc], a.Pn = (T *)c->P[pn], a.Pr = (const T *)c->Pr[pc], a.Prn = (T *)c->Pr[pn];
@@ -758,12 +764,12 @@ int enqueue_step(cc_ctx *c, int scheme) {
     double *qout = st == 2 ? qa : qb;
     a.Qin = qin, a.Qn = qa, a.Qout = qout;
     a.a = A[st], a.b = Bc[st], a.local_dt = 0;
-    a.dt_next = (st == 2 && !c->plan.has_wall) ? c->d_dt_next : nullptr;
+    a.dt_next = (st == 2 && !dt_after) ? c->d_dt_next : nullptr;
     a.vel = st == 2 ? c->d_vel : nullptr;
     if (int r = stage_and_halo<T, NS>(c, a, pn, pc, qout, qin)) return r;
     c->cur = pn;
   }
-  if (c->plan.has_wall)
+  if (dt_after)
     CK((Launch<T, NS>::dt_reduce(c->chem, c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur],
                                  (const T *)c->Pr[c->cur], (const T *)c->G, c->N, c->n_int, c->d_dt_next,
                                  c->stream)));
@@ -1222,6 +1228,148 @@ int cc_set_tuning(cc_ctx *c, int variant, int kz) {
   if (r) return r;
   CK(cudaStreamSynchronize(c->stream));
   return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+uint16_t f2bf(float f) {  // round to nearest even
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)(u >> 16);  // inf / nan
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+// rows x cols FP32 row-major matrix -> BF16 operand of R rows x K columns
+void pack_operand(std::vector<uint16_t> &blob, int byte0, int R, int K, const float *w, int rows, int cols) {
+  for (int r = 0; r < rows; ++r)
+    for (int k = 0; k < cols; ++k) blob[(byte0 + mlp_off(R, r, k)) / 2] = f2bf(w[(size_t)r * cols + k]);
+  (void)K;
+}
+
+template <int NS>
+int eval_transport_ns(cc_ctx *c, int64_t n, const double *T, const double *Y, int mode, double *out) {
+  const int ns = c->chem.ns, np = 6 + ns, npr = 2 + ns;
+  cudaStream_t st = c->stream;
+  std::vector<double> h((size_t)np * n, 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    h[i] = 1.0;  // rho > 0 marks a point to evaluate
+    h[5 * n + i] = T[i];
+    for (int l = 0; l < ns; ++l) h[(6 + l) * n + i] = Y[(size_t)l * n + i];
+  }
+  std::vector<double> o((size_t)npr * n);
+  if (mode == 0) {
+    double *dP = nullptr, *dPr = nullptr;
+    CK(cudaMalloc(&dP, sizeof(double) * np * n));
+    CK(cudaMalloc(&dPr, sizeof(double) * npr * n));
+    CK(cudaMemcpyAsync(dP, h.data(), sizeof(double) * np * n, cudaMemcpyHostToDevice, st));
+    CK((Launch<double, NS>::props_all(c->chem, dP, dPr, n, st)));
+    CK(cudaMemcpyAsync(o.data(), dPr, sizeof(double) * npr * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    cudaFree(dP);
+    cudaFree(dPr);
+  } else {
+    std::vector<float> hf(h.begin(), h.end()), of((size_t)npr * n);
+    float *dP = nullptr, *dPr = nullptr;
+    unsigned *dst = nullptr;
+    CK(cudaMalloc(&dP, sizeof(float) * np * n));
+    CK(cudaMalloc(&dPr, sizeof(float) * npr * n));
+    CK(cudaMalloc(&dst, sizeof(unsigned)));
+    CK(cudaMemsetAsync(dst, 0, sizeof(unsigned), st));
+    CK(cudaMemcpyAsync(dP, hf.data(), sizeof(float) * np * n, cudaMemcpyHostToDevice, st));
+    CK((Launch<float, NS>::props_mlp(dP, dPr, n, &c->cl, dst, c->chem, st)));
+    unsigned flags = 0;
+    CK(cudaMemcpyAsync(of.data(), dPr, sizeof(float) * npr * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&flags, dst, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    cudaFree(dP);
+    cudaFree(dPr);
+    cudaFree(dst);
+    if (flags) return fail(CC_ERR_CUDA, "closure kernel reported status " + std::to_string(flags));
+    o.assign(of.begin(), of.end());
+  }
+  std::memcpy(out, o.data(), sizeof(double) * o.size());
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cc_set_closure(cc_ctx *c, const cc_closure *m) {
+  if (int r = check_ctx(c)) return r;
+  const int ns = c->chem.ns, n_in = 2 + 2 * ns, n_out = 2 + ns;
+  if (!m || !m->w1 || !m->b1 || !m->w2 || !m->b2 || !m->w3 || !m->b3 || !m->w4 || !m->b4 || !m->out_mean ||
+      !m->out_scale)
+    return fail(CC_ERR_ARG, "cc_set_closure: null pointer");
+  if (ns < 1 || n_in > kMlpIn || n_out > kMlpOut)
+    return fail(CC_ERR_ARG, "cc_set_closure: the closure supports 1 to 14 species");
+  if (!(m->t_scale > 0) || !(m->t_max > m->t_min)) return fail(CC_ERR_ARG, "cc_set_closure: bad normalisation");
+  std::vector<uint16_t> blob(kMlpWBytes / 2, 0);
+  pack_operand(blob, 0, kMlpH, kMlpIn, m->w1, kMlpH, n_in);
+  pack_operand(blob, kMlpW1, kMlpH, kMlpH, m->w2, kMlpH, kMlpH);
+  pack_operand(blob, kMlpW1 + kMlpW2, kMlpH, kMlpH, m->w3, kMlpH, kMlpH);
+  pack_operand(blob, kMlpW1 + 2 * kMlpW2, kMlpOut, kMlpH, m->w4, n_out, kMlpH);
+  std::vector<float> bias(kMlpBias, 0.0f);
+  for (int i = 0; i < kMlpH; ++i) bias[i] = m->b1[i], bias[kMlpH + i] = m->b2[i], bias[2 * kMlpH + i] = m->b3[i];
+  for (int i = 0; i < n_out; ++i) bias[3 * kMlpH + i] = m->b4[i];
+  if (c->stream) CK(cudaStreamSynchronize(c->stream));
+  if (!c->cl.w) {
+    void *p = nullptr;
+    CK(cudaMalloc(&p, kMlpWBytes + sizeof(float) * kMlpBias + 2 * sizeof(unsigned long long)));
+    c->allocs.push_back(p);
+    c->cl.w = p;
+    c->cl.b = reinterpret_cast<const float *>(static_cast<unsigned char *>(p) + kMlpWBytes);
+    c->cl.counts = reinterpret_cast<unsigned long long *>(static_cast<unsigned char *>(p) + kMlpWBytes +
+                                                          sizeof(float) * kMlpBias);
+  }
+  CK(cudaMemcpy(const_cast<void *>(c->cl.w), blob.data(), kMlpWBytes, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(const_cast<float *>(c->cl.b), bias.data(), sizeof(float) * kMlpBias, cudaMemcpyHostToDevice));
+  CK(cudaMemset(c->cl.counts, 0, 2 * sizeof(unsigned long long)));
+  for (int i = 0; i < kMlpOut; ++i) {
+    c->cl.out_mean[i] = i < n_out ? m->out_mean[i] : 0.0f;
+    c->cl.out_scale[i] = i < n_out ? m->out_scale[i] : 0.0f;
+  }
+  c->cl.t_center = (float)m->t_center;
+  c->cl.t_inv_scale = (float)(1.0 / m->t_scale);
+  c->cl.t_min = (float)m->t_min;
+  c->cl.t_max = (float)m->t_max;
+  c->closure_set = true;
+  destroy_graphs(c);
+  return 0;
+}
+
+int cc_use_closure(cc_ctx *c, int on) {
+  if (int r = check_ctx(c)) return r;
+  if (on && !c->closure_set) return fail(CC_ERR_STATE, "cc_use_closure: no closure set (cc_set_closure)");
+  c->closure_on = on != 0;
+  destroy_graphs(c);
+  return 0;
+}
+
+int cc_closure_stats(cc_ctx *c, int64_t out[2]) {
+  if (int r = check_ctx(c)) return r;
+  if (!out) return fail(CC_ERR_ARG, "null pointer");
+  out[0] = out[1] = 0;
+  if (!c->cl.counts) return 0;
+  if (c->stream) CK(cudaStreamSynchronize(c->stream));
+  unsigned long long h[2];
+  CK(cudaMemcpy(h, c->cl.counts, sizeof h, cudaMemcpyDeviceToHost));
+  out[0] = (int64_t)h[0], out[1] = (int64_t)h[1];
+  return 0;
+}
+
+int cc_eval_transport(cc_ctx *c, int64_t n, const double *T, const double *Y, int mode, double *out) {
+  if (int r = check_ctx(c)) return r;
+  if (n <= 0 || !T || !out || (c->chem.ns > 0 && !Y)) return fail(CC_ERR_ARG, "cc_eval_transport: bad arguments");
+  if (mode != 0 && mode != 1) return fail(CC_ERR_ARG, "cc_eval_transport: mode must be 0 (exact) or 1 (closure)");
+  if (mode == 1 && !c->closure_set) return fail(CC_ERR_STATE, "cc_eval_transport: no closure set");
+  if (c->chem.ns == 0) return fail(CC_ERR_ARG, "cc_eval_transport: needs a mixture (n_spec > 0)");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CC_ERR_NODEVICE, "no CUDA device");
+  return c->chem.ns == 9 ? eval_transport_ns<9>(c, n, T, Y, mode, out) : eval_transport_ns<-1>(c, n, T, Y, mode, out);
 }
 
 int cc_set_launch_mode(cc_ctx *c, int per_block) {

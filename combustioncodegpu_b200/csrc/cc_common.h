@@ -44,6 +44,35 @@ struct ChemParams {
   SpecTables<float> f;
 };
 
+#if defined(__CUDACC__)
+#define CCB_HD __host__ __device__
+#else
+#define CCB_HD
+#endif
+
+// Learned transport closure (closure.cuh): tile of 128 points, 3 hidden
+// layers of 64, inputs padded to 32 (t and X_k as BF16 hi/lo pairs), outputs
+// padded to 16; BF16 weights in the MMA operand layout (W1 [64 x 32],
+// W2, W3 [64 x 64], W4 [16 x 64]), FP32 biases.
+constexpr int kMlpRows = 128, kMlpH = 64, kMlpIn = 32, kMlpOut = 16;
+constexpr int kMlpW1 = kMlpH * kMlpIn * 2, kMlpW2 = kMlpH * kMlpH * 2, kMlpW4 = kMlpOut * kMlpH * 2;
+constexpr int kMlpWBytes = kMlpW1 + 2 * kMlpW2 + kMlpW4;  // 22528
+constexpr int kMlpBias = 3 * kMlpH + kMlpOut;              // 208 floats
+constexpr int kMlpXBytes = kMlpRows * kMlpIn * 2, kMlpHBytes = kMlpRows * kMlpH * 2;
+
+// Byte offset of element (r, k) of an R-row, K-major BF16 operand without
+// swizzle: 8-row x 16-byte core matrices, 8-row groups 128 bytes apart, the
+// core matrices along K 16R bytes apart.
+CCB_HD constexpr int mlp_off(int R, int r, int k) { return (k / 8) * 16 * R + 16 * r + 2 * (k % 8); }
+
+struct ClosureDev {
+  const void *w;                        // kMlpWBytes of BF16 weights (16-byte aligned)
+  const float *b;                       // kMlpBias
+  float out_mean[kMlpOut], out_scale[kMlpOut];
+  float t_center, t_inv_scale, t_min, t_max;
+  unsigned long long *counts;           // [0] points evaluated, [1] exact fallbacks
+};
+
 // One block of the multiblock grid in the concatenated field arena.
 struct BlockInfo {
   int mx, my, mz, g;
@@ -109,6 +138,7 @@ struct StageArgs {
   int local_dt;              // 1: per-point time step of the current state
   int renorm_y;              // 1: renormalise Y_k to sum 1
   int q32;                   // 1: full-FP32 precision (conserved variables rounded to FP32, FP32 Newton)
+  int closure;               // 1: transport of the new state comes from the learned closure kernel (not here)
   // split variant (stage_split.cuh): face fluxes [3][n_var][N] (face d of
   // point p lies between p and p + e_d), the tiles of the minus-side face
   // layers (i, j or k = -1; direction in Tile::pad0), regular tile count

@@ -1,9 +1,12 @@
 // Definitions of the templated launchers (included by inst_*.cu only).
 #pragma once
+#include <algorithm>
+
 #include "launch.h"
 #include "stage.cuh"
 #include "stage_tma.cuh"
 #include "stage_split.cuh"
+#include "closure.cuh"
 
 namespace ccb {
 
@@ -42,6 +45,22 @@ cudaError_t Launch<T, NS>::update(const StageArgs<T> &a, const ChemParams &C, in
   if (n_tiles <= 0) return cudaSuccess;
   k_update<T, NS><<<n_tiles, dim3(kTX, kTY), update_smem(), s>>>(a, C);
   return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::props_mlp(const T *P, T *Pr, int64_t N, const void *cl, unsigned *status,
+                                     const ChemParams &C, cudaStream_t s) {
+  if constexpr (NS == 0) {
+    return cudaErrorInvalidValue;  // the closure is for mixtures
+  } else {
+    if (N <= 0) return cudaSuccess;
+    int dev = 0, n_sm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t tiles = (N + kMlpRows - 1) / kMlpRows;
+    const int grid = (int)std::min<int64_t>(tiles, (int64_t)n_sm * 4);
+    k_props_mlp<T, NS><<<grid, kMlpRows, kMlpSmem, s>>>(P, Pr, N, *static_cast<const ClosureDev *>(cl), status, C);
+    return cudaGetLastError();
+  }
 }
 
 template <typename T, int NS>

@@ -309,6 +309,7 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
 #pragma unroll
   for (int l = 0; l < A; ++l)
     if (l < ns) Yt[l] = T(Yd[l]), Pn[(6 + l) * N + p] = Yt[l];
+  if (a.closure) return;  // transport and the time step follow from the closure kernel
   T mu, lam, rd[A], gam, c;
   point_props<T, NS>(C, rec, T(temp), Yt, mu, lam, rd, gam, c);
   T* Prn = a.Prn;

@@ -194,6 +194,39 @@ int cc_set_tuning(cc_ctx *ctx, int variant, int kz);
  * the reference's granularity (Driver.cu:144-177 launches per block), kept for
  * comparison.  Results are identical; takes effect at the next cc_step. */
 int cc_set_launch_mode(cc_ctx *ctx, int per_block);
+/* Learned transport closure (a22: absent in the reference, which always
+ * evaluates Transport.cu:43-96).  An MLP maps (T, X_1..X_n) to
+ * (log mu, log lambda, log rhoD_1..rhoD_n): inputs t = (T - t_center)/t_scale
+ * and the mole fractions X_k, each fed as a BF16 pair (hi, value - hi), in the
+ * order [t_hi, t_lo, X_hi[n], X_lo[n]]; three hidden layers of 64 SiLU units;
+ * output o_j gives property_j = exp(o_j * out_scale[j] + out_mean[j]).
+ * Weights are row-major (output, input) FP32 and are stored as BF16 on the
+ * device; biases stay FP32; the tensor cores accumulate in FP32.  Points with
+ * T outside [t_min, t_max] (the training hull) or a mole fraction of at least
+ * 0.998 (where the exact rhoD_k switches branch) take the exact transport.
+ * Supports 1..14 species. */
+typedef struct cc_closure {
+  const float *w1, *b1;            /* [64][2 + 2 n_spec], [64] */
+  const float *w2, *b2;            /* [64][64], [64] */
+  const float *w3, *b3;            /* [64][64], [64] */
+  const float *w4, *b4;            /* [2 + n_spec][64], [2 + n_spec] */
+  const float *out_mean, *out_scale; /* [2 + n_spec] */
+  double t_center, t_scale;
+  double t_min, t_max;
+} cc_closure;
+/* Copies a closure to the device (any time after cc_create). */
+int cc_set_closure(cc_ctx *ctx, const cc_closure *closure);
+/* Stages take the transport properties of the new state from the closure
+ * (1) or from the exact Wilke / constant-Schmidt evaluation (0, default).
+ * With the closure on, the global time step is reduced after the halo. */
+int cc_use_closure(cc_ctx *ctx, int on);
+/* Points the closure kernel evaluated and, of those, how many took the
+ * exact fallback, since cc_set_closure. */
+int cc_closure_stats(cc_ctx *ctx, int64_t out[2]);
+/* Transport properties of n points (host arrays): T [n], Y [n_spec][n] ->
+ * out [2 + n_spec][n] = (mu, lambda, rhoD_k), by the exact FP64 evaluation
+ * (mode 0) or by the closure kernel (mode 1).  Needs a device, not cc_init. */
+int cc_eval_transport(cc_ctx *ctx, int64_t n, const double *T, const double *Y, int mode, double *out);
 /* Synchronises the context's stream. */
 int cc_sync(cc_ctx *ctx);
 
