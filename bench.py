@@ -39,7 +39,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128)
-    ap.add_argument("--err-steps", type=int, default=100, help="steps of the mixed-vs-FP64 error check")
+    ap.add_argument("--err-steps", type=int, default=1000, help="steps of the mixed-vs-FP64 error check")
     ap.add_argument("--workload", default="box128",
                     choices=["box128", "multiblock64", "mixing_layer", "box256_closure"],
                     help="box128: the headline 128^3 box; multiblock64: 64 uneven blocks, batched vs "

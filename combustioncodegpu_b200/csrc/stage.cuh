@@ -569,23 +569,59 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
   double q[5 + A];
   bool props_copy = false;
   RefPtrs<T> ra = resolve(a, nd.a);
+  // every field is loaded into registers before the first store: the stores
+  // may alias the sources as far as the compiler knows, and interleaving them
+  // would serialise one memory round trip per field
   if (nd.op == kHaloCopy) {
-    for (int f = 0; f < 6 + ns; ++f) a.sP[f * S + o] = ra.P[f * ra.stride + ra.idx];
-    for (int f = 0; f < 2 + ns; ++f) a.sPr[f * S + o] = ra.Pr[f * ra.stride + ra.idx];
-    for (int f = 0; f < nv; ++f) a.sQ[f * S + o] = ra.Q[f * ra.stride + ra.idx];
+    T vP[6 + A], vPr[2 + A];
+    double vQ[5 + A];
+#pragma unroll
+    for (int f = 0; f < 6 + A; ++f)
+      if (f < 6 + ns) vP[f] = ra.P[f * ra.stride + ra.idx];
+#pragma unroll
+    for (int f = 0; f < 2 + A; ++f)
+      if (f < 2 + ns) vPr[f] = ra.Pr[f * ra.stride + ra.idx];
+#pragma unroll
+    for (int f = 0; f < 5 + A; ++f)
+      if (f < nv) vQ[f] = ra.Q[f * ra.stride + ra.idx];
+#pragma unroll
+    for (int f = 0; f < 6 + A; ++f)
+      if (f < 6 + ns) a.sP[f * S + o] = vP[f];
+#pragma unroll
+    for (int f = 0; f < 2 + A; ++f)
+      if (f < 2 + ns) a.sPr[f * S + o] = vPr[f];
+#pragma unroll
+    for (int f = 0; f < 5 + A; ++f)
+      if (f < nv) a.sQ[f * S + o] = vQ[f];
     return;
   }
   if (nd.op == kHaloAvg) {
     RefPtrs<T> rb = resolve(a, nd.b);
+    T xa[6 + A], xb[6 + A], vPr[2 + A];
+    double qa[5 + A], qb[5 + A];
+#pragma unroll
+    for (int f = 0; f < 6 + A; ++f)
+      if (f < 6 + ns) xa[f] = ra.P[f * ra.stride + ra.idx], xb[f] = rb.P[f * rb.stride + rb.idx];
+#pragma unroll
+    for (int f = 0; f < 5 + A; ++f)
+      if (f < nv) qa[f] = ra.Q[f * ra.stride + ra.idx], qb[f] = rb.Q[f * rb.stride + rb.idx];
+#pragma unroll
+    for (int f = 0; f < 2 + A; ++f)
+      if (f < 2 + ns) vPr[f] = ra.Pr[f * ra.stride + ra.idx];
     bool same = true;
-    for (int f = 0; f < 6 + ns; ++f) {
-      const T x = ra.P[f * ra.stride + ra.idx], y = rb.P[f * rb.stride + rb.idx];
-      same = same && (x == y);
-      a.sP[f * S + o] = T(0.5) * (y + x);
-    }
-    for (int f = 0; f < nv; ++f) a.sQ[f * S + o] = 0.5 * (rb.Q[f * rb.stride + rb.idx] + ra.Q[f * ra.stride + ra.idx]);
+#pragma unroll
+    for (int f = 0; f < 6 + A; ++f)
+      if (f < 6 + ns) {
+        same = same && (xa[f] == xb[f]);
+        a.sP[f * S + o] = T(0.5) * (xb[f] + xa[f]);
+      }
+#pragma unroll
+    for (int f = 0; f < 5 + A; ++f)
+      if (f < nv) a.sQ[f * S + o] = 0.5 * (qb[f] + qa[f]);
     if (same) {
-      for (int f = 0; f < 2 + ns; ++f) a.sPr[f * S + o] = ra.Pr[f * ra.stride + ra.idx];
+#pragma unroll
+      for (int f = 0; f < 2 + A; ++f)
+        if (f < 2 + ns) a.sPr[f * S + o] = vPr[f];
       return;
     }
     // averaged state: recompute its transport properties below
@@ -691,9 +727,27 @@ __global__ void k_halo_copies(const HaloArgs<T> a, const __grid_constant__ ChemP
   if (e < a.end) {
     const HaloCopy c = a.copies[e];
     const RefPtrs<T> r = resolve(a, c.src);
-    for (int f = 0; f < np; ++f) a.P[f * a.N + c.dst] = r.P[f * r.stride + r.idx];
-    for (int f = 0; f < npr; ++f) a.Pr[f * a.N + c.dst] = r.Pr[f * r.stride + r.idx];
-    for (int f = 0; f < nq; ++f) a.Q[f * a.N + c.dst] = r.Q[f * r.stride + r.idx];
+    // all loads before the first store (see k_halo_nodes)
+    T vP[6 + A], vPr[2 + A];
+    double vQ[5 + A];
+#pragma unroll
+    for (int f = 0; f < 6 + A; ++f)
+      if (f < np) vP[f] = r.P[f * r.stride + r.idx];
+#pragma unroll
+    for (int f = 0; f < 2 + A; ++f)
+      if (f < npr) vPr[f] = r.Pr[f * r.stride + r.idx];
+#pragma unroll
+    for (int f = 0; f < 5 + A; ++f)
+      if (f < nq) vQ[f] = r.Q[f * r.stride + r.idx];
+#pragma unroll
+    for (int f = 0; f < 6 + A; ++f)
+      if (f < np) a.P[f * a.N + c.dst] = vP[f];
+#pragma unroll
+    for (int f = 0; f < 2 + A; ++f)
+      if (f < npr) a.Pr[f * a.N + c.dst] = vPr[f];
+#pragma unroll
+    for (int f = 0; f < 5 + A; ++f)
+      if (f < nq) a.Q[f * a.N + c.dst] = vQ[f];
     if (a.dt_next && (c.src.pad & 1)) {
       const int64_t p = c.dst, N = a.N;
       T Y[A], gam, cs;
