@@ -110,6 +110,7 @@ struct cc_ctx {
   bool closure_set = false;       // cc_set_closure: learned transport closure uploaded
   bool closure_on = false;        // cc_use_closure: stages take transport from the closure kernel
   ClosureDev cl{};                // device weights, biases, normalisation, counters
+  double *d_gcl = nullptr;        // [3][N] geometric term of the gauge-pressure momentum fluxes
   int kz = 1;                     // k-chunk of the stage tiles
   double tuned_ms = 0;            // stage-kernel time of the chosen configuration
   CUtensorMap *d_tmaps = nullptr; // [2][n_blocks]: primitive arenas P[0], P[1] per block
@@ -215,10 +216,12 @@ int copy_field_d2h(cc_ctx *c, const HostBlock &b, const double *dev_field, doubl
 }
 
 // T-precision field f of arena `src` -> FP64 tmp64
-int field_to64(cc_ctx *c, const void *src, int f) {
+int field_to64(cc_ctx *c, const void *src, int f, double shift = 0.0) {
   if (c->precision == CC_FP64) {
     CK(cudaMemcpyAsync(c->tmp64, (const double *)src + (int64_t)f * c->N, sizeof(double) * c->N,
                        cudaMemcpyDeviceToDevice, c->stream));
+  } else if (shift != 0.0) {
+    CK(launch_convert_f2d_shift((const float *)src + (int64_t)f * c->N, c->tmp64, c->N, shift, c->stream));
   } else {
     CK(launch_convert_f2d((const float *)src + (int64_t)f * c->N, c->tmp64, c->N, c->stream));
   }
@@ -400,6 +403,10 @@ int setup_device(cc_ctx *c) {
   }
   if (dev_alloc(c, &c->G, E * N * 10)) return CC_ERR_CUDA;
   if (dev_alloc(c, &c->faces, E * N * 3 * nv_of(c))) return CC_ERR_CUDA;
+  if (c->precision != CC_FP64) {
+    if (dev_alloc(c, &p, sizeof(double) * 3 * N)) return CC_ERR_CUDA;
+    c->d_gcl = (double *)p;
+  }
   build_edge_tiles(c);
   if (dev_alloc(c, &p, sizeof(Tile) * std::max<size_t>(1, c->hedges.size()))) return CC_ERR_CUDA;
   c->d_edges = (Tile *)p;
@@ -527,6 +534,11 @@ int derive_state(cc_ctx *c) {
   CK((Launch<T, NS>::cv_from_bv(c->chem, c->stage64, c->Q[0], N, c->d_vel, c->stream)));
   CK(cudaMemcpyAsync(c->Q[1], c->Q[0], sizeof(double) * N * nv_of(c), cudaMemcpyDeviceToDevice, c->stream));
   if (int r = from64(c, c->stage64, c->P[0], N * np_of(c))) return r;
+  if (c->chem.p_ref != 0.0) {  // the pressure field is stored as p - p_ref
+    CK(launch_convert_d2f_shift(c->stage64 + 4 * N, (float *)c->P[0] + 4 * N, N, c->chem.p_ref, c->stream));
+    CK((Launch<T, NS>::gcl(c->d_blocks, (int)c->hblocks.size(), (const T *)c->G, N, c->n_int, c->d_gcl,
+                           c->stream)));
+  }
   CK((Launch<T, NS>::props_all(c->chem, (const T *)c->P[0], (T *)c->Pr[0], N, c->stream)));
   CK(cudaMemcpyAsync(c->P[1], c->P[0], c->elem * N * np_of(c), cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->Pr[1], c->Pr[0], c->elem * N * npr_of(c), cudaMemcpyDeviceToDevice, c->stream));
@@ -744,6 +756,7 @@ int enqueue_step(cc_ctx *c, int scheme) {
   a.renorm_y = c->chem.ns > 0 && (c->renorm < 0 ? c->precision != CC_FP64 : c->renorm != 0);
   a.q32 = c->precision == CC_FP32;
   a.closure = c->closure_on ? 1 : 0;
+  a.gcl = c->chem.p_ref != 0.0 ? c->d_gcl : nullptr;
   const bool dt_after = c->plan.has_wall || c->closure_on;  // global dt reduced after the halo
   if (scheme == CC_STEADY_EULER) {
     const int pc = c->cur, pn = 1 - c->cur;
@@ -854,6 +867,7 @@ int cc_create(const cc_params *params, cc_ctx **out) {
   c->chem.Pr = params->prandtl_number;
   c->chem.cfl = params->cfl;
   c->chem.Sc = params->n_spec > 0 ? params->schmidt_number : 1.0;
+  c->chem.p_ref = 0.0;  // set at the first cc_init for the FP32 bulk precisions
   fill_tables(c->chem.d, params);
   fill_tables(c->chem.f, params);
   *out = c;
@@ -991,6 +1005,16 @@ int cc_init(cc_ctx *c, int precision) {
       c->own_stream = true;
     }
     c->precision = precision;
+    // gauge pressure reference of the FP32 primitives: the mean initial
+    // pressure of the first block, representable in FP32 (0 for FP64)
+    c->chem.p_ref = 0.0;
+    if (precision != CC_FP64) {
+      const std::vector<double> &bv = c->pend_bv[0];
+      const size_t ng = bv.size() / 6;
+      double sum = 0;
+      for (size_t i = 0; i < ng; ++i) sum += bv[4 * ng + i];
+      c->chem.p_ref = (double)(float)(sum / (double)std::max<size_t>(1, ng));
+    }
     if (int r = setup_device(c)) return r;
     for (size_t b = 0; b < c->blocks.size(); ++b) {
       if (int r = copy_fields_h2d(c, c->blocks[b], c->pend_bv[b].data(), c->stage64, 6)) return r;
@@ -1065,7 +1089,7 @@ int cc_get_state(cc_ctx *c, int block, double *bv, double *yk, double *cv) {
   const HostBlock &b = c->blocks[block];
   const int64_t ng = ng_user(b);
   for (int f = 0; f < 6 && bv; ++f) {
-    if (int r = field_to64(c, c->P[c->cur], f)) return r;
+    if (int r = field_to64(c, c->P[c->cur], f, f == 4 ? c->chem.p_ref : 0.0)) return r;  // gauge pressure
     if (int r = copy_field_d2h(c, b, c->tmp64, bv + f * ng)) return r;
   }
   for (int l = 0; l < c->chem.ns && yk; ++l) {

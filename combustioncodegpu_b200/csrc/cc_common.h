@@ -40,6 +40,10 @@ struct ChemParams {
   int reconstruction;  // 2 = MUSCL, else first order
   int viscous;         // 1 = second-order central viscous fluxes
   double Pr, cfl, Sc;
+  // gauge pressure of the FP32 primitives: the arena stores p - p_ref (0 in
+  // the FP64 path), and the momentum face fluxes carry p - p_ref, so that
+  // FP32 rounding acts on the pressure variations, not on ~1e5 Pa
+  double p_ref;
   SpecTables<double> d;
   SpecTables<float> f;
 };
@@ -139,6 +143,7 @@ struct StageArgs {
   int renorm_y;              // 1: renormalise Y_k to sum 1
   int q32;                   // 1: full-FP32 precision (conserved variables rounded to FP32, FP32 Newton)
   int closure;               // 1: transport of the new state comes from the learned closure kernel (not here)
+  const double *gcl;         // [3][N]: sum over directions of k(+) - k(-) per point (p_ref != 0), else null
   // split variant (stage_split.cuh): face fluxes [3][n_var][N] (face d of
   // point p lies between p and p + e_d), the tiles of the minus-side face
   // layers (i, j or k = -1; direction in Tile::pad0), regular tile count

@@ -64,6 +64,17 @@ cudaError_t Launch<T, NS>::props_mlp(const T *P, T *Pr, int64_t N, const void *c
 }
 
 template <typename T, int NS>
+cudaError_t Launch<T, NS>::gcl(const BlockInfo *blocks, int nblocks, const T *G, int64_t N, int64_t n_interior,
+                               double *out, cudaStream_t s) {
+  const int tpb = 256;
+  int64_t nb = (n_interior + tpb - 1) / tpb;
+  if (nb > 148 * 16) nb = 148 * 16;
+  if (nb < 1) return cudaSuccess;
+  k_gcl<T><<<(unsigned)nb, tpb, 0, s>>>(blocks, nblocks, G, N, n_interior, out);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
 cudaError_t Launch<T, NS>::configure() {
   cudaError_t e = cudaFuncSetAttribute(k_stage<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem());
   if (e != cudaSuccess) return e;

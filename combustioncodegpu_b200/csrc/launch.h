@@ -25,6 +25,9 @@ struct Launch {
   // learned transport closure (closure.cuh) over every arena point; cl is a ClosureDev
   static cudaError_t props_mlp(const T *P, T *Pr, int64_t N, const void *cl, unsigned *status, const ChemParams &C,
                                cudaStream_t s);
+  // geometric term of the gauge-pressure momentum fluxes (k_gcl)
+  static cudaError_t gcl(const BlockInfo *blocks, int nblocks, const T *G, int64_t N, int64_t n_interior,
+                         double *out, cudaStream_t s);
   static cudaError_t halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   static cudaError_t halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   static cudaError_t cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, double *vel,
@@ -45,6 +48,9 @@ CCB_DECLARE(float, -1)
 #undef CCB_DECLARE
 
 // Non-templated helpers (misc.cu).
+// dst = (float)(src - shift), dst = (double)src + shift (the gauge pressure field)
+cudaError_t launch_convert_d2f_shift(const double *src, float *dst, int64_t n, double shift, cudaStream_t s);
+cudaError_t launch_convert_f2d_shift(const float *src, double *dst, int64_t n, double shift, cudaStream_t s);
 cudaError_t launch_convert_d2f(const double *src, float *dst, int64_t n, cudaStream_t s);
 cudaError_t launch_convert_f2d(const float *src, double *dst, int64_t n, cudaStream_t s);
 cudaError_t launch_dt_finalize(double *dt, unsigned long long *dt_next, unsigned *status, double *dt_hist,

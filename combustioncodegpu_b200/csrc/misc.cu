@@ -27,6 +27,28 @@ cudaError_t launch_convert_f2d(const float *src, double *dst, int64_t n, cudaStr
   return cudaGetLastError();
 }
 
+__global__ void k_convert_d2f_shift(const double *src, float *dst, int64_t n, double shift) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (float)(src[i] - shift);
+}
+
+__global__ void k_convert_f2d_shift(const float *src, double *dst, int64_t n, double shift) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (double)src[i] + shift;
+}
+
+cudaError_t launch_convert_d2f_shift(const double *src, float *dst, int64_t n, double shift, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_convert_d2f_shift<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, dst, n, shift);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_convert_f2d_shift(const float *src, double *dst, int64_t n, double shift, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_convert_f2d_shift<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, dst, n, shift);
+  return cudaGetLastError();
+}
+
 // dt <- dt_next (when a candidate was reduced), dt_next <- +inf; the step's
 // dt is appended to the history slot.
 __global__ void k_dt_finalize(double *dt, unsigned long long *dt_next, unsigned *status, double *dt_hist) {

@@ -270,6 +270,35 @@ __device__ __forceinline__ T minmod(T a, T b) {
   return (a > T(0) && b > T(0)) ? m : ((a < T(0) && b < T(0)) ? -m : T(0));
 }
 
+// AUSM+ pressure splitting P+(M) = (M+1)^2 (2-M)/4 + a M (M^2-1)^2 and
+// P-(M) = (M-1)^2 (2+M)/4 - a M (M^2-1)^2 for |M| <= 1, 1 / 0 beyond, with
+// P+(M) + P-(M) = 1.  Returns P+(ml) + P-(mr) - 1 without the cancellation of
+// forming the sum: in the subsonic case it is P+(ml) - P+(mr) = (ml - mr) x
+// the divided difference of P+(M) = 1/2 + 3M/4 - M^3/4 + a (M^5 - 2M^3 + M).
+template <typename T>
+__device__ __forceinline__ T ausm_pressure_defect(T ml, T mr, T a) {
+  auto p_plus = [&](T m) {
+    const T q = m * m - T(1);
+    return (m + T(1)) * (m + T(1)) * (T(2) - m) * T(0.25) + a * m * q * q;
+  };
+  auto p_minus = [&](T m) {
+    const T q = m * m - T(1);
+    return (m - T(1)) * (m - T(1)) * (T(2) + m) * T(0.25) - a * m * q * q;
+  };
+  const bool sl = !(fabs(ml) > T(1)), sr = !(fabs(mr) > T(1));
+  if (sl && sr) {
+    const T x2 = ml * ml, y2 = mr * mr, xy = ml * mr;
+    const T s2 = x2 + xy + y2;
+    const T s4 = x2 * x2 + x2 * xy + xy * xy + xy * y2 + y2 * y2;
+    return (ml - mr) * (T(0.75) - T(0.25) * s2 + a * (s4 - T(2) * s2 + T(1)));
+  }
+  if (!sl) {                                        // P+(ml) is 1 or 0
+    if (ml > T(0)) return sr ? p_minus(mr) : (mr < T(0) ? T(1) : T(0));
+    return sr ? -p_plus(mr) : (mr < T(0) ? T(0) : T(-1));
+  }
+  return mr < T(0) ? p_plus(ml) : -p_minus(ml);     // P-(mr) is 1 or 0
+}
+
 // MUSCL (kappa = 1/3, minmod) or first-order states at the face between
 // points 1 and 2 of v[0..3], face thermodynamics, then AUSM+.
 // v[t][0..4] = rho,u,v,w,p ; v[t][5+l] = Y_l.  F receives n_var values.
@@ -302,12 +331,15 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T *rec,
     for (int l = 0; l < NV; ++l)
       if (l < nv) L[l] = v[1][l], R[l] = v[2][l];
   }
+  // L[4], R[4] hold the gauge pressure p - p_ref (p_ref = 0 in FP64)
+  const T pref = T(C.p_ref);
+  const T pl = L[4] + pref, pr = R[4] + pref;
   T el = T(0.5) * (L[1] * L[1] + L[2] * L[2] + L[3] * L[3]);
   T er = T(0.5) * (R[1] * R[1] + R[2] * R[2] + R[3] * R[3]);
   T El, Er, gam_l, gam_r;
   if (NS == 0 || (NS < 0 && ns == 0)) {
-    El = el * L[0] + L[4] / T(kGammaAir - 1);
-    Er = er * R[0] + R[4] / T(kGammaAir - 1);
+    El = el * L[0] + pl / T(kGammaAir - 1);
+    Er = er * R[0] + pr / T(kGammaAir - 1);
     gam_l = gam_r = T(kGammaAir);
   } else {
     const SpecTables<T> &S = tab<T>(C);
@@ -315,8 +347,8 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T *rec,
 #pragma unroll
     for (int l = 0; l < A; ++l)
       if (l < ns) mwl += L[5 + l] * S.inv_mw[l], mwr += R[5 + l] * S.inv_mw[l];
-    const T t_l = fdiv(L[4], L[0] * T(kRu) * mwl);
-    const T t_r = fdiv(R[4], R[0] * T(kRu) * mwr);
+    const T t_l = fdiv(pl, L[0] * T(kRu) * mwl);
+    const T t_r = fdiv(pr, R[0] * T(kRu) * mwr);
     T cpl = 0, cpr = 0, cvl = 0, cvr = 0;
 #pragma unroll
     for (int l = 0; l < A; ++l) {
@@ -332,8 +364,8 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T *rec,
         er += hr * R[5 + l];
       }
     }
-    El = L[0] * el - L[4];
-    Er = R[0] * er - R[4];
+    El = L[0] * el - pl;
+    Er = R[0] * er - pr;
     gam_l = fdiv(cpl, cvl);
     gam_r = fdiv(cpr, cvr);
   }
@@ -343,7 +375,7 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T *rec,
   const T igk = frcp(gk);
   const T ul = (k1 * L[1] + k2 * L[2] + k3 * L[3]) * igk;
   const T ur = (k1 * R[1] + k2 * R[2] + k3 * R[3]) * igk;
-  const T pl = L[4], pr = R[4], rho_l = L[0], rho_r = R[0];
+  const T rho_l = L[0], rho_r = R[0];
   const T c = T(0.5) * (fsqrt(fdiv(gam_l * pl, rho_l)) + fsqrt(fdiv(gam_r * pr, rho_r)));
   const T ic = frcp(c);
   const T mach_l = ul * ic, mach_r = ur * ic;
@@ -366,8 +398,23 @@ __device__ __forceinline__ void face_inviscid(const ChemParams &C, const T *rec,
     mrn = -a - T(0.125) * b;
     prn = a * (T(2) + mach_r) - alpha * mach_r * b;
   }
-  const T p_coeff = plp * pl + prn * pr;
-  const T m_half = mlp + mrn;
+  // pressure term of the momentum flux, less p_ref k: plp p'_l + prn p'_r
+  // + p_ref (plp + prn - 1), the last factor evaluated without cancellation
+  T p_coeff;
+  if (C.p_ref == 0.0) {
+    p_coeff = plp * pl + prn * pr;
+  } else {
+    p_coeff = plp * L[4] + prn * R[4] + pref * ausm_pressure_defect(mach_l, mach_r, alpha);
+  }
+  // interface Mach number M+(ml) + M-(mr); at low Mach both terms are near
+  // +-3/8 and their FP32 sum loses ~5 bits, so the FP32 path uses the
+  // cancellation-free form (the FP64 path keeps the reference's sum)
+  T m_half = mlp + mrn;
+  if (sizeof(T) == 4 && !(fabs(mach_l) > T(1)) && !(fabs(mach_r) > T(1))) {
+    // M+(M) + M-(M) = M: M+(ml) + M-(mr) = mr + (ml - mr) [1/2 + (ml + mr)(1/4 + (ml^2 + mr^2 - 2)/8)]
+    m_half = mach_r + (mach_l - mach_r) *
+                          (T(0.5) + (mach_l + mach_r) * (T(0.25) + T(0.125) * (mach_l * mach_l + mach_r * mach_r - T(2))));
+  }
   const T mach_pos = T(0.5) * (m_half + fabs(m_half));
   const T mach_neg = T(0.5) * (m_half - fabs(m_half));
   const T mass_flux_half = c * (rho_l * mach_pos + rho_r * mach_neg);

@@ -230,7 +230,10 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
 #pragma unroll
   for (int l = 0; l < NV; ++l) {
     if (l < nv) {
-      double qs = a.Qin[l * N + p] + dq[l] * dtj;
+      double dql = dq[l];
+      // momentum fluxes carry p - p_ref: add back -p_ref sum(k+ - k-) (zero on uniform grids)
+      if (a.gcl && l >= 1 && l <= 3) dql -= C.p_ref * a.gcl[(l - 1) * N + p];
+      double qs = a.Qin[l * N + p] + dql * dtj;
       if (l == 3 && !three_d) qs = 0;
       q[l] = (a.a != 0.0) ? a.a * a.Qn[l * N + p] + a.b * qs : qs;
       if (a.q32) q[l] = (double)(float)q[l];  // full-FP32 study: FP32 conserved state
@@ -303,7 +306,7 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
   Pn[N + p] = T(u);
   Pn[2 * N + p] = T(v);
   Pn[3 * N + p] = T(w);
-  Pn[4 * N + p] = T(pres);
+  Pn[4 * N + p] = T(pres - C.p_ref);  // gauge pressure
   Pn[5 * N + p] = T(temp);
   T Yt[A];
 #pragma unroll
@@ -636,7 +639,7 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
 #pragma unroll
       for (int l = 0; l < A; ++l)
         if (l < ns) Y[l] = bc.yk[l];
-      for (int f = 0; f < 6; ++f) a.sP[f * S + o] = T(pr[f]);
+      for (int f = 0; f < 6; ++f) a.sP[f * S + o] = T(f == 4 ? pr[f] - C.p_ref : pr[f]);
 #pragma unroll
       for (int l = 0; l < A; ++l)
         if (l < ns) a.sP[(6 + l) * S + o] = T(Y[l]);
@@ -657,7 +660,7 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
     } else {
       // BoundCond.cu:529-629 apply_wall
       const double t_in = (double)ra.P[5 * ra.stride + ra.idx];
-      const double p_in = (double)ra.P[4 * ra.stride + ra.idx];
+      const double p_in = (double)ra.P[4 * ra.stride + ra.idx] + C.p_ref;  // stored as gauge pressure
       double mwi = 0;
 #pragma unroll
       for (int l = 0; l < A; ++l)
@@ -684,7 +687,7 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
         pr[4] = p_in;
         pr[5] = tg;
       }
-      for (int f = 0; f < 6; ++f) a.sP[f * S + o] = T(pr[f]);
+      for (int f = 0; f < 6; ++f) a.sP[f * S + o] = T(f == 4 ? pr[f] - C.p_ref : pr[f]);
 #pragma unroll
       for (int l = 0; l < A; ++l)
         if (l < ns) a.sP[(6 + l) * S + o] = T(Y[l]);
@@ -814,7 +817,37 @@ __global__ void k_props_all(const __grid_constant__ ChemParams C, const T *P, T 
     if (l < ns) Pr[(2 + l) * N + p] = rd[l];
 }
 
-// Global time step of the current state over interior points.
+// Geometric part of the momentum flux difference that the gauge pressure
+// leaves out: gcl[c][p] = sum over the face directions d of k_c(p, +d) -
+// k_c(p, -d), with the face vector k = (J_0 m_0 + J_1 m_1) / 2 formed in the
+// bulk precision exactly as the face fluxes form it.  Zero on uniform grids.
+template <typename T>
+__global__ void k_gcl(const BlockInfo *blocks, int nblocks, const T *G, int64_t N, int64_t n_interior_total,
+                      double *gcl) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_interior_total;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    int b = 0;
+    while (b + 1 < nblocks && blocks[b + 1].interior_off <= g) ++b;
+    const BlockInfo B = blocks[b];
+    const int64_t r = g - B.interior_off;
+    const int i = (int)(r % B.mx), j = (int)((r / B.mx) % B.my), k = (int)(r / ((int64_t)B.mx * B.my));
+    const int64_t p = B.base + i + (int64_t)B.nx * j + (int64_t)B.nx * B.ny * k;
+    const int64_t st[3] = {1, B.nx, (int64_t)B.nx * B.ny};
+    double acc[3] = {0, 0, 0};
+    for (int d = 0; d < (B.mz > 1 ? 3 : 2); ++d) {
+      const int64_t q0 = p - st[d], q1 = p, q2 = p + st[d];
+      for (int c = 0; c < 3; ++c) {
+        const T *m = G + (1 + 3 * d + c) * N;
+        const T kp = T(0.5) * (G[q1] * m[q1] + G[q2] * m[q2]);
+        const T km = T(0.5) * (G[q0] * m[q0] + G[q1] * m[q1]);
+        acc[c] += (double)kp - (double)km;
+      }
+    }
+    for (int c = 0; c < 3; ++c) gcl[c * N + p] = acc[c];
+  }
+}
+
+// Global time step of the current state over interior points.// Global time step of the current state over interior points.
 template <typename T, int NS>
 __global__ void k_dt_reduce(const __grid_constant__ ChemParams C, const BlockInfo *blocks, int nblocks, const T *P,
                             const T *Pr, const T *G, int64_t N, int64_t n_interior_total,
