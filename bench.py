@@ -155,6 +155,23 @@ def ncu_traffic(kernel_tag):
     return None
 
 
+def max_over_ranks(ms, dist):
+    """The slowest rank's time (replicas run independently; the job takes
+    as long as its slowest GPU)."""
+    if not dist:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, npts, steps, ms_total):
+    """Mcell-updates/s of the whole job: every rank updates npts points 3
+    times per step, in the slowest rank's time."""
+    return world * npts * 3 * steps / (ms_total / 1e3) / 1e6
+
+
 def run_ours(args, rank, world, dist):
     import torch
     import combustioncodegpu_b200 as cc
@@ -183,11 +200,7 @@ def run_ours(args, rank, world, dist):
             e1.record(s)
             e1.synchronize()
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1), dist)
         kt = d.time_kernels(2)
         out[prec] = {"ms_total": ms, "ms_per_step": ms / args.steps, "npts": npts, "clocks": clk.summary(),
                      "kernels": kt, "info": info, "status": d.status(), "tuning": d.tuning()}
@@ -481,9 +494,8 @@ def main():
         return
     peaks, peak_kind = load_peaks()
     mixed, plain = out["mixed"], out["fp64"]
-    stages = 3 * args.steps
-    value = world * mixed["npts"] * stages / (mixed["ms_total"] / 1e3) / 1e6
-    value_plain = world * plain["npts"] * stages / (plain["ms_total"] / 1e3) / 1e6
+    value = whole_job_rate(world, mixed["npts"], args.steps, mixed["ms_total"])
+    value_plain = whole_job_rate(world, plain["npts"], args.steps, plain["ms_total"])
     bpp = algorithmic_bytes(9, "mixed")
     kt = mixed["kernels"]
     stage_ms = kt["stage_ms"]
