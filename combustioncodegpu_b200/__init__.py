@@ -109,6 +109,8 @@ EXPORTS = {
     "cc_use_closure": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_closure_stats": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "cc_eval_transport": ([ctypes.c_void_p, ctypes.c_int64, _dp, _dp, ctypes.c_int, _dp], ctypes.c_int),
+    "cc_save_checkpoint": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
+    "cc_load_checkpoint": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
     "cc_sync": ([ctypes.c_void_p], ctypes.c_int),
     "cc_residual_rms_noalloc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
                                 ctypes.c_int),
@@ -416,6 +418,15 @@ class Driver:
         """"batched": one launch per stage kernel over all blocks;
         "per_block": one launch per block per kernel (the reference's way)."""
         _check(self.lib.cc_set_launch_mode(self.ctx, {"batched": 0, "per_block": 1}[mode]))
+
+    def save_checkpoint(self, path):
+        """The current state, bit for bit (cc_save_checkpoint)."""
+        _check(self.lib.cc_save_checkpoint(self.ctx, str(path).encode()))
+
+    def load_checkpoint(self, path):
+        """Restore a state saved by save_checkpoint into this initialised
+        context (same blocks, species and precision)."""
+        _check(self.lib.cc_load_checkpoint(self.ctx, str(path).encode()))
 
     def set_closure(self, weights):
         """Upload a learned transport closure: a dict with w1, b1, ..., w4,

@@ -1396,6 +1396,98 @@ int cc_eval_transport(cc_ctx *c, int64_t n, const double *T, const double *Y, in
   return c->chem.ns == 9 ? eval_transport_ns<9>(c, n, T, Y, mode, out) : eval_transport_ns<-1>(c, n, T, Y, mode, out);
 }
 
+}  // extern "C"
+
+namespace {
+
+// Checkpoint file: header, then the current state's arrays as they are on
+// the device (so that a restart continues bit-identically): Q [n_var][N]
+// FP64, P [6+ns][N] and Pr [2+ns][N] in the bulk precision, |V| [N] FP64,
+// the time step and its history slot [2] FP64.
+struct CkptHeader {
+  char magic[8];  // "CCB2CKPT"
+  int32_t version, precision, n_spec, n_blocks;
+  int64_t N;
+  double p_ref;
+  int32_t dims[3 * 4096];
+};
+
+int ckpt_io(cc_ctx *c, const char *path, bool save) {
+  if (int r = check_ctx(c)) return r;
+  if (!path) return fail(CC_ERR_ARG, "checkpoint: null path");
+  if (!c->initialized) return fail(CC_ERR_STATE, "checkpoint: cc_init first");
+  if (c->blocks.size() > 4096) return fail(CC_ERR_ARG, "checkpoint: at most 4096 blocks");
+  if (c->state_dirty && save) {
+    int r = dispatch(c, [&](auto tt, auto nn) { return derive_state<typename decltype(tt)::type, decltype(nn)::value>(c); });
+    if (r) return r;
+  }
+  CkptHeader h;
+  std::memset(&h, 0, sizeof h);
+  std::memcpy(h.magic, "CCB2CKPT", 8);
+  h.version = 1, h.precision = c->precision, h.n_spec = c->chem.ns, h.n_blocks = (int32_t)c->blocks.size();
+  h.N = c->N, h.p_ref = c->chem.p_ref;
+  for (size_t b = 0; b < c->blocks.size(); ++b)
+    h.dims[3 * b] = c->blocks[b].mx, h.dims[3 * b + 1] = c->blocks[b].my, h.dims[3 * b + 2] = c->blocks[b].mz;
+  const size_t N = (size_t)c->N;
+  struct Part {
+    void *dev;
+    size_t bytes;
+  };
+  const Part parts[] = {{c->Q[c->qcur], sizeof(double) * N * nv_of(c)},
+                        {c->P[c->cur], c->elem * N * np_of(c)},
+                        {c->Pr[c->cur], c->elem * N * npr_of(c)},
+                        {c->d_vel, sizeof(double) * N},
+                        {c->d_dt, sizeof(double) * 2}};
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<unsigned char> buf;
+  FILE *f = std::fopen(path, save ? "wb" : "rb");
+  if (!f) return fail(CC_ERR_ARG, std::string("checkpoint: cannot open ") + path);
+  int rc = 0;
+  if (save) {
+    if (std::fwrite(&h, sizeof h, 1, f) != 1) rc = fail(CC_ERR_ARG, "checkpoint: write failed");
+    for (const Part &pt : parts) {
+      if (rc) break;
+      buf.resize(pt.bytes);
+      if (cudaMemcpy(buf.data(), pt.dev, pt.bytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        rc = fail(CC_ERR_CUDA, "checkpoint: device read failed");
+        break;
+      }
+      if (std::fwrite(buf.data(), 1, pt.bytes, f) != pt.bytes) rc = fail(CC_ERR_ARG, "checkpoint: write failed");
+    }
+  } else {
+    CkptHeader g;
+    if (std::fread(&g, sizeof g, 1, f) != 1 || std::memcmp(g.magic, "CCB2CKPT", 8) != 0 || g.version != 1)
+      rc = fail(CC_ERR_ARG, "checkpoint: not a checkpoint file");
+    else if (g.precision != h.precision || g.n_spec != h.n_spec || g.n_blocks != h.n_blocks || g.N != h.N ||
+             std::memcmp(g.dims, h.dims, sizeof(int32_t) * 3 * h.n_blocks) != 0)
+      rc = fail(CC_ERR_ARG, "checkpoint: written for another layout or precision");
+    for (const Part &pt : parts) {
+      if (rc) break;
+      buf.resize(pt.bytes);
+      if (std::fread(buf.data(), 1, pt.bytes, f) != pt.bytes) {
+        rc = fail(CC_ERR_ARG, "checkpoint: file too short");
+        break;
+      }
+      if (cudaMemcpy(pt.dev, buf.data(), pt.bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = fail(CC_ERR_CUDA, "checkpoint: device write failed");
+    }
+    if (!rc) {
+      c->chem.p_ref = g.p_ref;
+      c->state_dirty = false;
+      destroy_graphs(c);
+    }
+  }
+  std::fclose(f);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cc_save_checkpoint(cc_ctx *c, const char *path) { return ckpt_io(c, path, true); }
+int cc_load_checkpoint(cc_ctx *c, const char *path) { return ckpt_io(c, path, false); }
+
 int cc_set_launch_mode(cc_ctx *c, int per_block) {
   if (int r = check_ctx(c)) return r;
   c->per_block = per_block != 0;

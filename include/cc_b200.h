@@ -227,6 +227,13 @@ int cc_closure_stats(cc_ctx *ctx, int64_t out[2]);
  * out [2 + n_spec][n] = (mu, lambda, rhoD_k), by the exact FP64 evaluation
  * (mode 0) or by the closure kernel (mode 1).  Needs a device, not cc_init. */
 int cc_eval_transport(cc_ctx *ctx, int64_t n, const double *T, const double *Y, int mode, double *out);
+/* Checkpoint / restart (absent in the reference, Initialize.cu:14-22 only
+ * starts from inflow states): the current state as it is on the device
+ * (conserved variables, primitives and transport in the bulk precision, |V|,
+ * the time step), so that a restart continues bit-identically.  Loading
+ * needs a context initialised with the same blocks, species and precision. */
+int cc_save_checkpoint(cc_ctx *ctx, const char *path);
+int cc_load_checkpoint(cc_ctx *ctx, const char *path);
 /* Synchronises the context's stream. */
 int cc_sync(cc_ctx *ctx);
 

@@ -288,3 +288,32 @@ def test_full_size_conservation_and_mass_fractions(precision):
     assert np.isfinite(bv).all()
     assert d.status() == 0
     d.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_checkpoint_restart_is_bit_identical(precision, tmp_path):
+    case = CASES["channel"]
+    d = cc.Driver.from_case(case, precision)
+    d.initialize_computation()
+    d.simulate(3, "rk3")
+    path = tmp_path / "state.ckpt"
+    d.save_checkpoint(path)
+    d.simulate(3, "rk3", residual=True)
+    want, want_res = d.field[0].get_state(), d.residual()
+    d.close()
+    e = cc.Driver.from_case(case, precision)
+    e.initialize_computation()
+    e.load_checkpoint(path)
+    e.simulate(3, "rk3", residual=True)
+    got, got_res = e.field[0].get_state(), e.residual()
+    assert e.status() == 0
+    e.close()
+    for a, b in zip(want, got):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(want_res, got_res)
+    # a context of another precision refuses the file
+    f = cc.Driver.from_case(case, "fp64" if precision == "mixed" else "mixed")
+    f.initialize_computation()
+    with pytest.raises(RuntimeError, match="another layout or precision"):
+        f.load_checkpoint(path)
+    f.close()
