@@ -72,10 +72,12 @@ struct GlobalStencil {
 // Face flux (inviscid minus viscous) of the face between p0 and p0 + e_d;
 // transport properties and geometry are read from the arenas at the global
 // point gp (and gp + gsd).
-template <typename T, int NS, typename Stencil>
+// DIR >= 0 fixes the face direction at compile time (d_rt is then ignored).
+template <typename T, int NS, typename Stencil, int DIR = -1>
 __device__ __forceinline__ void face_flux_gen(const ChemParams &C, const T *rec, const Stencil &S,
                                               const T *__restrict__ Pr, const T *__restrict__ G, int N, int gp, int gsd,
-                                              int d, T *F) {
+                                              int d_rt, T *F) {
+  const int d = DIR >= 0 ? DIR : d_rt;
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   const int p = gp, p1 = gp + gsd;
@@ -178,12 +180,12 @@ __device__ __forceinline__ void face_flux_gen(const ChemParams &C, const T *rec,
   }
 }
 
-template <typename T, int NS>
+template <typename T, int NS, int DIR = -1>
 __device__ __forceinline__ void face_flux(const ChemParams &C, const T *rec, const T *__restrict__ P,
                                           const T *__restrict__ Pr, const T *__restrict__ G, int N, int p, int d,
                                           int sd, int sj, int sk, T *F) {
   GlobalStencil<T> S{P, N, p, sd, sj, sk};
-  face_flux_gen<T, NS>(C, rec, S, Pr, G, N, p, sd, d, F);
+  face_flux_gen<T, NS, GlobalStencil<T>, DIR>(C, rec, S, Pr, G, N, p, sd, d, F);
 }
 
 // gamma and acoustic speed of a point (Field.cu:187-200)
