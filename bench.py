@@ -46,6 +46,9 @@ def parse():
                          "per-block; mixing_layer: 1024x512x4 precision study (FP64 / mixed / FP32); "
                          "box256_closure: 256^3 box, exact transport vs the learned closure")
     ap.add_argument("--study-steps", default="100,1000,2000", help="mixing_layer: error snapshot steps")
+    ap.add_argument("--variant", default="auto", choices=["auto", "l1", "tma", "split"],
+                    help="stage kernels: autotuned (default) or pinned (profiling runs, where the autotuner's "
+                         "timings are distorted)")
     return ap.parse_args()
 
 
@@ -184,6 +187,8 @@ def run_ours(args, rank, world, dist):
     states = {}
     for prec in ("fp64", "mixed"):
         d = cc.Driver.from_case(case, prec)
+        if args.variant != "auto":
+            d.set_tuning(args.variant, 4)
         d.initialize_computation()
         s = torch.cuda.ExternalStream(d.stream())
         info = d.info()
