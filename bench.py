@@ -242,6 +242,8 @@ def run_ours(args, rank, world, dist):
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
         bv_h, yk_h = pin(blk["bv"]), pin(blk["yk"])
         d = cc.Driver.from_case(case, "mixed")
+        if args.variant != "auto":
+            d.set_tuning(args.variant, 4)
         d.initialize_computation()
         d.simulate(2)
         d.sync()

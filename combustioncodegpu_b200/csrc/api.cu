@@ -83,6 +83,7 @@ struct cc_ctx {
   HaloPlan plan;
   HaloNode *d_nodes = nullptr;
   HaloCopy *d_copies = nullptr;
+  int64_t *d_icopies = nullptr;   // copies that rewrite an interior point
   void *sP = nullptr, *sPr = nullptr;
   double *sQ = nullptr;
   int64_t ns_cap = 1;
@@ -433,6 +434,11 @@ int setup_device(cc_ctx *c) {
   c->d_nodes = (HaloNode *)p;
   if (dev_alloc(c, &p, sizeof(HaloCopy) * std::max<size_t>(1, c->plan.copies.size()))) return CC_ERR_CUDA;
   c->d_copies = (HaloCopy *)p;
+  if (dev_alloc(c, &p, sizeof(int64_t) * std::max<size_t>(1, c->plan.interior_copies.size()))) return CC_ERR_CUDA;
+  c->d_icopies = (int64_t *)p;
+  if (!c->plan.interior_copies.empty())
+    CK(cudaMemcpyAsync(c->d_icopies, c->plan.interior_copies.data(),
+                       sizeof(int64_t) * c->plan.interior_copies.size(), cudaMemcpyHostToDevice, c->stream));
   if (dev_alloc(c, &p, sizeof(BcDevice) * std::max<size_t>(1, c->bcs.size()))) return CC_ERR_CUDA;
   c->d_bcs = (BcDevice *)p;
   if (dev_alloc(c, &p, sizeof(double) * 4)) return CC_ERR_CUDA;
@@ -505,6 +511,8 @@ HaloArgs<T> halo_args(cc_ctx *c, int pn, int pp, double *qn, const double *qp) {
   h.bcs = c->d_bcs;
   h.nodes = c->d_nodes;
   h.copies = c->d_copies;
+  h.icopies = c->d_icopies;
+  h.n_icopies = (int64_t)c->plan.interior_copies.size();
   return h;
 }
 

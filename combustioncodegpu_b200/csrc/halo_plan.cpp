@@ -3,6 +3,8 @@
 #include "halo_plan.h"
 
 #include <algorithm>
+#include <climits>
+#include <cstdint>
 #include <cstdlib>
 #include <functional>
 #include <unordered_map>
@@ -243,10 +245,29 @@ bool Replay::run(HaloPlan &plan) {
   for (int id = 0; id < nn; ++id)
     if (level[id] >= 0) max_level = std::max(max_level, level[id]);
 
+  // Scratch slots follow the destination order of phase B: each node is
+  // placed by the smallest destination index among the copies that read it,
+  // handed down to the lower-level nodes it reads, so that consecutive
+  // copies read consecutive slots.
+  std::vector<int64_t> pos(nn, INT64_MAX);
+  for (const auto &kv : changed)
+    if (kv.second.kind == 2) pos[kv.second.idx] = std::min(pos[kv.second.idx], kv.first);
+  for (int L = max_level; L > 0; --L)
+    for (int id = 0; id < nn; ++id) {
+      if (level[id] != L) continue;
+      const SymNode &sn = nodes_[id];
+      const bool two = sn.op == kHaloAvg || sn.op == kHaloWallGhost;
+      if (sn.op != kHaloInflow && sn.a.kind == 2) pos[sn.a.idx] = std::min(pos[sn.a.idx], pos[id]);
+      if (two && sn.b.kind == 2) pos[sn.b.idx] = std::min(pos[sn.b.idx], pos[id]);
+    }
   std::vector<int> order;
   for (int id = 0; id < nn; ++id)
     if (level[id] >= 0) order.push_back(id);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return level[a] < level[b]; });
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    if (level[a] != level[b]) return level[a] < level[b];
+    if (pos[a] != pos[b]) return pos[a] < pos[b];
+    return a < b;
+  });
   std::vector<int64_t> slot(nn, -1);
   for (size_t s = 0; s < order.size(); ++s) slot[order[s]] = (int64_t)s;
   plan.n_slots = (int64_t)order.size();
@@ -287,6 +308,7 @@ bool Replay::run(HaloPlan &plan) {
   wall_points_.erase(std::unique(wall_points_.begin(), wall_points_.end()), wall_points_.end());
   plan.vel_zero = wall_points_;
   plan.copies.clear();
+  plan.interior_copies.clear();
   plan.copies.reserve(changed.size());
   for (const auto &kv : changed) {
     HaloCopy hc{kv.first, to_ref(kv.second)};
@@ -302,6 +324,7 @@ bool Replay::run(HaloPlan &plan) {
       break;
     }
     hc.src.pad = flags;
+    if (flags & 1) plan.interior_copies.push_back((int64_t)plan.copies.size());
     plan.copies.push_back(hc);
   }
   return true;

@@ -51,6 +51,7 @@ struct HaloPlan {
   std::vector<HaloNode> nodes;          // ordered by level
   std::vector<int64_t> level_begin;     // nodes[level_begin[l] .. level_begin[l+1])
   std::vector<HaloCopy> copies;         // phase B
+  std::vector<int64_t> interior_copies; // indices of the copies that rewrite an interior point
   std::vector<int64_t> vel_zero;       // interior points a wall condition writes (DZone::vel = 0)
   int64_t n_slots = 0;
   bool has_wall = false;

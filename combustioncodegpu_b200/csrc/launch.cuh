@@ -112,8 +112,12 @@ template <typename T, int NS>
 cudaError_t Launch<T, NS>::halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s) {
   const int64_t n = a.end - a.begin;
   if (n <= 0) return cudaSuccess;
+  const int ns = C.ns, np = 6 + ns, npr = 2 + ns, nq = 5 + ns;
   const int tpb = 256;
-  k_halo_copies<T, NS><<<(unsigned)((n + tpb - 1) / tpb), tpb, 0, s>>>(a, C);
+  k_halo_copy_fields<T, NS><<<dim3((unsigned)((n + tpb - 1) / tpb), np + npr + nq), tpb, 0, s>>>(a, np, npr, nq);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !a.dt_next || a.n_icopies <= 0) return e;
+  k_halo_copy_dt<T, NS><<<(unsigned)((a.n_icopies + tpb - 1) / tpb), tpb, 0, s>>>(a, C);
   return cudaGetLastError();
 }
 

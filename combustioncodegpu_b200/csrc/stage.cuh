@@ -718,58 +718,52 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
   }
 }
 
-// Phase B: write every changed point from its resolved source.  Interior
-// points rewritten here (coincident interface layers) contribute their
-// post-exchange local time step to the next global step, as the reference
-// evaluates the step after the exchange (Driver.cu:150-163).
+// Phase B: write every changed point from its resolved source, one thread
+// per (copy, field): consecutive threads move one field of consecutive
+// copies, so every thread issues one load and one store and the list's
+// destination order keeps them coalesced.
 template <typename T, int NS>
-__global__ void k_halo_copies(const HaloArgs<T> a, const __grid_constant__ ChemParams C) {
+__global__ void k_halo_copy_fields(const HaloArgs<T> a, int np, int npr, int nq) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // copy (grid x)
+  const int f = blockIdx.y;                                           // field (grid y)
+  if (e >= a.end - a.begin) return;
+  const HaloCopy c = a.copies[a.begin + e];
+  const RefPtrs<T> r = resolve(a, c.src);
+  if (f < np) {
+    a.P[f * a.N + c.dst] = r.P[f * r.stride + r.idx];
+  } else if (f < np + npr) {
+    const int g = f - np;
+    a.Pr[g * a.N + c.dst] = r.Pr[g * r.stride + r.idx];
+  } else {
+    const int g = f - np - npr;
+    a.Q[g * a.N + c.dst] = r.Q[g * r.stride + r.idx];
+  }
+}
+
+// Interior points rewritten by phase B (coincident interface layers)
+// contribute their post-exchange local time step to the next global step,
+// as the reference evaluates the step after the exchange (Driver.cu:150-163).
+template <typename T, int NS>
+__global__ void k_halo_copy_dt(const HaloArgs<T> a, const __grid_constant__ ChemParams C) {
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
-  const int np = 6 + ns, npr = 2 + ns, nq = 5 + ns;
-  const int64_t e = a.begin + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double dt_min = 1e300;
-  if (e < a.end) {
-    const HaloCopy c = a.copies[e];
-    const RefPtrs<T> r = resolve(a, c.src);
-    // all loads before the first store (see k_halo_nodes)
-    T vP[6 + A], vPr[2 + A];
-    double vQ[5 + A];
+  if (e < a.n_icopies) {
+    const HaloCopy c = a.copies[a.icopies[e]];
+    const int64_t p = c.dst, N = a.N;
+    T Y[A], gam, cs;
 #pragma unroll
-    for (int f = 0; f < 6 + A; ++f)
-      if (f < np) vP[f] = r.P[f * r.stride + r.idx];
-#pragma unroll
-    for (int f = 0; f < 2 + A; ++f)
-      if (f < npr) vPr[f] = r.Pr[f * r.stride + r.idx];
-#pragma unroll
-    for (int f = 0; f < 5 + A; ++f)
-      if (f < nq) vQ[f] = r.Q[f * r.stride + r.idx];
-#pragma unroll
-    for (int f = 0; f < 6 + A; ++f)
-      if (f < np) a.P[f * a.N + c.dst] = vP[f];
-#pragma unroll
-    for (int f = 0; f < 2 + A; ++f)
-      if (f < npr) a.Pr[f * a.N + c.dst] = vPr[f];
-#pragma unroll
-    for (int f = 0; f < 5 + A; ++f)
-      if (f < nq) a.Q[f * a.N + c.dst] = vQ[f];
-    if (a.dt_next && (c.src.pad & 1)) {
-      const int64_t p = c.dst, N = a.N;
-      T Y[A], gam, cs;
-#pragma unroll
-      for (int l = 0; l < A; ++l)
-        if (l < ns) Y[l] = a.P[(6 + l) * N + p];
-      gamma_and_c<T, NS>(C, param_rec<T>(C), a.P[5 * N + p], Y, gam, cs);
-      dt_min = local_time_step<T>(C, a.G, N, p, (double)a.P[p], (double)a.P[N + p], (double)a.P[2 * N + p],
-                                  (double)a.P[3 * N + p], (double)cs, (double)gam, (double)a.Pr[p],
-                                  (c.src.pad & 2) != 0);
-    }
+    for (int l = 0; l < A; ++l)
+      if (l < ns) Y[l] = a.P[(6 + l) * N + p];
+    gamma_and_c<T, NS>(C, param_rec<T>(C), a.P[5 * N + p], Y, gam, cs);
+    dt_min = local_time_step<T>(C, a.G, N, p, (double)a.P[p], (double)a.P[N + p], (double)a.P[2 * N + p],
+                                (double)a.P[3 * N + p], (double)cs, (double)gam, (double)a.Pr[p],
+                                (c.src.pad & 2) != 0);
   }
-  if (a.dt_next) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) dt_min = fmin(dt_min, __shfl_xor_sync(0xffffffffu, dt_min, o));
-    if ((threadIdx.x & 31) == 0) atomic_min_pos_double(a.dt_next, dt_min);
-  }
+  for (int o = 16; o > 0; o >>= 1) dt_min = fmin(dt_min, __shfl_xor_sync(0xffffffffu, dt_min, o));
+  if ((threadIdx.x & 31) == 0) atomic_min_pos_double(a.dt_next, dt_min);
 }
 
 // ------------------------------------------------------------ setup / misc
