@@ -46,7 +46,7 @@ def parse():
                          "per-block; mixing_layer: 1024x512x4 precision study (FP64 / mixed / FP32); "
                          "box256_closure: 256^3 box, exact transport vs the learned closure")
     ap.add_argument("--study-steps", default="100,1000,2000", help="mixing_layer: error snapshot steps")
-    ap.add_argument("--variant", default="auto", choices=["auto", "l1", "tma", "split"],
+    ap.add_argument("--variant", default="auto", choices=["auto", "l1", "tma", "split", "split-tma"],
                     help="stage kernels: autotuned (default) or pinned (profiling runs, where the autotuner's "
                          "timings are distorted)")
     return ap.parse_args()
@@ -506,10 +506,11 @@ def main():
     bpp = algorithmic_bytes(9, "mixed")
     kt = mixed["kernels"]
     stage_ms = kt["stage_ms"]
-    split = mixed["tuning"]["variant"] == "split"
+    split = mixed["tuning"]["variant"] in ("split", "split-tma")
     stage_achieved = bpp * mixed["npts"] / (stage_ms / 1e3) / 1e9
     if split:  # dominant kernel: the face kernel
-        kname, kbpp, kms = "k_faces<float,9>", face_kernel_bytes(9, "mixed"), kt["faces_ms"]
+        kname = "k_faces_tma<float,9>" if mixed["tuning"]["variant"] == "split-tma" else "k_faces<float,9>"
+        kbpp, kms = face_kernel_bytes(9, "mixed"), kt["faces_ms"]
         traffic = ncu_traffic("faces_kernel_box128_mixed")
     else:
         kname, kbpp, kms = "k_stage<float,9>", bpp, stage_ms
@@ -517,7 +518,10 @@ def main():
     achieved = kbpp * mixed["npts"] / (kms / 1e3) / 1e9
     cpu = cpu_baseline(args, os.cpu_count() or 1, steps=2, n=96)
     levels = mixed["info"]["halo_levels"]
-    launches_per_step = 3 * ((2 if split else 1) + levels + 1) + 1
+    # per stage: stage kernels, halo node levels, halo copies; per step: the
+    # third stage's post-exchange dt of rewritten interior points, dt finalize
+    n_stage = {"l1": 1, "tma": 1, "split": 2, "split-tma": 3}[mixed["tuning"]["variant"]]
+    launches_per_step = 3 * (n_stage + levels + 1) + 2
     line = {
         "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak",

@@ -29,7 +29,7 @@ MAX_SPECIES = 16
 CC_FP64, CC_MIXED, CC_FP32 = 0, 1, 2
 CC_RK3, CC_STEADY_EULER = 0, 1
 PRECISIONS = {"fp64": CC_FP64, "mixed": CC_MIXED, "fp32": CC_FP32}
-VARIANTS = ("l1", "tma", "split")  # stage-kernel variants, cc_tuning order
+VARIANTS = ("l1", "tma", "split", "split-tma")  # stage-kernel variants, cc_tuning order
 SCHEMES = {"rk3": CC_RK3, "steady": CC_STEADY_EULER}
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -403,14 +403,15 @@ class Driver:
     def tuning(self):
         """Stage-kernel configuration in use: variant ("l1" fused with L1
         stencil reads, "tma" fused with TMA-staged planes, "split" face and
-        update kernels), k-planes per tile, measured ms per stage."""
+        update kernels, "split-tma" the same with TMA-staged planes in the
+        face kernel), k-planes per tile, measured ms per stage."""
         v, kz, ms = ctypes.c_int(), ctypes.c_int(), np.zeros(1)
         _check(self.lib.cc_tuning(self.ctx, ctypes.byref(v), ctypes.byref(kz), _ptr(ms)))
         return {"variant": VARIANTS[v.value], "kz": kz.value, "stage_ms": float(ms[0])}
 
     def set_tuning(self, variant="auto", kz=0):
-        """Pin the stage-kernel configuration: variant "auto", "l1", "tma" or
-        "split"; kz k-planes per tile (0 = autotune)."""
+        """Pin the stage-kernel configuration: variant "auto", "l1", "tma",
+        "split" or "split-tma"; kz k-planes per tile (0 = autotune)."""
         v = (-1 if variant == "auto" else VARIANTS.index(variant)) if isinstance(variant, str) else int(variant)
         _check(self.lib.cc_set_tuning(self.ctx, v, int(kz)))
 

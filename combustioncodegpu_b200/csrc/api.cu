@@ -625,7 +625,7 @@ int prof_event(cc_ctx *c, std::vector<cudaEvent_t> &pool, size_t &next) {
   return 0;
 }
 
-const char *const kVariantName[3] = {"fused-l1", "fused-tma", "split"};
+const char *const kVariantName[4] = {"fused-l1", "fused-tma", "split", "split-tma"};
 
 // One stage's kernels of the given variant over the current tile list:
 // one launch per kernel over all blocks, or (per_block) one per block.
@@ -651,10 +651,15 @@ template <typename T, int NS>
 int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge) {
   if (variant == 1) {
     CK((Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
-  } else if (variant == 2) {
+  } else if (variant == 2 || variant == 3) {
     a.faces = (T *)c->faces;
     if (!a.edge_tiles) a.edge_tiles = c->d_edges;
-    CK((Launch<T, NS>::faces(a, c->chem, nt, n_edge, c->stream)));
+    if (variant == 2) {
+      CK((Launch<T, NS>::faces(a, c->chem, nt, n_edge, c->stream)));
+    } else {  // regular tiles from TMA-staged planes, edge tiles through L1
+      CK((Launch<T, NS>::faces_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
+      CK((Launch<T, NS>::faces(a, c->chem, 0, n_edge, c->stream)));
+    }
     if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
     CK((Launch<T, NS>::update(a, c->chem, nt, c->stream)));
   } else {
@@ -718,8 +723,8 @@ int autotune(cc_ctx *c) {
   if (c->force_variant >= 0)
     variants.push_back(c->force_variant);
   else
-    for (int v : {0, 1, 2})
-      if (v != 1 || c->tma_ok) variants.push_back(v);
+    for (int v : {0, 1, 2, 3})
+      if ((v != 1 && v != 3) || c->tma_ok) variants.push_back(v);
   for (int variant : variants) {
     for (int kz : kzs) {
       build_tiles_kz(c, kz);
@@ -1247,14 +1252,15 @@ int cc_tuning(cc_ctx *c, int *variant, int *kz, double *stage_ms) {
 
 int cc_set_tuning(cc_ctx *c, int variant, int kz) {
   if (int r = check_ctx(c)) return r;
-  if (variant < -1 || variant > 2)
-    return fail(CC_ERR_ARG, "variant must be -1 (autotune), 0 (fused, L1), 1 (fused, TMA) or 2 (split)");
+  if (variant < -1 || variant > 3)
+    return fail(CC_ERR_ARG,
+                "variant must be -1 (autotune), 0 (fused, L1), 1 (fused, TMA), 2 (split) or 3 (split, TMA faces)");
   if (kz < 0) return fail(CC_ERR_ARG, "kz must be >= 0");
   c->force_variant = variant;
   c->force_kz = kz;
   if (!c->initialized) return 0;
-  if (variant == 1 && !c->tma_ok)
-    return fail(CC_ERR_ARG, "the TMA variant needs CC_MIXED with 0 or 9 species");
+  if ((variant == 1 || variant == 3) && !c->tma_ok)
+    return fail(CC_ERR_ARG, "the TMA variants need the FP32 bulk precision with 0 or 9 species");
   destroy_graphs(c);
   int r = dispatch(c, [&](auto tt, auto nn) { return autotune<typename decltype(tt)::type, decltype(nn)::value>(c); });
   if (r) return r;

@@ -41,6 +41,20 @@ cudaError_t Launch<T, NS>::faces(const StageArgs<T> &a, const ChemParams &C, int
 }
 
 template <typename T, int NS>
+size_t Launch<T, NS>::faces_tma_smem() {
+  return FacesTmaLayout<T, NS>::kBytes;
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::faces_tma(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
+                                     cudaStream_t s) {
+  if (n_tiles <= 0) return cudaSuccess;
+  if (faces_tma_smem() > 227 * 1024) return cudaErrorInvalidConfiguration;
+  k_faces_tma<T, NS><<<n_tiles, dim3(kTX, kTY), faces_tma_smem(), s>>>(a, (const CUtensorMap *)maps, C);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
 cudaError_t Launch<T, NS>::update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;
   k_update<T, NS><<<n_tiles, dim3(kTX, kTY), update_smem(), s>>>(a, C);
@@ -80,6 +94,8 @@ cudaError_t Launch<T, NS>::configure() {
   if (e != cudaSuccess) return e;
   if (stage_tma_smem() <= 227 * 1024)
     e = cudaFuncSetAttribute(k_stage_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_tma_smem());
+  if (e == cudaSuccess && faces_tma_smem() <= 227 * 1024)
+    e = cudaFuncSetAttribute(k_faces_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)faces_tma_smem());
   return e;
 }
 

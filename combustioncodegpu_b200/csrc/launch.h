@@ -22,6 +22,10 @@ struct Launch {
   static size_t update_smem();
   static cudaError_t faces(const StageArgs<T> &a, const ChemParams &C, int n_regular, int n_edge, cudaStream_t s);
   static cudaError_t update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s);
+  // split variant with TMA-staged planes in the face kernel (regular tiles only)
+  static size_t faces_tma_smem();
+  static cudaError_t faces_tma(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
+                               cudaStream_t s);
   // learned transport closure (closure.cuh) over every arena point; cl is a ClosureDev
   static cudaError_t props_mlp(const T *P, T *Pr, int64_t N, const void *cl, unsigned *status, const ChemParams &C,
                                cudaStream_t s);

@@ -309,3 +309,128 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
 }
 
 }  // namespace ccb
+
+namespace ccb {
+
+// Face kernel of the split stage with TMA-staged primitive planes: the
+// regular tiles of k_faces, each computing the +x, +y, +z faces of its points
+// from a ring of 4 planes (k-1 .. k+2) in shared memory; plane k+3 is
+// requested into the slot of plane k-1 once the faces of plane k are done.
+// Without the fused kernel's flux planes the ring fits twice per SM.
+// Transport and geometry are read through L1; the edge tiles stay with
+// k_faces.  Waits are bounded as in k_stage_tma.
+template <typename T, int NS>
+struct FacesTmaLayout {
+  static constexpr int kRing = 4;
+  static constexpr size_t kPlaneBytes = TmaLayout<T, NS>::kPlaneBytes;
+  static constexpr size_t kRec = ((sizeof(T) * SpecCount<NS>::kArr * 2 * kRecLen + 15) / 16) * 16;
+  // alignment slack + barriers + ring + NASA records
+  static constexpr size_t kBytes = 128 + 128 + kRing * kPlaneBytes + kRec;
+};
+
+template <typename T, int NS>
+__global__ void __launch_bounds__(kTX *kTY, 2)
+    k_faces_tma(const StageArgs<T> a, const CUtensorMap *__restrict__ maps, const __grid_constant__ ChemParams C) {
+  using L = FacesTmaLayout<T, NS>;
+  constexpr int NV = 5 + SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  const int nv = 5 + ns;
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char *smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  unsigned char *ring = smem_raw + 128;
+  T *sRec = reinterpret_cast<T *>(ring + L::kRing * L::kPlaneBytes);
+
+  const Tile t = a.tiles[blockIdx.x];
+  const BlockInfo B = a.blocks[t.blk];
+  const CUtensorMap *map = maps + t.blk;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+  const int i = t.i0 + tx, j = t.j0 + ty;
+  const bool act = (i < B.mx) && (j < B.my);
+  const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
+  const int col = (int)B.base + i + sj * j;
+  const bool three_d = B.mz > 1;
+  const unsigned plane_bytes = (unsigned)(sizeof(T) * (6 + ns) * kPlaneVals);
+  // tensor coordinates of plane kp: x = i0 - 2 + g, y = j0 - 2 + g, z = kp + g
+  const int tx0 = t.i0 - 2 + B.g, ty0 = t.j0 - 2 + B.g;
+  const int kfirst = t.k0 - 1, klast = t.k1 + 1;  // planes the sweep reads
+
+  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * kTY) sRec[e] = param_rec<T>(C)[e];
+  if (tid == 0) {
+    for (int b = 0; b < L::kRing; ++b) mbar_init(&bars[b], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+                 : "memory");
+  }
+  __syncthreads();
+  // plane kp lives in slot (kp - kfirst) % 4 as that slot's n-th load, n = (kp - kfirst) / 4
+  auto slot_of = [&](int kp) { return (kp - kfirst) & (L::kRing - 1); };
+  auto parity_of = [&](int kp) { return (unsigned)(((kp - kfirst) / L::kRing) & 1); };
+  const int k_pro = min(klast, kfirst + L::kRing - 1);
+  if (tid == 0)
+    for (int kp = kfirst; kp <= k_pro; ++kp) {
+      const int sl = slot_of(kp);
+      mbar_arrive_expect_tx(&bars[sl], plane_bytes);
+      tma_load_plane(ring + sl * L::kPlaneBytes, map, tx0, ty0, kp + B.g, &bars[sl]);
+    }
+  int k_issued = k_pro;
+
+  const int q = (ty + 2) * kHX + (tx + 2);  // in-plane index of this thread's point
+  T F[NV];
+  bool aborted = false;
+  for (int k = t.k0; k < t.k1; ++k) {
+    bool late = false;
+    for (int kp = k - 1; kp <= k + 2; ++kp) {
+      long spins = 0;
+      while (!mbar_try_wait(&bars[slot_of(kp)], parity_of(kp)))
+        if (++spins > kMaxSpins) {
+          late = true;
+          break;
+        }
+    }
+    if (__syncthreads_or(late)) {
+      if (tid == 0) atomicOr(a.status, kStatusTmaTimeout);
+      aborted = true;
+      break;
+    }
+    const T *plm = reinterpret_cast<const T *>(ring + slot_of(k - 1) * L::kPlaneBytes);
+    const T *pl0 = reinterpret_cast<const T *>(ring + slot_of(k) * L::kPlaneBytes);
+    const T *pl1 = reinterpret_cast<const T *>(ring + slot_of(k + 1) * L::kPlaneBytes);
+    const T *pl2 = reinterpret_cast<const T *>(ring + slot_of(k + 2) * L::kPlaneBytes);
+    const int p = col + sk * k;
+    if (act) {
+#pragma unroll 1
+      for (int it = three_d ? 0 : 1; it < 3; ++it) {
+        const int d = it == 0 ? 2 : it - 1;
+        const int sd = d == 0 ? 1 : (d == 1 ? sj : sk);
+        SmemStencil<T> S{plm, pl0, pl1, pl2, q, d};
+        face_flux_gen<T, NS>(C, sRec, S, a.Pr, a.G, N, p, sd, d, F);
+#pragma unroll
+        for (int l = 0; l < NV; ++l)
+          if (l < nv) a.faces[(d * nv + l) * N + p] = F[l];
+      }
+    }
+    __syncthreads();  // plane k-1 is no longer read
+    if (k + 3 <= klast) {
+      if (tid == 0) {
+        const int sl = slot_of(k + 3);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_expect_tx(&bars[sl], plane_bytes);
+        tma_load_plane(ring + sl * L::kPlaneBytes, map, tx0, ty0, k + 3 + B.g, &bars[sl]);
+      }
+      k_issued = k + 3;
+    }
+  }
+  if (aborted) {
+    // let this CTA's copies in flight land before it exits (bounded)
+    if (tid == 0)
+      for (int kp = max(kfirst, k_issued - L::kRing + 1); kp <= k_issued; ++kp) {
+        long spins = 0;
+        while (!mbar_try_wait(&bars[slot_of(kp)], parity_of(kp)) && ++spins < kMaxSpins) {
+        }
+      }
+    __syncthreads();
+  }
+}
+
+}  // namespace ccb

@@ -179,13 +179,14 @@ int cc_time_kernels(cc_ctx *ctx, int n_steps, int scheme, double out_ms[6]);
  * first cc_init, or pinned by cc_set_tuning) and its measured time per
  * stage: variant 0 = fused stage kernel with L1 stencil reads, 1 = fused
  * with TMA-staged primitive planes, 2 = split (face kernel, then update
- * kernel); kz = k-planes per tile.  CC_AUTOTUNE=0 keeps the heuristic. */
+ * kernel), 3 = split with TMA-staged planes in the face kernel; kz =
+ * k-planes per tile.  CC_AUTOTUNE=0 keeps the heuristic. */
 int cc_tuning(cc_ctx *ctx, int *variant, int *kz, double *stage_ms);
 /* No counterpart in the reference (its launch shapes are fixed).  Pins the
  * stage-kernel configuration instead of autotuning it: variant -1 = autotune,
- * 0 = fused with L1 stencil reads, 1 = fused with TMA-staged planes (CC_MIXED
- * with 0 or 9 species only), 2 = split faces / update; kz = k-planes per
- * tile, 0 = autotune.  Before cc_init it applies to
+ * 0 = fused with L1 stencil reads, 1 = fused with TMA-staged planes, 2 =
+ * split faces / update, 3 = split with TMA-staged face planes (1 and 3: FP32
+ * bulk precision with 0 or 9 species); kz = k-planes per tile, 0 = autotune.  Before cc_init it applies to
  * the first cc_init; after it, the new configuration is timed and used from
  * the next cc_step on. */
 int cc_set_tuning(cc_ctx *ctx, int variant, int kz);

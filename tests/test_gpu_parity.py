@@ -99,10 +99,11 @@ def test_mixed_close_to_oracle(name, scheme):
 # Every stage-kernel variant on every case, with k-chunks that split the
 # sweep (kz=3) and that do not (kz=64).  The TMA variant exists for the
 # mixed path with 0 or 9 species.
+@pytest.mark.parametrize("variant", ["tma", "split-tma"])
 @pytest.mark.parametrize("kz", [3, 64])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_tma_variant_close_to_oracle(name, kz):
-    errs, status = compare(CASES[name], "rk3", 2, "mixed", "tma", kz)
+def test_tma_variant_close_to_oracle(name, kz, variant):
+    errs, status = compare(CASES[name], "rk3", 2, "mixed", variant, kz)
     assert status == 0
     tol = {"res": 5e-3, "dt": 1e-5}
     bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-4)}
@@ -128,9 +129,11 @@ def test_split_variant_mixed_close_to_oracle(name):
     assert not bad, errs
 
 
-@pytest.mark.parametrize("variant", ["l1", "split"])
+@pytest.mark.parametrize("variant", ["l1", "split", "split-tma"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_k_chunking_is_bit_identical(precision, variant):
+    if variant == "split-tma" and precision == "fp64":
+        pytest.skip("the TMA variants run in the FP32 bulk precision")
     """A face at a k-chunk boundary is computed by both chunks through the
     same call site: the state after two steps must not depend on kz."""
     case = CASES["multiblock"]
@@ -154,7 +157,7 @@ def test_variants_agree_at_64(precision):
     split-variant edge tiles span several CTAs per face layer) after two
     RK3 steps: FP64 to 1e-13, mixed to 1e-6 relative per field."""
     case = cases.case_box(64, species=cases.synthetic_species(), seed=5)
-    variants = ["l1", "split"] + (["tma"] if precision == "mixed" else [])
+    variants = ["l1", "split"] + (["tma", "split-tma"] if precision == "mixed" else [])
     out = {}
     for v in variants:
         d = cc.Driver.from_case(case, precision)
