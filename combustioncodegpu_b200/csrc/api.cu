@@ -649,6 +649,8 @@ int launch_stage(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt) {
 
 template <typename T, int NS>
 int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge) {
+  if ((variant == 1 || variant == 3) && !c->d_tmaps)
+    return fail(CC_ERR_STATE, "TMA variant without tensor maps");
   if (variant == 1) {
     CK((Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
   } else if (variant == 2 || variant == 3) {
@@ -720,6 +722,8 @@ int autotune(cc_ctx *c) {
   int best_variant = 0;
   if (c->force_kz > 0) kzs.assign(1, c->force_kz);
   std::vector<int> variants;
+  if ((c->force_variant == 1 || c->force_variant == 3) && !c->tma_ok)
+    return fail(CC_ERR_ARG, "the TMA variants need the FP32 bulk precision with 0 or 9 species (cc_set_tuning)");
   if (c->force_variant >= 0)
     variants.push_back(c->force_variant);
   else

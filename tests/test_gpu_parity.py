@@ -320,3 +320,14 @@ def test_checkpoint_restart_is_bit_identical(precision, tmp_path):
     with pytest.raises(RuntimeError, match="another layout or precision"):
         f.load_checkpoint(path)
     f.close()
+
+
+@pytest.mark.parametrize("variant", ["tma", "split-tma"])
+def test_tma_variant_refused_without_tensor_maps(variant):
+    """The TMA variants exist in the FP32 bulk precision only: pinning one on
+    an FP64 context fails at cc_init, before any kernel runs."""
+    d = cc.Driver.from_case(CASES["box"], "fp64")
+    d.set_tuning(variant, 4)
+    with pytest.raises(RuntimeError, match="TMA variants"):
+        d.initialize_computation()
+    d.close()
