@@ -510,9 +510,10 @@ def main():
     split = mixed["tuning"]["variant"] in ("split", "split-tma")
     stage_achieved = bpp * mixed["npts"] / (stage_ms / 1e3) / 1e9
     if split:  # dominant kernel: the face kernel
-        kname = "k_faces_tma<float,9>" if mixed["tuning"]["variant"] == "split-tma" else "k_faces<float,9>"
+        tma = mixed["tuning"]["variant"] == "split-tma"
+        kname = "k_faces_tma<float,9>" if tma else "k_faces<float,9>"
         kbpp, kms = face_kernel_bytes(9, "mixed"), kt["faces_ms"]
-        traffic = ncu_traffic("faces_kernel_box128_mixed")
+        traffic = ncu_traffic("faces_tma_kernel_box128_mixed" if tma else "faces_kernel_box128_mixed")
     else:
         kname, kbpp, kms = "k_stage<float,9>", bpp, stage_ms
         traffic = ncu_traffic("stage_kernel_box128_mixed")
