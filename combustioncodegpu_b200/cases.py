@@ -418,6 +418,28 @@ def case_box(n=128, L=2e-3, species=None, seed=1234, viscous=True):
     return {"name": "box%d" % n, "params": default_params(species, viscous=viscous), "blocks": [blk], "bcs": []}
 
 
+def case_box_distorted(n=16, L=2e-3, amp=0.08, species=None, seed=21):
+    """Periodic viscous box on a curvilinear grid: every coordinate is moved
+    by a periodic sinusoid of the others (amplitude amp of a cell), so the
+    metrics vary from point to point while the periodic continuation of the
+    lattice into the ghosts stays exact."""
+    species = species or synthetic_species()
+    dims = (n, n, n)
+    x, y, z = block_coordinates(dims, (L, L, L))
+    h = L / (n - 1)
+    w = 2 * math.pi / (h * (n - 1))  # one period across the block (the shared end layers coincide)
+    xd = x + amp * h * np.sin(w * y) * np.cos(w * z)
+    yd = y + amp * h * np.sin(w * z) * np.cos(w * x)
+    zd = z + amp * h * np.sin(w * x) * np.cos(w * y)
+    jac, met = jac_metric(xd, yd, zd)
+    bv, yk = multispecies_fields(dims, species, seed=seed)
+    faces = []
+    for a in range(3):
+        faces += periodic_raw(dims, a)
+    blk = {"dims": dims, "jac": jac, "metric": met, "bv": bv, "yk": yk, "boundaries": [], "inner_faces": faces}
+    return {"name": "box_distorted%d" % n, "params": default_params(species), "blocks": [blk], "bcs": []}
+
+
 def case_multiblock(sizes_per_axis, L_cell=2e-3 / 127, species=None, seed=7):
     """Conforming periodic layout of blocks (a,b,c) = (nx_a, ny_b, nz_c);
     neighbouring blocks share their interface layer; the layout wraps

@@ -33,6 +33,8 @@ def _cases():
         "multiblock": cases.case_multiblock(([6, 7], [6, 5], [5]), species=sp),
         "air_visc": mg.load("air_visc_o1")[0],
         "mixing": cases.case_mixing_layer(40, 24, 4, h=4e-3 / 39, delta=4e-4, species=sp),
+        # curvilinear periodic grid: non-zero geometric term of the gauge-pressure momentum fluxes
+        "box_distorted": cases.case_box_distorted(12, amp=0.3, species=sp),
     }
 
 
