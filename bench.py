@@ -187,9 +187,8 @@ def run_ours(args, rank, world, dist):
     states = {}
     for prec in ("fp64", "mixed"):
         d = cc.Driver.from_case(case, prec)
-        if args.variant != "auto":  # the TMA variants exist in the FP32 bulk precision only
-            d.set_tuning({"tma": "l1", "split-tma": "split"}.get(args.variant, args.variant) if prec == "fp64"
-                         else args.variant, 4)
+        if args.variant != "auto":  # the fused TMA variant exists in the FP32 bulk precision only
+            d.set_tuning("l1" if prec == "fp64" and args.variant == "tma" else args.variant, 4)
         d.initialize_computation()
         s = torch.cuda.ExternalStream(d.stream())
         info = d.info()

@@ -416,7 +416,7 @@ int setup_device(cc_ctx *c) {
                        c->stream));
   {
     const char *no_tma = std::getenv("CC_NO_TMA");
-    c->tma_ok = c->precision != CC_FP64 && (c->ns_key == 0 || c->ns_key == 9) && !(no_tma && no_tma[0] == '1');
+    c->tma_ok = (c->ns_key == 0 || c->ns_key == 9) && !(no_tma && no_tma[0] == '1');
     if (c->tma_ok)
       if (int r = build_tensor_maps(c)) return r;
     c->variant = 0;
@@ -627,6 +627,15 @@ int prof_event(cc_ctx *c, std::vector<cudaEvent_t> &pool, size_t &next) {
 
 const char *const kVariantName[4] = {"fused-l1", "fused-tma", "split", "split-tma"};
 
+// Variants this context can run: the TMA-staged ones need the tensor maps
+// (0 or 9 species); the fused TMA kernel's planes and flux planes fit in
+// shared memory in the FP32 bulk precision only.
+bool variant_ok(const cc_ctx *c, int v) {
+  if (v == 3) return c->tma_ok;
+  if (v == 1) return c->tma_ok && c->precision != CC_FP64;
+  return v == 0 || v == 2;
+}
+
 // One stage's kernels of the given variant over the current tile list:
 // one launch per kernel over all blocks, or (per_block) one per block.
 template <typename T, int NS>
@@ -722,13 +731,14 @@ int autotune(cc_ctx *c) {
   int best_variant = 0;
   if (c->force_kz > 0) kzs.assign(1, c->force_kz);
   std::vector<int> variants;
-  if ((c->force_variant == 1 || c->force_variant == 3) && !c->tma_ok)
-    return fail(CC_ERR_ARG, "the TMA variants need the FP32 bulk precision with 0 or 9 species (cc_set_tuning)");
+  if (c->force_variant >= 0 && !variant_ok(c, c->force_variant))
+    return fail(CC_ERR_ARG, "the TMA variants need 0 or 9 species, the fused one also the FP32 bulk precision "
+                            "(cc_set_tuning)");
   if (c->force_variant >= 0)
     variants.push_back(c->force_variant);
   else
     for (int v : {0, 1, 2, 3})
-      if ((v != 1 && v != 3) || c->tma_ok) variants.push_back(v);
+      if (variant_ok(c, v)) variants.push_back(v);
   for (int variant : variants) {
     for (int kz : kzs) {
       build_tiles_kz(c, kz);
@@ -1263,8 +1273,8 @@ int cc_set_tuning(cc_ctx *c, int variant, int kz) {
   c->force_variant = variant;
   c->force_kz = kz;
   if (!c->initialized) return 0;
-  if ((variant == 1 || variant == 3) && !c->tma_ok)
-    return fail(CC_ERR_ARG, "the TMA variants need the FP32 bulk precision with 0 or 9 species");
+  if (!variant_ok(c, variant))
+    return fail(CC_ERR_ARG, "the TMA variants need 0 or 9 species, the fused one also the FP32 bulk precision");
   destroy_graphs(c);
   int r = dispatch(c, [&](auto tt, auto nn) { return autotune<typename decltype(tt)::type, decltype(nn)::value>(c); });
   if (r) return r;

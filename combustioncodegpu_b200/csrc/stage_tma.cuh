@@ -316,7 +316,8 @@ namespace ccb {
 // regular tiles of k_faces, each computing the +x, +y, +z faces of its points
 // from a ring of 4 planes (k-1 .. k+2) in shared memory; plane k+3 is
 // requested into the slot of plane k-1 once the faces of plane k are done.
-// Without the fused kernel's flux planes the ring fits twice per SM.
+// Without the fused kernel's flux planes the ring fits twice per SM in FP32
+// (once in FP64, 208 KB).
 // Transport and geometry are read through L1; the edge tiles stay with
 // k_faces.  Waits are bounded as in k_stage_tma.
 template <typename T, int NS>
@@ -329,7 +330,7 @@ struct FacesTmaLayout {
 };
 
 template <typename T, int NS>
-__global__ void __launch_bounds__(kTX *kTY, 2)
+__global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
     k_faces_tma(const StageArgs<T> a, const CUtensorMap *__restrict__ maps, const __grid_constant__ ChemParams C) {
   using L = FacesTmaLayout<T, NS>;
   constexpr int NV = 5 + SpecCount<NS>::kArr;

@@ -99,8 +99,8 @@ def test_mixed_close_to_oracle(name, scheme):
 
 
 # Every stage-kernel variant on every case, with k-chunks that split the
-# sweep (kz=3) and that do not (kz=64).  The TMA variant exists for the
-# mixed path with 0 or 9 species.
+# sweep (kz=3) and that do not (kz=64).  The TMA variants exist for 0 or 9
+# species; the fused one for the FP32 bulk precision only.
 @pytest.mark.parametrize("variant", ["tma", "split-tma"])
 @pytest.mark.parametrize("kz", [3, 64])
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -112,11 +112,12 @@ def test_tma_variant_close_to_oracle(name, kz, variant):
     assert not bad, errs
 
 
+@pytest.mark.parametrize("variant", ["split", "split-tma"])
 @pytest.mark.parametrize("scheme", ["steady", "rk3"])
 @pytest.mark.parametrize("kz", [3, 64])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_split_variant_fp64_matches_oracle(name, kz, scheme):
-    errs, status = compare(CASES[name], scheme, 2, "fp64", "split", kz)
+def test_split_variant_fp64_matches_oracle(name, kz, scheme, variant):
+    errs, status = compare(CASES[name], scheme, 2, "fp64", variant, kz)
     assert status == 0
     bad = {k: v for k, v in errs.items() if not v < 1e-10}
     assert not bad, errs
@@ -134,8 +135,6 @@ def test_split_variant_mixed_close_to_oracle(name):
 @pytest.mark.parametrize("variant", ["l1", "split", "split-tma"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_k_chunking_is_bit_identical(precision, variant):
-    if variant == "split-tma" and precision == "fp64":
-        pytest.skip("the TMA variants run in the FP32 bulk precision")
     """A face at a k-chunk boundary is computed by both chunks through the
     same call site: the state after two steps must not depend on kz."""
     case = CASES["multiblock"]
@@ -159,7 +158,7 @@ def test_variants_agree_at_64(precision):
     split-variant edge tiles span several CTAs per face layer) after two
     RK3 steps: FP64 to 1e-13, mixed to 1e-6 relative per field."""
     case = cases.case_box(64, species=cases.synthetic_species(), seed=5)
-    variants = ["l1", "split"] + (["tma", "split-tma"] if precision == "mixed" else [])
+    variants = ["l1", "split", "split-tma"] + (["tma"] if precision == "mixed" else [])
     out = {}
     for v in variants:
         d = cc.Driver.from_case(case, precision)
@@ -324,12 +323,40 @@ def test_checkpoint_restart_is_bit_identical(precision, tmp_path):
     f.close()
 
 
-@pytest.mark.parametrize("variant", ["tma", "split-tma"])
-def test_tma_variant_refused_without_tensor_maps(variant):
-    """The TMA variants exist in the FP32 bulk precision only: pinning one on
-    an FP64 context fails at cc_init, before any kernel runs."""
+# A species count without a compiled specialisation (4: H2, O2, H2O, N2) runs
+# the kernels' runtime-count path.
+SP4 = cases.synthetic_species([cases.H2O2_N2_SPECIES[i] for i in (0, 1, 2, 8)])
+
+
+@pytest.mark.parametrize("variant", ["l1", "split"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_runtime_species_count_matches_oracle(precision, variant):
+    case = cases.case_box_distorted(10, amp=0.3, species=SP4, seed=4)
+    errs, status = compare(case, "rk3", 2, precision, variant, 3)
+    assert status == 0
+    tol = {"res": 5e-3, "dt": 1e-5} if precision == "mixed" else {}
+    bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-4 if precision == "mixed" else 1e-10)}
+    assert not bad, errs
+
+
+def test_fused_tma_variant_refused_in_fp64():
+    """The fused TMA variant exists in the FP32 bulk precision only (its FP64
+    planes do not fit in shared memory): pinning it on an FP64 context fails
+    at cc_init, before any kernel runs."""
     d = cc.Driver.from_case(CASES["box"], "fp64")
-    d.set_tuning(variant, 4)
+    d.set_tuning("tma", 4)
     with pytest.raises(RuntimeError, match="TMA variants"):
         d.initialize_computation()
     d.close()
+
+
+def test_tma_variants_refused_without_tensor_maps():
+    """Tensor maps exist for 0 or 9 species only: pinning a TMA variant on a
+    context with another species count fails at cc_init."""
+    case = cases.case_box(8, species=SP4, seed=2)
+    for variant in ("tma", "split-tma"):
+        d = cc.Driver.from_case(case, "mixed")
+        d.set_tuning(variant, 4)
+        with pytest.raises(RuntimeError, match="TMA variants"):
+            d.initialize_computation()
+        d.close()
