@@ -717,7 +717,7 @@ int autotune(cc_ctx *c) {
   int max_mz = 1;
   for (const auto &b : c->blocks) max_mz = std::max(max_mz, b.mz);
   std::vector<int> kzs;
-  for (int kz : {4, 8, 16, 32, 64, 128})
+  for (int kz : {2, 3, 4, 6, 8, 16, 32, 64, 128})
     if (kz <= max_mz) kzs.push_back(kz);
   kzs.push_back(max_mz);
   kzs.push_back(heuristic_kz(c));
