@@ -99,7 +99,8 @@ struct cc_ctx {
   int64_t *d_vel_zero = nullptr;  // wall-face points (vel = 0 after the wall condition)
   uint32_t *d_skip_dt = nullptr;  // bitmask: interior points the halo rewrites
   int renorm = -1;                // Y renormalisation: -1 = by precision (mixed on, FP64 off)
-  int variant = 0;                // stage kernels: 0 fused (L1 stencil reads), 1 fused TMA planes, 2 split faces/update
+  int variant = 0;                // stage kernels: 0 fused (L1 stencil reads), 1 fused TMA planes, 2 split faces/update,
+                                  // 3 split with TMA-staged face planes
   std::vector<Tile> hedges;       // split variant: tiles of the minus-side face layers
   std::vector<int> tile_begin, edge_begin;  // per block: first tile / edge tile (lists are block-ordered), + end
   bool per_block = false;         // cc_set_launch_mode: one launch per block per kernel instead of one per stage
@@ -115,12 +116,15 @@ struct cc_ctx {
   int kz = 1;                     // k-chunk of the stage tiles
   double tuned_ms = 0;            // stage-kernel time of the chosen configuration
   CUtensorMap *d_tmaps = nullptr; // [2][n_blocks]: primitive arenas P[0], P[1] per block
+  LusgsArgs lu{};                 // LU-SGS work arrays (allocated by the first LU-SGS step)
+  int lu_planes = 0;              // sweep hyperplanes: max over blocks of mx + my + mz - 2
+  int lu_cols = 0;                // max over blocks of my * mz (threads of a sweep launch per block)
   int n_partials = 296;
 
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   bool use_graph = true;
-  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  cudaGraphExec_t graph[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
   int64_t device_bytes = 0;
   std::vector<void *> allocs;
   // kernel timing (cc_time_kernels): events around every stage and halo launch
@@ -679,17 +683,81 @@ int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, i
   return 0;
 }
 
+// The closure transport of the new state (when on), the end of the stage's
+// timing bracket and the halo program.
 template <typename T, int NS>
-int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin) {
-  const int nt = (int)c->htiles.size();
-  if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
-  if (int r = launch_stage<T, NS>(c, a, pc, c->variant, nt)) return r;
+int after_stage(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin) {
   if (c->closure_on) CK((Launch<T, NS>::props_mlp(a.Pn, a.Prn, c->N, &c->cl, c->d_status, c->chem, c->stream)));
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
   if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next)) return r;
   if (a.vel) CK(launch_zero_points(c->d_vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream));
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
+  return 0;
+}
+
+template <typename T, int NS>
+int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin) {
+  const int nt = (int)c->htiles.size();
+  if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
+  if (int r = launch_stage<T, NS>(c, a, pc, c->variant, nt)) return r;
+  return after_stage<T, NS>(c, a, pn, pc, qout, qin);
+}
+
+// LU-SGS steady step (lusgs.cuh): the face fluxes of the current state (the
+// split variant's face kernels), the right-hand side and diagonal, the lower
+// and upper sweeps one hyperplane per launch, Q += dQ with the primitive
+// recovery, then the halo program as after an explicit step.
+template <typename T, int NS>
+int lusgs_and_halo(cc_ctx *c, StageArgs<T> a, int pn, int pc) {
+  const int nt = (int)c->htiles.size(), n_edge = (int)c->hedges.size(), nb = (int)c->blocks.size();
+  if (!c->lu.R) return fail(CC_ERR_STATE, "LU-SGS work arrays missing");
+  a.faces = (T *)c->faces;
+  a.edge_tiles = c->d_edges;
+  if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
+  if (c->tma_ok && c->d_tmaps) {
+    CK((Launch<T, NS>::faces_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
+    CK((Launch<T, NS>::faces(a, c->chem, 0, n_edge, c->stream)));
+  } else {
+    CK((Launch<T, NS>::faces(a, c->chem, nt, n_edge, c->stream)));
+  }
+  if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
+  LusgsArgs L = c->lu;
+  CK((Launch<T, NS>::lusgs_rhs(a, L, c->chem, nt, c->stream)));
+  for (int h = 0; h < c->lu_planes; ++h) {
+    L.h = h;
+    CK((Launch<T, NS>::lusgs_sweep(a, L, c->chem, 1, nb, c->lu_cols, c->stream)));
+  }
+  for (int h = c->lu_planes - 1; h >= 0; --h) {
+    L.h = h;
+    CK((Launch<T, NS>::lusgs_sweep(a, L, c->chem, -1, nb, c->lu_cols, c->stream)));
+  }
+  a.gcl = nullptr;  // the geometric term is part of the right-hand side
+  CK((Launch<T, NS>::lusgs_update(a, L, c->chem, nt, c->stream)));
+  return after_stage<T, NS>(c, a, pn, pc, c->Q[c->qcur], c->Q[c->qcur]);
+}
+
+// Work arrays of the LU-SGS step, allocated once (outside any capture).
+int lusgs_alloc(cc_ctx *c) {
+  if (c->lu.R) return 0;
+  const size_t N = (size_t)c->N;
+  void *p;
+  if (dev_alloc(c, &p, sizeof(double) * N * nv_of(c))) return CC_ERR_CUDA;
+  c->lu.R = (double *)p;
+  if (dev_alloc(c, &p, sizeof(double) * N * 3)) return CC_ERR_CUDA;
+  c->lu.rad = (double *)p;
+  if (dev_alloc(c, &p, sizeof(double) * N)) return CC_ERR_CUDA;
+  c->lu.diag = (double *)p;
+  if (dev_alloc(c, &p, sizeof(double) * N)) return CC_ERR_CUDA;
+  c->lu.gam = (double *)p;
+  if (dev_alloc(c, &p, sizeof(double) * N * std::max(1, c->chem.ns))) return CC_ERR_CUDA;
+  c->lu.psi = (double *)p;
+  c->lu_planes = c->lu_cols = 0;
+  for (const auto &b : c->blocks) {
+    c->lu_planes = std::max(c->lu_planes, b.mx + b.my + b.mz - 2);
+    c->lu_cols = std::max(c->lu_cols, b.my * b.mz);
+  }
+  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
@@ -791,6 +859,15 @@ int enqueue_step(cc_ctx *c, int scheme) {
     a.Qin = c->Q[c->qcur], a.Qn = nullptr, a.Qout = c->Q[c->qcur];
     a.a = 0.0, a.b = 1.0, a.local_dt = 1, a.dt_next = nullptr, a.vel = c->d_vel;
     if (int r = stage_and_halo<T, NS>(c, a, pn, pc, c->Q[c->qcur], c->Q[c->qcur])) return r;
+    c->cur = pn;
+    return 0;
+  }
+  if (scheme == CC_STEADY_LUSGS) {
+    const int pc = c->cur, pn = 1 - c->cur;
+    a.P = (const T *)c->P[pc], a.Pn = (T *)c->P[pn], a.Pr = (const T *)c->Pr[pc], a.Prn = (T *)c->Pr[pn];
+    a.Qin = c->Q[c->qcur], a.Qn = nullptr, a.Qout = c->Q[c->qcur];
+    a.a = 0.0, a.b = 1.0, a.local_dt = 1, a.dt_next = nullptr, a.vel = c->d_vel;
+    if (int r = lusgs_and_halo<T, NS>(c, a, pn, pc)) return r;
     c->cur = pn;
     return 0;
   }
@@ -1072,8 +1149,11 @@ int cc_init(cc_ctx *c, int precision) {
 int cc_step(cc_ctx *c, int n_steps, int scheme, int want_residual) {
   if (int r = check_ctx(c)) return r;
   if (!c->initialized) return fail(CC_ERR_STATE, "cc_step before cc_init");
-  if (scheme != CC_RK3 && scheme != CC_STEADY_EULER) return fail(CC_ERR_ARG, "unknown time scheme");
+  if (scheme != CC_RK3 && scheme != CC_STEADY_EULER && scheme != CC_STEADY_LUSGS)
+    return fail(CC_ERR_ARG, "unknown time scheme");
   if (n_steps < 0) return fail(CC_ERR_ARG, "n_steps must be >= 0");
+  if (scheme == CC_STEADY_LUSGS)
+    if (int r = lusgs_alloc(c)) return r;
   if (c->state_dirty) {
     destroy_graphs(c);
     int r = dispatch(c, [&](auto tt, auto nn) { return derive_state<typename decltype(tt)::type, decltype(nn)::value>(c); });
@@ -1212,6 +1292,10 @@ int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[6]) {
   if (int r = check_ctx(c)) return r;
   if (!c->initialized) return fail(CC_ERR_STATE, "cc_time_kernels before cc_init");
   if (!out_ms || n_steps < 1) return fail(CC_ERR_ARG, "bad arguments");
+  if (scheme != CC_RK3 && scheme != CC_STEADY_EULER && scheme != CC_STEADY_LUSGS)
+    return fail(CC_ERR_ARG, "unknown time scheme");
+  if (scheme == CC_STEADY_LUSGS)
+    if (int r = lusgs_alloc(c)) return r;
   if (c->state_dirty) {
     destroy_graphs(c);
     int r = dispatch(c, [&](auto tt, auto nn) { return derive_state<typename decltype(tt)::type, decltype(nn)::value>(c); });

@@ -152,6 +152,16 @@ struct StageArgs {
   int n_regular;
 };
 
+// Work arrays of the LU-SGS steady step (lusgs.cuh).
+struct LusgsArgs {
+  double *R;     // [n_var][N]: dq, then dQ*, then dQ
+  double *rad;   // [3][N]: r_d = J (sigma_d + 2 sigv_d)
+  double *diag;  // [N]: J / dt_local + sum_d r_d
+  double *gam;   // [N]: gamma of the current state
+  double *psi;   // [n_spec][N]: dp / d(rho Y_k) at fixed rho e: gamma R_k T - (gamma - 1) h_k(T)
+  int h;         // hyperplane i + j + k of a sweep launch
+};
+
 // A source reference of the halo program: kind 0 = point of the new state,
 // 1 = point of the previous state, 2 = scratch slot of an evaluated node.
 struct HaloRef {

@@ -7,6 +7,7 @@
 #include "stage_tma.cuh"
 #include "stage_split.cuh"
 #include "closure.cuh"
+#include "lusgs.cuh"
 
 namespace ccb {
 
@@ -112,6 +113,35 @@ template <typename T, int NS>
 cudaError_t Launch<T, NS>::stage(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;
   k_stage<T, NS><<<n_tiles, dim3(kTX, kTY), stage_smem(), s>>>(a, C);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::lusgs_rhs(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int n_tiles,
+                                     cudaStream_t s) {
+  if (n_tiles <= 0) return cudaSuccess;
+  k_lusgs_rhs<T, NS><<<n_tiles, dim3(kTX, kTY), 0, s>>>(a, L, C);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::lusgs_sweep(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int dir,
+                                       int nblocks, int max_cols, cudaStream_t s) {
+  if (nblocks <= 0 || max_cols <= 0) return cudaSuccess;
+  const int tpb = 256;
+  const dim3 grid((unsigned)((max_cols + tpb - 1) / tpb), (unsigned)nblocks);
+  if (dir > 0)
+    k_lusgs_sweep<T, NS, 1><<<grid, tpb, 0, s>>>(a, L, C);
+  else
+    k_lusgs_sweep<T, NS, -1><<<grid, tpb, 0, s>>>(a, L, C);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::lusgs_update(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int n_tiles,
+                                        cudaStream_t s) {
+  if (n_tiles <= 0) return cudaSuccess;
+  k_lusgs_update<T, NS><<<n_tiles, dim3(kTX, kTY), update_smem(), s>>>(a, L, C);
   return cudaGetLastError();
 }
 

@@ -32,6 +32,14 @@ struct Launch {
   // geometric term of the gauge-pressure momentum fluxes (k_gcl)
   static cudaError_t gcl(const BlockInfo *blocks, int nblocks, const T *G, int64_t N, int64_t n_interior,
                          double *out, cudaStream_t s);
+  // LU-SGS steady step (lusgs.cuh): right-hand side and diagonal over the
+  // tiles, one sweep hyperplane (dir +1 lower, -1 upper) over all blocks, Q += dQ
+  static cudaError_t lusgs_rhs(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int n_tiles,
+                               cudaStream_t s);
+  static cudaError_t lusgs_sweep(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int dir,
+                                 int nblocks, int max_cols, cudaStream_t s);
+  static cudaError_t lusgs_update(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int n_tiles,
+                                  cudaStream_t s);
   static cudaError_t halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   static cudaError_t halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   static cudaError_t cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, double *vel,

@@ -48,7 +48,10 @@ enum cc_precision {
 
 enum cc_time_scheme {
   CC_RK3 = 0,          /* SSP-RK3 with a global time step (min of the local CFL step) */
-  CC_STEADY_EULER = 1  /* the reference's loop: explicit Euler with the per-point local step */
+  CC_STEADY_EULER = 1, /* the reference's loop: explicit Euler with the per-point local step */
+  CC_STEADY_LUSGS = 2  /* implicit steady step: scalar LU-SGS with the per-point local step
+                          (the scheme the reference declares as temporal_scheme 1,
+                          TemporalScheme.cuh:19-21, Driver.cu:318-321, without a body) */
 };
 
 /* Scalar parameters and species tables, as in DParameter (DParameter.h:9-39)

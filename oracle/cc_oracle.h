@@ -91,6 +91,9 @@ int oc_init(oc_solver *s);
 /* One pass of the reference's steady explicit-Euler loop body with the
  * per-point local time step (Driver.cu:189-244); renorm_y as for RK3. */
 int oc_steady_step(oc_solver *s, int renorm_y);
+/* One implicit steady step: scalar LU-SGS with the per-point local time step
+ * (the scheme the reference declares as temporal_scheme 1 without a body). */
+int oc_lusgs_step(oc_solver *s, int renorm_y);
 /* One SSP-RK3 step with a global time step; renorm_y renormalises the
  * mass fractions to sum 1 after each stage. */
 int oc_rk3_step(oc_solver *s, int renorm_y);
@@ -115,6 +118,9 @@ void oc_kat_face_inviscid(const oc_params *p, const double *pv4, const double ml
 void oc_kat_h_cp(const oc_params *p, double t, double *h, double *cp);
 void oc_kat_transport(const oc_params *p, double t, const double *Y, double *mu, double *lam, double *rhod);
 double oc_kat_temperature(const oc_params *p, const double *q5, const double *Y, double t0);
+/* The LU-SGS Jacobian-vector product dF = A dQ of the flux along k. */
+void oc_kat_lusgs_jac_vec(int nv, const double *Q, double p, double gam, const double *psi, const double k[3],
+                          const double *dQ, double *dF);
 int oc_apply_boundaries(oc_solver *s);
 
 #ifdef __cplusplus

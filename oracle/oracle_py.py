@@ -79,6 +79,7 @@ def lib():
         L.oc_init.argtypes = [ctypes.c_void_p]
         L.oc_steady_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oc_rk3_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oc_lusgs_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oc_compute_dq.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.oc_get_state.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
         L.oc_get_props.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
@@ -163,6 +164,10 @@ class Oracle:
     def steady_step(self, n=1, renorm_y=False):
         for _ in range(n):
             lib().oc_steady_step(self.s, 1 if renorm_y else 0)
+
+    def lusgs_step(self, n=1, renorm_y=False):
+        for _ in range(n):
+            lib().oc_lusgs_step(self.s, 1 if renorm_y else 0)
 
     def rk3_step(self, n=1, renorm_y=False):
         for _ in range(n):
@@ -305,6 +310,18 @@ def kat_temperature(species, q5, Y, t0):
     L.oc_kat_temperature.restype = ctypes.c_double
     L.oc_kat_temperature.argtypes = [ctypes.POINTER(OcParams), _dp, _dp, ctypes.c_double]
     return L.oc_kat_temperature(ctypes.byref(p), _p(q), _p(Y), float(t0))
+
+
+def kat_lusgs_jac_vec(Q, p, gam, psi, k, dQ):
+    Q = np.ascontiguousarray(Q, dtype=np.float64)
+    dQ = np.ascontiguousarray(dQ, dtype=np.float64)
+    psi = np.ascontiguousarray(psi if len(psi) else [0.0], dtype=np.float64)
+    k = np.ascontiguousarray(k, dtype=np.float64)
+    dF = np.zeros_like(Q)
+    L = lib()
+    L.oc_kat_lusgs_jac_vec.argtypes = [ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp]
+    L.oc_kat_lusgs_jac_vec(len(Q), _p(Q), float(p), float(gam), _p(psi), _p(k), _p(dQ), _p(dF))
+    return dF
 
 
 def apply_boundaries(oracle):

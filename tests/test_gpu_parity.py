@@ -52,6 +52,8 @@ def compare(case, scheme, n, precision, variant="auto", kz=0):
         assert d.tuning()["variant"] == variant
     if scheme == "rk3":
         o.rk3_step(n, renorm_y=renorm)
+    elif scheme == "lusgs":
+        o.lusgs_step(n, renorm_y=renorm)
     else:
         o.steady_step(n, renorm_y=renorm)
     d.simulate(n, scheme, residual=True)
@@ -321,6 +323,46 @@ def test_checkpoint_restart_is_bit_identical(precision, tmp_path):
     with pytest.raises(RuntimeError, match="another layout or precision"):
         f.load_checkpoint(path)
     f.close()
+
+
+# LU-SGS steady steps (the implicit scheme of temporal_scheme 1) against the
+# oracle's lexicographic sweeps: at the cases' CFL 0.5 and at CFL 5.
+def _with_cfl(case, cfl):
+    c = dict(case)
+    c["params"] = dict(case["params"], cfl=cfl)
+    return c
+
+
+@pytest.mark.parametrize("cfl", [0.5, 5.0])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_lusgs_fp64_matches_oracle(name, cfl):
+    errs, status = compare(_with_cfl(CASES[name], cfl), "lusgs", 3, "fp64")
+    assert status == 0
+    bad = {k: v for k, v in errs.items() if not v < 1e-10}
+    assert not bad, errs
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_lusgs_mixed_close_to_oracle(name):
+    errs, status = compare(_with_cfl(CASES[name], 5.0), "lusgs", 3, "mixed")
+    assert status == 0
+    tol = {"res": 5e-3, "dt": 1e-5}
+    bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-4)}
+    assert not bad, errs
+
+
+def test_lusgs_graph_replay_equals_launches():
+    case = _with_cfl(CASES["multiblock"], 5.0)
+    out = []
+    for graph in (True, False):
+        d = cc.Driver.from_case(case, "mixed")
+        d.use_graph(graph)
+        d.initialize_computation()
+        d.simulate(3, "lusgs")
+        out.append([d.field[b].get_state()[2] for b in range(len(case["blocks"]))])
+        d.close()
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
 
 
 # A species count without a compiled specialisation (4: H2, O2, H2O, N2) runs
