@@ -41,10 +41,11 @@ def parse():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--err-steps", type=int, default=1000, help="steps of the mixed-vs-FP64 error check")
     ap.add_argument("--workload", default="box128",
-                    choices=["box128", "multiblock64", "mixing_layer", "box256_closure"],
+                    choices=["box128", "multiblock64", "mixing_layer", "box256_closure", "box128_lusgs"],
                     help="box128: the headline 128^3 box; multiblock64: 64 uneven blocks, batched vs "
                          "per-block; mixing_layer: 1024x512x4 precision study (FP64 / mixed / FP32); "
-                         "box256_closure: 256^3 box, exact transport vs the learned closure")
+                         "box256_closure: 256^3 box, exact transport vs the learned closure; "
+                         "box128_lusgs: LU-SGS steady steps on the 128^3 box")
     ap.add_argument("--study-steps", default="100,1000,2000", help="mixing_layer: error snapshot steps")
     ap.add_argument("--variant", default="auto", choices=["auto", "l1", "tma", "split", "split-tma"],
                     help="stage kernels: autotuned (default) or pinned (profiling runs, where the autotuner's "
@@ -319,6 +320,55 @@ def run_multiblock(args):
     print(json.dumps(line), flush=True)
 
 
+def run_lusgs(args):
+    """LU-SGS steady steps (the implicit scheme of temporal_scheme 1) on the
+    128^3 box at CFL 5, both precisions: step time from CUDA events around
+    graph replays, and the split of a step from an event-timed run (face
+    kernels; right-hand side + 2 x (mx+my+mz-2) sweep hyperplanes + update;
+    halo program)."""
+    import torch
+    import combustioncodegpu_b200 as cc
+    from combustioncodegpu_b200 import cases
+
+    case = cases.case_box(args.n, species=cases.synthetic_species(), seed=1234)
+    case["params"]["cfl"] = 5.0
+    res = {}
+    for prec in ("mixed", "fp64"):
+        d = cc.Driver.from_case(case, prec)
+        d.initialize_computation()
+        s = torch.cuda.ExternalStream(d.stream())
+        npts = d.info()["n_points"]
+        d.simulate(args.warmup, "lusgs")
+        d.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            e0.record(s)
+            d.simulate(args.steps, "lusgs")
+            e1.record(s)
+            e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        kt = d.time_kernels(2, "lusgs")
+        res[prec] = {"value": npts * args.steps / (ms / 1e3) / 1e6, "ms_per_step": ms / args.steps,
+                     "split_ms": {"faces": kt["faces_ms"], "rhs_sweeps_update": kt["update_ms"],
+                                  "halo": kt["halo_ms"]},
+                     "clocks": clk.summary(), "status": d.status(), "npts": npts}
+        d.close()
+    m = res["mixed"]
+    n = args.n
+    line = {"metric": "Mcell-updates/s per LU-SGS steady step", "value": m["value"], "unit": "Mcell-updates/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 fluxes/transport + f64 conserved/sweeps/Newton", "data": "synthetic",
+            "config": {"workload": "box%d_9sp_viscous_lusgs" % n, "grid": "%d^3 points, 2 mm periodic cube" % n,
+                       "scheme": "LU-SGS, local time step, CFL 5", "precision": "mixed",
+                       "sweep_launches_per_step": 2 * (3 * n - 2), "l2": "inputs larger than L2 (no flush)",
+                       "graph": "one CUDA graph per step"},
+            "split_ms": m["split_ms"], "plain_fp64": {k: res["fp64"][k] for k in ("value", "ms_per_step", "split_ms")},
+            "clocks": m["clocks"], "status": {k: v["status"] for k, v in res.items()}}
+    print(json.dumps(line), flush=True)
+
+
 def run_mixing_layer(args):
     """Precision study on the 1024x512x4 H2/air temporal mixing layer: FP64,
     mixed and full-FP32 runs from the same state (Y renormalised in all
@@ -487,10 +537,10 @@ def main():
             dist.destroy_process_group()
         return
 
-    if args.workload in ("multiblock64", "mixing_layer", "box256_closure"):
+    if args.workload in ("multiblock64", "mixing_layer", "box256_closure", "box128_lusgs"):
         if rank == 0:
             {"multiblock64": run_multiblock, "mixing_layer": run_mixing_layer,
-             "box256_closure": run_closure}[args.workload](args)
+             "box256_closure": run_closure, "box128_lusgs": run_lusgs}[args.workload](args)
         if dist:
             dist.destroy_process_group()
         return

@@ -117,8 +117,10 @@ struct cc_ctx {
   double tuned_ms = 0;            // stage-kernel time of the chosen configuration
   CUtensorMap *d_tmaps = nullptr; // [2][n_blocks]: primitive arenas P[0], P[1] per block
   LusgsArgs lu{};                 // LU-SGS work arrays (allocated by the first LU-SGS step)
-  int lu_planes = 0;              // sweep hyperplanes: max over blocks of mx + my + mz - 2
-  int lu_cols = 0;                // max over blocks of my * mz (threads of a sweep launch per block)
+  std::vector<int64_t> lu_hb;     // sweep positions where each hyperplane begins, + end
+  SweepWork lu_w{};               // chunk tables and counters of the one-launch sweeps
+  bool lu_per_plane = false;      // CC_LUSGS_SWEEP=planes: one launch per hyperplane instead
+  int lu_ctas = 0;                // SMs a one-launch sweep fills with resident CTAs
   int n_partials = 296;
 
   cudaStream_t stream = nullptr;
@@ -710,7 +712,7 @@ int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qou
 // recovery, then the halo program as after an explicit step.
 template <typename T, int NS>
 int lusgs_and_halo(cc_ctx *c, StageArgs<T> a, int pn, int pc) {
-  const int nt = (int)c->htiles.size(), n_edge = (int)c->hedges.size(), nb = (int)c->blocks.size();
+  const int nt = (int)c->htiles.size(), n_edge = (int)c->hedges.size();
   if (!c->lu.R) return fail(CC_ERR_STATE, "LU-SGS work arrays missing");
   a.faces = (T *)c->faces;
   a.edge_tiles = c->d_edges;
@@ -724,39 +726,125 @@ int lusgs_and_halo(cc_ctx *c, StageArgs<T> a, int pn, int pc) {
   if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
   LusgsArgs L = c->lu;
   CK((Launch<T, NS>::lusgs_rhs(a, L, c->chem, nt, c->stream)));
-  for (int h = 0; h < c->lu_planes; ++h) {
-    L.h = h;
-    CK((Launch<T, NS>::lusgs_sweep(a, L, c->chem, 1, nb, c->lu_cols, c->stream)));
-  }
-  for (int h = c->lu_planes - 1; h >= 0; --h) {
-    L.h = h;
-    CK((Launch<T, NS>::lusgs_sweep(a, L, c->chem, -1, nb, c->lu_cols, c->stream)));
+  if (c->lu_per_plane) {
+    const int H = (int)c->lu_hb.size() - 1;
+    for (int h = 0; h < H; ++h) {
+      L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1];
+      CK((Launch<T, NS>::lusgs_sweep(L, c->chem, 1, c->stream)));
+    }
+    for (int h = H - 1; h >= 0; --h) {
+      L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1];
+      CK((Launch<T, NS>::lusgs_sweep(L, c->chem, -1, c->stream)));
+    }
+  } else {
+    CK((Launch<T, NS>::lusgs_sweep_all(L, &c->lu_w, c->chem, 1, c->lu_ctas, c->stream)));
+    CK((Launch<T, NS>::lusgs_sweep_all(L, &c->lu_w, c->chem, -1, c->lu_ctas, c->stream)));
   }
   a.gcl = nullptr;  // the geometric term is part of the right-hand side
   CK((Launch<T, NS>::lusgs_update(a, L, c->chem, nt, c->stream)));
   return after_stage<T, NS>(c, a, pn, pc, c->Q[c->qcur], c->Q[c->qcur]);
 }
 
-// Work arrays of the LU-SGS step, allocated once (outside any capture).
+// Work arrays of the LU-SGS step and its sweep order, built once (outside
+// any capture): interior points sorted by hyperplane h = i + j + k, then
+// block, k, j; per point the positions of its six neighbours in the block.
 int lusgs_alloc(cc_ctx *c) {
   if (c->lu.R) return 0;
-  const size_t N = (size_t)c->N;
-  void *p;
-  if (dev_alloc(c, &p, sizeof(double) * N * nv_of(c))) return CC_ERR_CUDA;
-  c->lu.R = (double *)p;
-  if (dev_alloc(c, &p, sizeof(double) * N * 3)) return CC_ERR_CUDA;
-  c->lu.rad = (double *)p;
-  if (dev_alloc(c, &p, sizeof(double) * N)) return CC_ERR_CUDA;
-  c->lu.diag = (double *)p;
-  if (dev_alloc(c, &p, sizeof(double) * N)) return CC_ERR_CUDA;
-  c->lu.gam = (double *)p;
-  if (dev_alloc(c, &p, sizeof(double) * N * std::max(1, c->chem.ns))) return CC_ERR_CUDA;
-  c->lu.psi = (double *)p;
-  c->lu_planes = c->lu_cols = 0;
-  for (const auto &b : c->blocks) {
-    c->lu_planes = std::max(c->lu_planes, b.mx + b.my + b.mz - 2);
-    c->lu_cols = std::max(c->lu_cols, b.my * b.mz);
+  const int64_t N = c->N, S = c->n_int;
+  const int lp = lusgs_lanes(nv_of(c));
+  if (3 * lp * S >= (int64_t)1 << 31 || N >= (int64_t)1 << 31)
+    return fail(CC_ERR_ARG, "LU-SGS: too many points for 32-bit sweep offsets");
+  std::vector<int> pos((size_t)N, -1), lo((size_t)(3 * S), -1), hi((size_t)(3 * S), -1);
+  std::vector<int64_t> pt((size_t)S);
+  int H = 0;
+  for (const auto &b : c->blocks) H = std::max(H, b.mx + b.my + b.mz - 2);
+  c->lu_hb.assign((size_t)H + 1, 0);
+  int64_t sp = 0;
+  for (int h = 0; h < H; ++h) {
+    c->lu_hb[h] = sp;
+    for (size_t bi = 0; bi < c->blocks.size(); ++bi) {
+      const HostBlock &b = c->blocks[bi];
+      const BlockInfo &B = c->hblocks[bi];
+      for (int k = std::max(0, h - (b.mx - 1) - (b.my - 1)); k <= std::min(b.mz - 1, h); ++k)
+        for (int j = std::max(0, h - k - (b.mx - 1)); j <= std::min(b.my - 1, h - k); ++j) {
+          const int i = h - j - k;
+          const int64_t p = B.base + i + (int64_t)B.nx * j + (int64_t)B.nx * B.ny * k;
+          pos[(size_t)p] = (int)sp;
+          pt[(size_t)sp++] = p;
+        }
+    }
   }
+  c->lu_hb[H] = sp;
+  if (sp != S) return fail(CC_ERR_STATE, "LU-SGS: sweep order does not cover the interior");
+  for (size_t bi = 0; bi < c->blocks.size(); ++bi) {
+    const HostBlock &b = c->blocks[bi];
+    const BlockInfo &B = c->hblocks[bi];
+    const int64_t st[3] = {1, (int64_t)B.nx, (int64_t)B.nx * B.ny};
+    const int m[3] = {b.mx, b.my, b.mz};
+    for (int k = 0; k < b.mz; ++k)
+      for (int j = 0; j < b.my; ++j)
+        for (int i = 0; i < b.mx; ++i) {
+          const int64_t p = B.base + i + st[1] * j + st[2] * k;
+          const int64_t s = pos[(size_t)p];
+          const int id[3] = {i, j, k};
+          for (int d = 0; d < 3; ++d) {
+            if (id[d] >= 1) lo[(size_t)(d * S + s)] = pos[(size_t)(p - st[d])];
+            if (id[d] + 1 < m[d]) hi[(size_t)(d * S + s)] = pos[(size_t)(p + st[d])];
+          }
+        }
+  }
+  void *p;
+  auto dbl = [&](double **dst, int64_t n) -> int {
+    if (dev_alloc(c, &p, sizeof(double) * (size_t)n)) return CC_ERR_CUDA;
+    *dst = (double *)p;
+    return 0;
+  };
+  if (dbl(&c->lu.R, lp * S) || dbl(&c->lu.Qs, lp * S) || dbl(&c->lu.ps, S) || dbl(&c->lu.kv, 9 * S) ||
+      dbl(&c->lu.rad, 3 * S) || dbl(&c->lu.rdiag, S) || dbl(&c->lu.vel, 4 * S) || dbl(&c->lu.gam, S) ||
+      dbl(&c->lu.psi, lp * S) || dbl(&c->lu.Cn, 3 * lp * S))
+    return CC_ERR_CUDA;
+  int *ip[3];
+  const size_t nint[3] = {(size_t)N, (size_t)(3 * S), (size_t)(3 * S)};
+  const std::vector<int> *src[3] = {&pos, &lo, &hi};
+  for (int q = 0; q < 3; ++q) {
+    if (dev_alloc(c, &p, sizeof(int) * nint[q])) return CC_ERR_CUDA;
+    ip[q] = (int *)p;
+    CK(cudaMemcpyAsync(ip[q], src[q]->data(), sizeof(int) * nint[q], cudaMemcpyHostToDevice, c->stream));
+  }
+  c->lu.pos = ip[0], c->lu.lo = ip[1], c->lu.hi = ip[2];
+  c->lu.S = S, c->lu.lp = lp;
+  // chunks of the one-launch sweeps: each hyperplane cut into lusgs_chunk_points(n_var)-point pieces
+  const int cp = lusgs_chunk_points(nv_of(c));
+  std::vector<int> chunk_h, h_chunks((size_t)H);
+  std::vector<int64_t> chunk_s0, h_end((size_t)H);
+  for (int h = 0; h < H; ++h) {
+    const int64_t b0 = c->lu_hb[h], b1 = c->lu_hb[h + 1];
+    h_end[h] = b1;
+    h_chunks[h] = (int)((b1 - b0 + cp - 1) / cp);
+    for (int64_t x = b0; x < b1; x += cp) chunk_h.push_back(h), chunk_s0.push_back(x);
+  }
+  const int nc = (int)chunk_h.size();
+  SweepWork &W = c->lu_w;
+  W.n_chunks = nc, W.H = H, W.status = c->d_status;
+  if (dev_alloc(c, &p, sizeof(int) * std::max(1, nc))) return CC_ERR_CUDA;
+  W.chunk_h = (const int *)p;
+  CK(cudaMemcpyAsync(p, chunk_h.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, c->stream));
+  if (dev_alloc(c, &p, sizeof(int64_t) * std::max(1, nc))) return CC_ERR_CUDA;
+  W.chunk_s0 = (const int64_t *)p;
+  CK(cudaMemcpyAsync(p, chunk_s0.data(), sizeof(int64_t) * nc, cudaMemcpyHostToDevice, c->stream));
+  if (dev_alloc(c, &p, sizeof(int) * std::max(1, H))) return CC_ERR_CUDA;
+  W.h_chunks = (const int *)p;
+  CK(cudaMemcpyAsync(p, h_chunks.data(), sizeof(int) * H, cudaMemcpyHostToDevice, c->stream));
+  if (dev_alloc(c, &p, sizeof(int64_t) * std::max(1, H))) return CC_ERR_CUDA;
+  W.h_end = (const int64_t *)p;
+  CK(cudaMemcpyAsync(p, h_end.data(), sizeof(int64_t) * H, cudaMemcpyHostToDevice, c->stream));
+  if (dev_alloc(c, &p, sizeof(unsigned) * (size_t)(2 + H))) return CC_ERR_CUDA;
+  W.counters = (unsigned *)p;
+  int dev = 0, n_sm = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  c->lu_ctas = n_sm;
+  const char *mode = std::getenv("CC_LUSGS_SWEEP");
+  c->lu_per_plane = mode && std::strcmp(mode, "planes") == 0;
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }

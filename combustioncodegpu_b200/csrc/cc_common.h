@@ -117,6 +117,7 @@ enum StatusBits : unsigned {
   kStatusNewtonCap = 1u,     // temperature Newton hit its iteration cap
   kStatusNonFinite = 2u,     // NaN/Inf or non-positive rho/p/T after an update
   kStatusBadDt = 4u,         // global time step not positive and finite
+  kStatusSweepTimeout = 32u, // an LU-SGS one-launch sweep's wait for a hyperplane gave up
 };
 
 // Arguments of one stage launch (see stage.cuh).
@@ -152,14 +153,49 @@ struct StageArgs {
   int n_regular;
 };
 
-// Work arrays of the LU-SGS steady step (lusgs.cuh).
+// Work arrays of the LU-SGS steady step (lusgs.cuh), in sweep order: the
+// interior points sorted by hyperplane h = i + j + k, then block, k and j,
+// so that the points of one hyperplane are contiguous and a warp's
+// neighbours in the adjacent hyperplane are too.  Per-variable arrays are
+// rows of lp doubles per point (lp = lusgs_lanes(n_var), lanes l < n_var
+// used), the sweeps' lane-per-variable layout; per-point scalars are plain
+// arrays.
 struct LusgsArgs {
-  double *R;     // [n_var][N]: dq, then dQ*, then dQ
-  double *rad;   // [3][N]: r_d = J (sigma_d + 2 sigv_d)
-  double *diag;  // [N]: J / dt_local + sum_d r_d
-  double *gam;   // [N]: gamma of the current state
-  double *psi;   // [n_spec][N]: dp / d(rho Y_k) at fixed rho e: gamma R_k T - (gamma - 1) h_k(T)
-  int h;         // hyperplane i + j + k of a sweep launch
+  int64_t S;         // interior points (sweep positions)
+  int lp;            // row length of the per-variable arrays
+  const int *pos;    // [N]: sweep position of an interior arena point (-1 elsewhere)
+  const int *lo;     // [3][S]: sweep position of p - e_d in the block, or -1
+  const int *hi;     // [3][S]: sweep position of p + e_d in the block, or -1
+  double *R;         // [S][lp]: dq, then dQ*, then dQ
+  double *Qs;        // [S][lp]: conserved state of the step
+  double *psi;       // [S][lp]: lanes l >= 5: dp / d(rho Y_{l-5}) at fixed rho e,
+                     //          gamma R_k T - (gamma - 1) h_k(T); lanes < 5: 0
+  double *Cn;        // [3][S][lp]: A+-_d(q) dQ(q) of the neighbour q in direction d, stored by q
+                     //             at this point's row (zero where the block has no such neighbour)
+  double *ps;        // [S]: pressure (absolute)
+  double *kv;        // [3][3][S]: k_d = J grad xi_d
+  double *rad;       // [3][S]: r_d = J (sigma_d + 2 sigv_d)
+  double *rdiag;     // [S]: 1 / D, D = J / dt_local + sum_d r_d
+  double *vel;       // [4][S]: 1 / rho, u, v, w of the conserved state (u = (rho u) (1 / rho))
+  double *gam;       // [S]: gamma
+  int64_t s0, s1;    // sweep positions of one launch (one hyperplane)
+};
+
+// Lanes per point of the LU-SGS sweeps (a power of two >= n_var) and the
+// points of one sweep chunk (a CTA of kSweepThreads threads).
+CCB_HD constexpr int lusgs_lanes(int nv) { return nv <= 8 ? 8 : (nv <= 16 ? 16 : 32); }
+constexpr int kSweepThreads = 512;
+CCB_HD constexpr int lusgs_chunk_points(int nv) { return kSweepThreads / lusgs_lanes(nv); }
+
+// Chunk tables and counters of a one-launch LU-SGS sweep (k_lusgs_sweep_all).
+struct SweepWork {
+  const int *chunk_h;       // [n_chunks]: hyperplane of chunk c (ascending)
+  const int64_t *chunk_s0;  // [n_chunks]: first sweep position of chunk c
+  const int *h_chunks;      // [H]: chunks per hyperplane
+  const int64_t *h_end;     // [H]: end position of hyperplane h
+  unsigned *counters;       // [2 + H]: ticket, abort, chunks done per hyperplane (zeroed before the sweep)
+  unsigned *status;
+  int n_chunks, H;
 };
 
 // A source reference of the halo program: kind 0 = point of the new state,

@@ -12,9 +12,9 @@
 //   r_d      = J (sigma_d + 2 sigv_d)
 //   D        = J / dt_local + sum_d r_d     (dt_local: TemporalScheme.cu:11-43)
 //   A+-_d dQ = (A_d dQ +- r_d dQ) / 2,      A_d = d(J grad xi_d . F)/dQ
-// the two sweeps are
-//   D dQ*(p) = dq(p) + sum_d A+_d(p - e_d) dQ*(p - e_d)        (lower, i+j+k ascending)
-//   dQ(p)    = dQ*(p) - D^-1 sum_d A-_d(p + e_d) dQ(p + e_d)   (upper, descending)
+// the two sweeps are (with the reciprocal 1/D formed once per point)
+//   dQ*(p) = (dq(p) + sum_d A+_d(p - e_d) dQ*(p - e_d)) (1/D)       (lower, i+j+k ascending)
+//   dQ(p)  = dQ*(p) - (sum_d A-_d(p + e_d) dQ(p + e_d)) (1/D)       (upper, descending)
 // over the interior points of each block (neighbours outside the block
 // contribute nothing: the block interfaces and boundaries stay explicit), and
 // Q += dQ.  A_d dQ is the Jacobian-vector product of the J-weighted flux of
@@ -27,21 +27,23 @@
 //
 // A point of sweep hyperplane h = i + j + k depends only on hyperplane h - 1
 // (h + 1 for the upper sweep), so each hyperplane is one launch over all
-// blocks, in order.  The arithmetic of each point is the oracle's
-// lexicographic sweep, term for term.
+// blocks, in order.  The sweeps read and write arrays in sweep order (points
+// sorted by hyperplane, block, k, j; LusgsArgs): the points of a hyperplane
+// are contiguous and the neighbours a warp reads in the adjacent hyperplane
+// are too.  The arithmetic of each point is the oracle's lexicographic sweep,
+// term for term.
 #pragma once
 #include "stage.cuh"
 
 namespace ccb {
 
 // dF = A_d(q) dQ for the J-weighted flux along k = J grad xi_d at q; Q is the
-// conserved state at q, p its pressure, psi its species pressure derivatives.
+// conserved state at q, inv = 1 / rho and u, v, w = Q[1..3] * inv, p its
+// pressure, psi its species pressure derivatives.
 template <int NV>
-__device__ __forceinline__ void lusgs_jac_vec(int nv, const double (&Q)[NV], double p, double gam,
-                                              const double (&psi)[NV], const double k[3], const double (&dQ)[NV],
-                                              double (&dF)[NV]) {
-  const double rho = Q[0], inv = 1.0 / rho;
-  const double u = Q[1] * inv, v = Q[2] * inv, w = Q[3] * inv;
+__device__ __forceinline__ void lusgs_jac_vec(int nv, const double (&Q)[NV], double inv, double u, double v, double w,
+                                              double p, double gam, const double (&psi)[NV], const double k[3],
+                                              const double (&dQ)[NV], double (&dF)[NV]) {
   const double U = k[0] * u + k[1] * v + k[2] * w;
   const double dm = k[0] * dQ[1] + k[1] * dQ[2] + k[2] * dQ[3];
   const double dU = (dm - U * dQ[0]) * inv;
@@ -59,8 +61,9 @@ __device__ __forceinline__ void lusgs_jac_vec(int nv, const double (&Q)[NV], dou
     if (l < nv) dF[l] = dQ[l] * U + Q[l] * dU;
 }
 
-// Right-hand side, spectral radii and diagonal of every interior point of
-// the tiles (the split variant's face arena holds the current fluxes).
+// Right-hand side, spectral radii, diagonal and the Jacobian inputs of every
+// interior point of the tiles (the split variant's face arena holds the
+// current fluxes), written in sweep order.
 template <typename T, int NS>
 __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, const LusgsArgs L,
                                                       const __grid_constant__ ChemParams C) {
@@ -73,6 +76,7 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, co
   const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
   if (i >= B.mx || j >= B.my) return;
   const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
+  const int64_t S = L.S;
   const bool three_d = B.mz > 1;
   const T *__restrict__ P = a.P;
   const T *__restrict__ G = a.G;
@@ -83,6 +87,7 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, co
   const int col = (int)B.base + i + sj * j;
   for (int k = t.k0; k < t.k1; ++k) {
     const int p = col + sk * k;
+    const int64_t sp = L.pos[p];
 #pragma unroll
     for (int l = 0; l < NV; ++l) {
       if (l < nv) {
@@ -92,9 +97,18 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, co
         if (three_d) acc += Fz[o] - Fz[o - sk];
         double dq = -(double)acc;
         if (a.gcl && l >= 1 && l <= 3) dq -= C.p_ref * a.gcl[(l - 1) * N + p];
-        L.R[o] = dq;
+        L.R[sp * L.lp + l] = dq;
+        L.Qs[sp * L.lp + l] = a.Qin[o];
       }
     }
+    {
+      const double inv = 1.0 / a.Qin[p];
+      L.vel[sp] = inv;
+      L.vel[S + sp] = a.Qin[N + p] * inv;
+      L.vel[2 * S + sp] = a.Qin[2 * N + p] * inv;
+      L.vel[3 * S + sp] = a.Qin[3 * N + p] * inv;
+    }
+    L.ps[sp] = (double)P[4 * N + p] + C.p_ref;
     T Y[A];
 #pragma unroll
     for (int l = 0; l < A; ++l)
@@ -111,9 +125,9 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, co
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       double r = 0;
+      const double m0 = (double)G[(1 + 3 * d) * N + p], m1 = (double)G[(2 + 3 * d) * N + p],
+                   m2 = (double)G[(3 + 3 * d) * N + p];
       if (d < 2 || three_d) {
-        const double m0 = (double)G[(1 + 3 * d) * N + p], m1 = (double)G[(2 + 3 * d) * N + p],
-                     m2 = (double)G[(3 + 3 * d) * N + p];
         const double g = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
         const double U = u * m0 + v * m1 + w * m2;
         r = fabs(U) + (double)c * g;
@@ -121,74 +135,190 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, co
         r *= J;
         D += r;
       }
-      L.rad[d * N + p] = r;
+      L.rad[d * S + sp] = r;
+      L.kv[(3 * d) * S + sp] = J * m0;
+      L.kv[(3 * d + 1) * S + sp] = J * m1;
+      L.kv[(3 * d + 2) * S + sp] = J * m2;
     }
-    L.diag[p] = D;
-    L.gam[p] = (double)gam;
+    L.rdiag[sp] = 1.0 / D;
+    L.gam[sp] = (double)gam;
+    const int id[3] = {i, j, k};
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (id[d] == 0)  // no lower neighbour: nothing arrives in this slot during the lower sweep
+#pragma unroll
+        for (int l = 0; l < NV; ++l)
+          if (l < nv) L.Cn[(d * S + sp) * L.lp + l] = 0.0;
     if (ns > 0) {
       const double td = (double)P[5 * N + p], g1 = (double)gam - 1.0;
 #pragma unroll
       for (int l = 0; l < A; ++l)
         if (l < ns)
-          L.psi[l * N + p] = (double)gam * C.d.cv_shift[l] * td - g1 * nasa_h<double>(C.d, param_rec<double>(C), l, td);
+          L.psi[sp * L.lp + 5 + l] =
+              (double)gam * C.d.cv_shift[l] * td - g1 * nasa_h<double>(C.d, param_rec<double>(C), l, td);
     }
   }
 }
 
-// One hyperplane i + j + k = L.h of the lower (DIR = +1) or upper (DIR = -1)
-// sweep; blockIdx.y is the block, threads run over its (j, k) columns.
-template <typename T, int NS, int DIR>
-__global__ void __launch_bounds__(256) k_lusgs_sweep(const StageArgs<T> a, const LusgsArgs L,
-                                                     const __grid_constant__ ChemParams C) {
-  constexpr int A = SpecCount<NS>::kArr;
-  constexpr int NV = 5 + A;
-  const int ns = SpecCount<NS>::n(C);
-  const int nv = 5 + ns;
-  const BlockInfo B = a.blocks[blockIdx.y];
-  const int cidx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cidx >= B.my * B.mz) return;
-  const int j = cidx % B.my, k = cidx / B.my;
-  const int i = L.h - j - k;
-  if (i < 0 || i >= B.mx) return;
-  const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
-  const bool three_d = B.mz > 1;
-  const int p = (int)B.base + i + sj * j + sk * k;
-  const T *__restrict__ G = a.G;
-  double acc[NV];
+constexpr long kSweepPolls = 1L << 22;  // polls of a hyperplane counter before giving up (~0.5 s)
+
+// One point of the lower (DIR = +1) or upper (DIR = -1) sweep, held by a
+// group of LP = lusgs_lanes(n_var) lanes of a warp, lane l owning variable l.
+// load() reads the point's own data (none of it depends on the sweep's
+// progress, so a one-launch sweep issues it before waiting for the preceding
+// hyperplane); solve() finishes the point.  The neighbour terms
+// A+-_d(q) dQ(q) arrive in this point's rows of L.Cn, stored there by the
+// neighbour q when it was solved, so the only loads after the wait are these
+// rows.  After solving, the group forms its own terms for the neighbours of
+// the next hyperplane: the couplings of the Jacobian (rho, momentum, energy,
+// and the species pressure terms in ascending order) come from the other
+// lanes by shuffles, and every lane evaluates the oracle's expressions in
+// its order.  In the lower sweep a point also clears the rows that no
+// neighbour fills in the upper sweep.  Every lane of the warp runs the
+// shuffles; lanes without a point or a variable only mask their memory
+// accesses.  Offsets are 32-bit (3 lp S < 2^31 is checked at allocation).
+template <int NS, int DIR>
+struct LusgsLane {
+  static constexpr int A = SpecCount<NS>::kArr;
+  static constexpr int NV = 5 + A;
+  static constexpr int LP = lusgs_lanes(NV);
+  int s, S, l, nb[3];
+  bool act, var;  // the group has a point; this lane has a variable
+  double R, Q, psi, kv[9], rad[3], rD, ps, gam, inv, u, v, w;
+
+  __device__ __forceinline__ void load(const LusgsArgs &L, int nv, int s_, int l_, bool act_) {
+    s = s_, S = (int)L.S, l = l_, act = act_, var = act_ && l_ < nv;
+    const int *__restrict__ next = DIR > 0 ? L.hi : L.lo;  // neighbours of the next hyperplane
+    R = Q = psi = 0.0;
+    if (var) R = L.R[s * LP + l], Q = L.Qs[s * LP + l], psi = L.psi[s * LP + l];
 #pragma unroll
-  for (int l = 0; l < NV; ++l)
-    if (l < nv) acc[l] = DIR > 0 ? L.R[l * N + p] : 0.0;
+    for (int d = 0; d < 3; ++d) nb[d] = act ? next[d * S + s] : -1;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    if (d == 2 && !three_d) break;
-    const int id = d == 0 ? i : (d == 1 ? j : k);
-    const int md = d == 0 ? B.mx : (d == 1 ? B.my : B.mz);
-    const int sd = d == 0 ? 1 : (d == 1 ? sj : sk);
-    if (DIR > 0 ? id < 1 : id + 1 >= md) continue;
-    const int q = DIR > 0 ? p - sd : p + sd;
-    double X[NV], Qq[NV], dF[NV], psi[NV];
+    for (int e = 0; e < 9; ++e) kv[e] = act ? L.kv[e * S + s] : 0.0;
 #pragma unroll
-    for (int l = 0; l < NV; ++l)
-      if (l < nv) X[l] = L.R[l * N + q], Qq[l] = a.Qin[l * N + q], psi[l] = l >= 5 ? L.psi[(l - 5) * N + q] : 0.0;
-    const double Jq = (double)G[q];
-    const double kv[3] = {Jq * (double)G[(1 + 3 * d) * N + q], Jq * (double)G[(2 + 3 * d) * N + q],
-                          Jq * (double)G[(3 + 3 * d) * N + q]};
-    const double pq = (double)a.P[4 * N + q] + C.p_ref;
-    lusgs_jac_vec<NV>(nv, Qq, pq, L.gam[q], psi, kv, X, dF);
-    const double r = DIR * L.rad[d * N + q];
-#pragma unroll
-    for (int l = 0; l < NV; ++l)
-      if (l < nv) acc[l] += 0.5 * (dF[l] + r * X[l]);
+    for (int d = 0; d < 3; ++d) rad[d] = act ? L.rad[d * S + s] : 0.0;
+    rD = act ? L.rdiag[s] : 0.0, ps = act ? L.ps[s] : 0.0, gam = act ? L.gam[s] : 1.0;
+    inv = act ? L.vel[s] : 0.0, u = act ? L.vel[S + s] : 0.0, v = act ? L.vel[2 * S + s] : 0.0;
+    w = act ? L.vel[3 * S + s] : 0.0;
   }
-  const double D = L.diag[p];
+
+  // CG: read the rows through L2 (written by other CTAs of the same launch)
+  template <bool CG>
+  __device__ __forceinline__ void solve(const LusgsArgs &L, int nv) {
+    double *__restrict__ Cn = L.Cn;
+    double acc = DIR > 0 ? R : 0.0;
 #pragma unroll
-  for (int l = 0; l < NV; ++l) {
-    if (l < nv) {
-      if (DIR > 0)
-        L.R[l * N + p] = acc[l] / D;
-      else
-        L.R[l * N + p] = L.R[l * N + p] - acc[l] / D;
+    for (int d = 0; d < 3; ++d) {
+      const double *c = Cn + ((int64_t)d * S + s) * LP + l;
+      if (var) acc += CG ? __ldcg(c) : *c;
     }
+    const double X = DIR > 0 ? acc * rD : R - acc * rD;
+    if (var) L.R[s * LP + l] = X;
+    if (DIR > 0 && var) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (nb[d] < 0) Cn[((int64_t)d * S + s) * LP + l] = 0.0;
+    }
+    // couplings from the other lanes of the group
+    const unsigned full = 0xffffffffu;
+    const double x0 = __shfl_sync(full, X, 0, LP), x1 = __shfl_sync(full, X, 1, LP);
+    const double x2 = __shfl_sync(full, X, 2, LP), x3 = __shfl_sync(full, X, 3, LP);
+    const double x4 = __shfl_sync(full, X, 4, LP);
+    const double pX = psi * X;
+    double dp = (gam - 1.0) * (x4 - (u * x1 + v * x2 + w * x3) + 0.5 * (u * u + v * v + w * w) * x0);
+#pragma unroll
+    for (int m = 5; m < NV; ++m) {
+      const double t = __shfl_sync(full, pX, m, LP);
+      if (m < nv) dp += t;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (nb[d] < 0 || !var) continue;
+      const double k0 = kv[3 * d], k1 = kv[3 * d + 1], k2 = kv[3 * d + 2];
+      const double U = k0 * u + k1 * v + k2 * w;
+      const double dm = k0 * x1 + k1 * x2 + k2 * x3;
+      const double dU = (dm - U * x0) * inv;
+      double dF;
+      if (l == 0)
+        dF = dm;
+      else if (l <= 3)
+        dF = X * U + Q * dU + (l == 1 ? k0 : (l == 2 ? k1 : k2)) * dp;
+      else if (l == 4)
+        dF = (X + dp) * U + (Q + ps) * dU;
+      else
+        dF = X * U + Q * dU;
+      const double r = DIR * rad[d];
+      Cn[((int64_t)d * S + nb[d]) * LP + l] = 0.5 * (dF + r * X);
+    }
+  }
+};
+
+// One hyperplane (sweep positions [L.s0, L.s1)) per launch.
+template <int NS, int DIR>
+__global__ void __launch_bounds__(kSweepThreads) k_lusgs_sweep(const LusgsArgs L,
+                                                               const __grid_constant__ ChemParams C) {
+  using Lane = LusgsLane<NS, DIR>;
+  const int nv = 5 + SpecCount<NS>::n(C);
+  const int64_t s = L.s0 + (int64_t)blockIdx.x * (kSweepThreads / Lane::LP) + threadIdx.x / Lane::LP;
+  Lane pt;
+  pt.load(L, nv, (int)s, threadIdx.x % Lane::LP, s < L.s1);
+  pt.template solve<false>(L, nv);
+}
+
+// A whole sweep in one launch.  The hyperplanes are cut into chunks of
+// lusgs_chunk_points(n_var) points; CTAs take chunk tickets in sweep order
+// (ascending hyperplanes for the lower sweep, descending for the upper) from
+// W.counters[0], load their points' own data, wait until every chunk of the
+// preceding hyperplane has been counted in W.counters[2 + h], solve and count
+// their chunk.  A ticket is only taken by a running CTA, and every chunk a
+// CTA waits for has a lower ticket, so the waits end without any assumption
+// on how many CTAs are resident.  A wait that exceeds kSweepPolls polls sets
+// kStatusSweepTimeout and W.counters[1]; every CTA then leaves (the step's
+// result is invalid and the status word says so).
+template <int NS, int DIR>
+__global__ void __launch_bounds__(kSweepThreads) k_lusgs_sweep_all(const LusgsArgs L, const SweepWork W,
+                                                                   const __grid_constant__ ChemParams C) {
+  using Lane = LusgsLane<NS, DIR>;
+  __shared__ int sh_c, sh_abort;
+  volatile unsigned *vabort = W.counters + 1;
+  const int nv = 5 + SpecCount<NS>::n(C);
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int t = (int)atomicAdd(W.counters, 1u);
+      sh_c = t < W.n_chunks ? (DIR > 0 ? t : W.n_chunks - 1 - t) : -1;
+    }
+    __syncthreads();
+    const int c = sh_c;
+    if (c < 0) return;
+    const int h = W.chunk_h[c];
+    const int64_t s = W.chunk_s0[c] + threadIdx.x / Lane::LP;
+    Lane pt;
+    pt.load(L, nv, (int)s, threadIdx.x % Lane::LP, s < W.h_end[h]);  // in flight while thread 0 waits
+    if (threadIdx.x == 0) {
+      int abort = *vabort != 0;
+      const int hw = h - DIR;  // hyperplane this chunk depends on
+      if (!abort && hw >= 0 && hw < W.H) {
+        const unsigned need = (unsigned)W.h_chunks[hw];
+        volatile unsigned *done = W.counters + 2 + hw;
+        long polls = 0;
+        while (*done < need) {
+          if (*vabort || ++polls > kSweepPolls) {
+            if (polls > kSweepPolls) atomicOr(W.status, kStatusSweepTimeout), atomicExch(W.counters + 1, 1u);
+            abort = 1;
+            break;
+          }
+          __nanosleep(32);
+        }
+        __threadfence();  // acquire: the counted chunks' stores are visible from here
+      }
+      sh_abort = abort;
+    }
+    __syncthreads();
+    if (sh_abort) return;
+    pt.template solve<true>(L, nv);
+    __threadfence();  // release this thread's stores before the chunk is counted
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(W.counters + 2 + h, 1u);
   }
 }
 
@@ -222,10 +352,11 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_update(const StageArgs<T> a,
     const int col = (int)B.base + i + sj * j;
     for (int k = t.k0; k < t.k1; ++k) {
       const int p = col + sk * k;
+      const int64_t sp = L.pos[p];
       double dq[NV];
 #pragma unroll
       for (int l = 0; l < NV; ++l)
-        if (l < nv) dq[l] = L.R[l * N + p];
+        if (l < nv) dq[l] = L.R[sp * L.lp + l];
       point_update<T, NS>(C, sRec, sRecD, a, p, N, dq, (double)a.G[p], (double)a.P[5 * N + p], three_d, flags,
                           dt_min);
     }

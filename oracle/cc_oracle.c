@@ -37,7 +37,7 @@ typedef struct {
   double *cv, *bv, *yk;                 /* [nv][ng], [6][ng], [ns][ng] */
   double *vel, *acoustic, *mul, *cond, *gamma, *rho_d, *mach;
   double *dq, *dt_local, *bv_last, *qn; /* interior: [nv][n], [n], [4][n], [nv][n] */
-  double *lu_rad, *lu_diag, *lu_psi;    /* LU-SGS, interior: [3][n], [n], [ns][n] (allocated on first use) */
+  double *lu_rad, *lu_diag, *lu_psi;    /* LU-SGS, interior: r_d [3][n], 1/D [n], psi [ns][n] (on first use) */
   oc_boundary *bnd;
   int n_bnd, cap_bnd;
   oc_inner_face *inf;
@@ -1210,12 +1210,12 @@ int oc_steady_step(oc_solver *s, int renorm_y) {
  *         of the thermally perfect mixture:
  *         dp = (gamma-1)(dE - u.dm + |u|^2/2 drho) + sum_k psi_k d(rho Y_k),
  *         psi_k = gamma R_k T - (gamma-1) h_k(T) (no sum for the air model);
- * lower sweep (lexicographic)  D dQ*(p) = dq(p) + sum_d A+_d(p-e_d) dQ*(p-e_d),
- * upper sweep (reversed)       dQ(p) = dQ*(p) - D^-1 sum_d A-_d(p+e_d) dQ(p+e_d),
+ * lower sweep (lexicographic)  dQ*(p) = (dq(p) + sum_d A+_d(p-e_d) dQ*(p-e_d)) (1/D),
+ * upper sweep (reversed)       dQ(p) = dQ*(p) - (sum_d A-_d(p+e_d) dQ(p+e_d)) (1/D),
  * neighbours outside the block contribute nothing; then cv += dQ. */
 static void lusgs_jac_vec(int nv, const double *Q, double p, double gam, const double *psi, const double k[3],
                           const double *dQ, double *dF) {
-  const double rho = Q[0], inv = 1.0 / rho;
+  const double inv = 1.0 / Q[0];
   const double u = Q[1] * inv, v = Q[2] * inv, w = Q[3] * inv;
   const double U = k[0] * u + k[1] * v + k[2] * w;
   const double dm = k[0] * dQ[1] + k[1] * dQ[2] + k[2] * dQ[3];
@@ -1278,7 +1278,7 @@ static void lusgs_block(const oc_solver *s, oblk *B) {
           }
           B->lu_rad[(size_t)d * n + qi] = r;
         }
-        B->lu_diag[qi] = D;
+        B->lu_diag[qi] = 1.0 / D;
         if (s->ns > 0) {
           double h[MAXS];
           const double t = B->bv[5 * ng + q];
@@ -1296,8 +1296,8 @@ static void lusgs_block(const oc_solver *s, oblk *B) {
         if (i > 0) lusgs_neighbour(s, B, i - 1, j, k, 0, 1.0, acc);
         if (j > 0) lusgs_neighbour(s, B, i, j - 1, k, 1, 1.0, acc);
         if (dim == 3 && k > 0) lusgs_neighbour(s, B, i, j, k - 1, 2, 1.0, acc);
-        const double D = B->lu_diag[qi];
-        for (int l = 0; l < nv; ++l) B->dq[(size_t)l * n + qi] = acc[l] / D;
+        const double rD = B->lu_diag[qi];
+        for (int l = 0; l < nv; ++l) B->dq[(size_t)l * n + qi] = acc[l] * rD;
       }
   for (int k = B->mz - 1; k >= 0; --k)
     for (int j = B->my - 1; j >= 0; --j)
@@ -1307,8 +1307,8 @@ static void lusgs_block(const oc_solver *s, oblk *B) {
         if (i + 1 < B->mx) lusgs_neighbour(s, B, i + 1, j, k, 0, -1.0, acc);
         if (j + 1 < B->my) lusgs_neighbour(s, B, i, j + 1, k, 1, -1.0, acc);
         if (dim == 3 && k + 1 < B->mz) lusgs_neighbour(s, B, i, j, k + 1, 2, -1.0, acc);
-        const double D = B->lu_diag[qi];
-        for (int l = 0; l < nv; ++l) B->dq[(size_t)l * n + qi] = B->dq[(size_t)l * n + qi] - acc[l] / D;
+        const double rD = B->lu_diag[qi];
+        for (int l = 0; l < nv; ++l) B->dq[(size_t)l * n + qi] = B->dq[(size_t)l * n + qi] - acc[l] * rD;
       }
 }
 

@@ -351,6 +351,30 @@ def test_lusgs_mixed_close_to_oracle(name):
     assert not bad, errs
 
 
+def test_lusgs_multiblock64_small_matches_oracle():
+    errs, status = compare(_with_cfl(MB64_SMALL, 5.0), "lusgs", 3, "fp64")
+    assert status == 0
+    bad = {k: v for k, v in errs.items() if not v < 1e-10}
+    assert not bad, errs
+
+
+def test_lusgs_one_launch_sweeps_equal_per_plane_launches(monkeypatch):
+    """The one-launch sweeps (chunk tickets, counted hyperplanes) give the
+    state of one launch per hyperplane bit for bit, on uneven blocks."""
+    case = _with_cfl(MB64_SMALL, 5.0)
+    out = []
+    for mode in ("planes", "one"):
+        monkeypatch.setenv("CC_LUSGS_SWEEP", mode)
+        d = cc.Driver.from_case(case, "fp64")
+        d.initialize_computation()
+        d.simulate(3, "lusgs")
+        assert d.status() == 0
+        out.append([d.field[b].get_state()[2] for b in range(len(case["blocks"]))])
+        d.close()
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_lusgs_graph_replay_equals_launches():
     case = _with_cfl(CASES["multiblock"], 5.0)
     out = []
