@@ -118,9 +118,6 @@ struct cc_ctx {
   CUtensorMap *d_tmaps = nullptr; // [2][n_blocks]: primitive arenas P[0], P[1] per block
   LusgsArgs lu{};                 // LU-SGS work arrays (allocated by the first LU-SGS step)
   std::vector<int64_t> lu_hb;     // sweep positions where each hyperplane begins, + end
-  SweepWork lu_w{};               // chunk tables and counters of the one-launch sweeps
-  bool lu_per_plane = false;      // CC_LUSGS_SWEEP=planes: one launch per hyperplane instead
-  int lu_ctas = 0;                // SMs a one-launch sweep fills with resident CTAs
   int n_partials = 296;
 
   cudaStream_t stream = nullptr;
@@ -726,19 +723,14 @@ int lusgs_and_halo(cc_ctx *c, StageArgs<T> a, int pn, int pc) {
   if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
   LusgsArgs L = c->lu;
   CK((Launch<T, NS>::lusgs_rhs(a, L, c->chem, nt, c->stream)));
-  if (c->lu_per_plane) {
-    const int H = (int)c->lu_hb.size() - 1;
-    for (int h = 0; h < H; ++h) {
-      L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1];
-      CK((Launch<T, NS>::lusgs_sweep(L, c->chem, 1, c->stream)));
-    }
-    for (int h = H - 1; h >= 0; --h) {
-      L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1];
-      CK((Launch<T, NS>::lusgs_sweep(L, c->chem, -1, c->stream)));
-    }
-  } else {
-    CK((Launch<T, NS>::lusgs_sweep_all(L, &c->lu_w, c->chem, 1, c->lu_ctas, c->stream)));
-    CK((Launch<T, NS>::lusgs_sweep_all(L, &c->lu_w, c->chem, -1, c->lu_ctas, c->stream)));
+  const int H = (int)c->lu_hb.size() - 1;
+  for (int h = 0; h < H; ++h) {
+    L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1];
+    CK((Launch<T, NS>::lusgs_sweep(L, c->chem, 1, c->stream)));
+  }
+  for (int h = H - 1; h >= 0; --h) {
+    L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1];
+    CK((Launch<T, NS>::lusgs_sweep(L, c->chem, -1, c->stream)));
   }
   a.gcl = nullptr;  // the geometric term is part of the right-hand side
   CK((Launch<T, NS>::lusgs_update(a, L, c->chem, nt, c->stream)));
@@ -752,7 +744,7 @@ int lusgs_alloc(cc_ctx *c) {
   if (c->lu.R) return 0;
   const int64_t N = c->N, S = c->n_int;
   const int lp = lusgs_lanes(nv_of(c));
-  if (3 * lp * S >= (int64_t)1 << 31 || N >= (int64_t)1 << 31)
+  if (std::max(3 * lp, (int)kLuScalars) * S >= (int64_t)1 << 31 || N >= (int64_t)1 << 31)
     return fail(CC_ERR_ARG, "LU-SGS: too many points for 32-bit sweep offsets");
   std::vector<int> pos((size_t)N, -1), lo((size_t)(3 * S), -1), hi((size_t)(3 * S), -1);
   std::vector<int64_t> pt((size_t)S);
@@ -799,8 +791,7 @@ int lusgs_alloc(cc_ctx *c) {
     *dst = (double *)p;
     return 0;
   };
-  if (dbl(&c->lu.R, lp * S) || dbl(&c->lu.Qs, lp * S) || dbl(&c->lu.ps, S) || dbl(&c->lu.kv, 9 * S) ||
-      dbl(&c->lu.rad, 3 * S) || dbl(&c->lu.rdiag, S) || dbl(&c->lu.vel, 4 * S) || dbl(&c->lu.gam, S) ||
+  if (dbl(&c->lu.R, lp * S) || dbl(&c->lu.Qs, lp * S) || dbl(&c->lu.pt, kLuScalars * S) ||
       dbl(&c->lu.psi, lp * S) || dbl(&c->lu.Cn, 3 * lp * S))
     return CC_ERR_CUDA;
   int *ip[3];
@@ -813,38 +804,6 @@ int lusgs_alloc(cc_ctx *c) {
   }
   c->lu.pos = ip[0], c->lu.lo = ip[1], c->lu.hi = ip[2];
   c->lu.S = S, c->lu.lp = lp;
-  // chunks of the one-launch sweeps: each hyperplane cut into lusgs_chunk_points(n_var)-point pieces
-  const int cp = lusgs_chunk_points(nv_of(c));
-  std::vector<int> chunk_h, h_chunks((size_t)H);
-  std::vector<int64_t> chunk_s0, h_end((size_t)H);
-  for (int h = 0; h < H; ++h) {
-    const int64_t b0 = c->lu_hb[h], b1 = c->lu_hb[h + 1];
-    h_end[h] = b1;
-    h_chunks[h] = (int)((b1 - b0 + cp - 1) / cp);
-    for (int64_t x = b0; x < b1; x += cp) chunk_h.push_back(h), chunk_s0.push_back(x);
-  }
-  const int nc = (int)chunk_h.size();
-  SweepWork &W = c->lu_w;
-  W.n_chunks = nc, W.H = H, W.status = c->d_status;
-  if (dev_alloc(c, &p, sizeof(int) * std::max(1, nc))) return CC_ERR_CUDA;
-  W.chunk_h = (const int *)p;
-  CK(cudaMemcpyAsync(p, chunk_h.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, c->stream));
-  if (dev_alloc(c, &p, sizeof(int64_t) * std::max(1, nc))) return CC_ERR_CUDA;
-  W.chunk_s0 = (const int64_t *)p;
-  CK(cudaMemcpyAsync(p, chunk_s0.data(), sizeof(int64_t) * nc, cudaMemcpyHostToDevice, c->stream));
-  if (dev_alloc(c, &p, sizeof(int) * std::max(1, H))) return CC_ERR_CUDA;
-  W.h_chunks = (const int *)p;
-  CK(cudaMemcpyAsync(p, h_chunks.data(), sizeof(int) * H, cudaMemcpyHostToDevice, c->stream));
-  if (dev_alloc(c, &p, sizeof(int64_t) * std::max(1, H))) return CC_ERR_CUDA;
-  W.h_end = (const int64_t *)p;
-  CK(cudaMemcpyAsync(p, h_end.data(), sizeof(int64_t) * H, cudaMemcpyHostToDevice, c->stream));
-  if (dev_alloc(c, &p, sizeof(unsigned) * (size_t)(2 + H))) return CC_ERR_CUDA;
-  W.counters = (unsigned *)p;
-  int dev = 0, n_sm = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  c->lu_ctas = n_sm;
-  const char *mode = std::getenv("CC_LUSGS_SWEEP");
-  c->lu_per_plane = mode && std::strcmp(mode, "planes") == 0;
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }

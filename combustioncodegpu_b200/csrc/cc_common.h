@@ -117,7 +117,6 @@ enum StatusBits : unsigned {
   kStatusNewtonCap = 1u,     // temperature Newton hit its iteration cap
   kStatusNonFinite = 2u,     // NaN/Inf or non-positive rho/p/T after an update
   kStatusBadDt = 4u,         // global time step not positive and finite
-  kStatusSweepTimeout = 32u, // an LU-SGS one-launch sweep's wait for a hyperplane gave up
 };
 
 // Arguments of one stage launch (see stage.cuh).
@@ -172,31 +171,20 @@ struct LusgsArgs {
                      //          gamma R_k T - (gamma - 1) h_k(T); lanes < 5: 0
   double *Cn;        // [3][S][lp]: A+-_d(q) dQ(q) of the neighbour q in direction d, stored by q
                      //             at this point's row (zero where the block has no such neighbour)
-  double *ps;        // [S]: pressure (absolute)
-  double *kv;        // [3][3][S]: k_d = J grad xi_d
-  double *rad;       // [3][S]: r_d = J (sigma_d + 2 sigv_d)
-  double *rdiag;     // [S]: 1 / D, D = J / dt_local + sum_d r_d
-  double *vel;       // [4][S]: 1 / rho, u, v, w of the conserved state (u = (rho u) (1 / rho))
-  double *gam;       // [S]: gamma
+  double *pt;        // [S][kLuScalars]: the point's scalars, at the kLu* offsets
   int64_t s0, s1;    // sweep positions of one launch (one hyperplane)
 };
 
+// Offsets in a point's scalar row (LusgsArgs::pt): 1 / D (D = J / dt_local +
+// sum_d r_d), the absolute pressure, gamma, 1 / rho and u, v, w of the
+// conserved state (u = (rho u) (1 / rho)), k_d = J grad xi_d (3 x 3) and
+// r_d = J (sigma_d + 2 sigv_d) (3); rows are two 128-byte lines.
+enum LuScalar : int { kLuRD = 0, kLuP = 1, kLuGam = 2, kLuInv = 3, kLuU = 4, kLuK = 7, kLuRad = 16, kLuScalars = 32 };
+
 // Lanes per point of the LU-SGS sweeps (a power of two >= n_var) and the
-// points of one sweep chunk (a CTA of kSweepThreads threads).
+// points of one sweep CTA (kSweepThreads threads).
 CCB_HD constexpr int lusgs_lanes(int nv) { return nv <= 8 ? 8 : (nv <= 16 ? 16 : 32); }
 constexpr int kSweepThreads = 512;
-CCB_HD constexpr int lusgs_chunk_points(int nv) { return kSweepThreads / lusgs_lanes(nv); }
-
-// Chunk tables and counters of a one-launch LU-SGS sweep (k_lusgs_sweep_all).
-struct SweepWork {
-  const int *chunk_h;       // [n_chunks]: hyperplane of chunk c (ascending)
-  const int64_t *chunk_s0;  // [n_chunks]: first sweep position of chunk c
-  const int *h_chunks;      // [H]: chunks per hyperplane
-  const int64_t *h_end;     // [H]: end position of hyperplane h
-  unsigned *counters;       // [2 + H]: ticket, abort, chunks done per hyperplane (zeroed before the sweep)
-  unsigned *status;
-  int n_chunks, H;
-};
 
 // A source reference of the halo program: kind 0 = point of the new state,
 // 1 = point of the previous state, 2 = scratch slot of an evaluated node.

@@ -139,30 +139,6 @@ cudaError_t Launch<T, NS>::lusgs_sweep(const LusgsArgs &L, const ChemParams &C, 
 }
 
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::lusgs_sweep_all(const LusgsArgs &L, const void *Wv, const ChemParams &C, int dir,
-                                           int n_sms, cudaStream_t s) {
-  const SweepWork &W = *static_cast<const SweepWork *>(Wv);
-  if (W.n_chunks <= 0) return cudaSuccess;
-  if (L.lp != LusgsLane<NS, 1>::LP) return cudaErrorInvalidValue;  // chunk tables built for another lane count
-  cudaError_t e = cudaMemsetAsync(W.counters, 0, sizeof(unsigned) * (size_t)(2 + W.H), s);
-  if (e != cudaSuccess) return e;
-  // resident CTAs only (more would start when the resident ones leave)
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    int a1 = 1, a2 = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a1, k_lusgs_sweep_all<NS, 1>, kSweepThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a2, k_lusgs_sweep_all<NS, -1>, kSweepThreads, 0);
-    per_sm = std::max(1, std::min(a1, a2));
-  }
-  const unsigned grid = (unsigned)std::max(1, std::min(n_sms * per_sm, W.n_chunks));
-  if (dir > 0)
-    k_lusgs_sweep_all<NS, 1><<<grid, kSweepThreads, 0, s>>>(L, W, C);
-  else
-    k_lusgs_sweep_all<NS, -1><<<grid, kSweepThreads, 0, s>>>(L, W, C);
-  return cudaGetLastError();
-}
-
-template <typename T, int NS>
 cudaError_t Launch<T, NS>::lusgs_update(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int n_tiles,
                                         cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;

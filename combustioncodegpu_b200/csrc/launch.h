@@ -37,10 +37,6 @@ struct Launch {
   static cudaError_t lusgs_rhs(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int n_tiles,
                                cudaStream_t s);
   static cudaError_t lusgs_sweep(const LusgsArgs &L, const ChemParams &C, int dir, cudaStream_t s);
-  // a whole sweep in one launch (W is a SweepWork; its counters are zeroed here) on n_sms x the
-  // resident CTAs per SM
-  static cudaError_t lusgs_sweep_all(const LusgsArgs &L, const void *W, const ChemParams &C, int dir, int n_sms,
-                                     cudaStream_t s);
   static cudaError_t lusgs_update(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int n_tiles,
                                   cudaStream_t s);
   static cudaError_t halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);

@@ -65,7 +65,7 @@ __device__ __forceinline__ void lusgs_jac_vec(int nv, const double (&Q)[NV], dou
 // interior point of the tiles (the split variant's face arena holds the
 // current fluxes), written in sweep order.
 template <typename T, int NS>
-__global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, const LusgsArgs L,
+__global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2) k_lusgs_rhs(const StageArgs<T> a, const LusgsArgs L,
                                                       const __grid_constant__ ChemParams C) {
   constexpr int A = SpecCount<NS>::kArr;
   constexpr int NV = 5 + A;
@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, co
   for (int k = t.k0; k < t.k1; ++k) {
     const int p = col + sk * k;
     const int64_t sp = L.pos[p];
+    double *row = L.pt + sp * kLuScalars;
 #pragma unroll
     for (int l = 0; l < NV; ++l) {
       if (l < nv) {
@@ -103,12 +104,12 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, co
     }
     {
       const double inv = 1.0 / a.Qin[p];
-      L.vel[sp] = inv;
-      L.vel[S + sp] = a.Qin[N + p] * inv;
-      L.vel[2 * S + sp] = a.Qin[2 * N + p] * inv;
-      L.vel[3 * S + sp] = a.Qin[3 * N + p] * inv;
+      row[kLuInv] = inv;
+      row[kLuU] = a.Qin[N + p] * inv;
+      row[kLuU + 1] = a.Qin[2 * N + p] * inv;
+      row[kLuU + 2] = a.Qin[3 * N + p] * inv;
     }
-    L.ps[sp] = (double)P[4 * N + p] + C.p_ref;
+    row[kLuP] = (double)P[4 * N + p] + C.p_ref;
     T Y[A];
 #pragma unroll
     for (int l = 0; l < A; ++l)
@@ -135,13 +136,13 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, co
         r *= J;
         D += r;
       }
-      L.rad[d * S + sp] = r;
-      L.kv[(3 * d) * S + sp] = J * m0;
-      L.kv[(3 * d + 1) * S + sp] = J * m1;
-      L.kv[(3 * d + 2) * S + sp] = J * m2;
+      row[kLuRad + d] = r;
+      row[kLuK + 3 * d] = J * m0;
+      row[kLuK + 3 * d + 1] = J * m1;
+      row[kLuK + 3 * d + 2] = J * m2;
     }
-    L.rdiag[sp] = 1.0 / D;
-    L.gam[sp] = (double)gam;
+    row[kLuRD] = 1.0 / D;
+    row[kLuGam] = (double)gam;
     const int id[3] = {i, j, k};
 #pragma unroll
     for (int d = 0; d < 3; ++d)
@@ -160,12 +161,9 @@ __global__ void __launch_bounds__(kTX *kTY) k_lusgs_rhs(const StageArgs<T> a, co
   }
 }
 
-constexpr long kSweepPolls = 1L << 22;  // polls of a hyperplane counter before giving up (~0.5 s)
-
 // One point of the lower (DIR = +1) or upper (DIR = -1) sweep, held by a
 // group of LP = lusgs_lanes(n_var) lanes of a warp, lane l owning variable l.
-// load() reads the point's own data (none of it depends on the sweep's
-// progress, so a one-launch sweep issues it before waiting for the preceding
+// load() reads the point's own data (none of it depends on the preceding
 // hyperplane); solve() finishes the point.  The neighbour terms
 // A+-_d(q) dQ(q) arrive in this point's rows of L.Cn, stored there by the
 // neighbour q when it was solved, so the only loads after the wait are these
@@ -193,24 +191,23 @@ struct LusgsLane {
     if (var) R = L.R[s * LP + l], Q = L.Qs[s * LP + l], psi = L.psi[s * LP + l];
 #pragma unroll
     for (int d = 0; d < 3; ++d) nb[d] = act ? next[d * S + s] : -1;
+    const double *row = L.pt + (int64_t)(act ? s : 0) * kLuScalars;
 #pragma unroll
-    for (int e = 0; e < 9; ++e) kv[e] = act ? L.kv[e * S + s] : 0.0;
+    for (int e = 0; e < 9; ++e) kv[e] = act ? row[kLuK + e] : 0.0;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) rad[d] = act ? L.rad[d * S + s] : 0.0;
-    rD = act ? L.rdiag[s] : 0.0, ps = act ? L.ps[s] : 0.0, gam = act ? L.gam[s] : 1.0;
-    inv = act ? L.vel[s] : 0.0, u = act ? L.vel[S + s] : 0.0, v = act ? L.vel[2 * S + s] : 0.0;
-    w = act ? L.vel[3 * S + s] : 0.0;
+    for (int d = 0; d < 3; ++d) rad[d] = act ? row[kLuRad + d] : 0.0;
+    rD = act ? row[kLuRD] : 0.0, ps = act ? row[kLuP] : 0.0, gam = act ? row[kLuGam] : 1.0;
+    inv = act ? row[kLuInv] : 0.0, u = act ? row[kLuU] : 0.0, v = act ? row[kLuU + 1] : 0.0;
+    w = act ? row[kLuU + 2] : 0.0;
   }
 
-  // CG: read the rows through L2 (written by other CTAs of the same launch)
-  template <bool CG>
   __device__ __forceinline__ void solve(const LusgsArgs &L, int nv) {
     double *__restrict__ Cn = L.Cn;
     double acc = DIR > 0 ? R : 0.0;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double *c = Cn + ((int64_t)d * S + s) * LP + l;
-      if (var) acc += CG ? __ldcg(c) : *c;
+      if (var) acc += *c;
     }
     const double X = DIR > 0 ? acc * rD : R - acc * rD;
     if (var) L.R[s * LP + l] = X;
@@ -262,64 +259,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_lusgs_sweep(const LusgsArgs L
   const int64_t s = L.s0 + (int64_t)blockIdx.x * (kSweepThreads / Lane::LP) + threadIdx.x / Lane::LP;
   Lane pt;
   pt.load(L, nv, (int)s, threadIdx.x % Lane::LP, s < L.s1);
-  pt.template solve<false>(L, nv);
-}
-
-// A whole sweep in one launch.  The hyperplanes are cut into chunks of
-// lusgs_chunk_points(n_var) points; CTAs take chunk tickets in sweep order
-// (ascending hyperplanes for the lower sweep, descending for the upper) from
-// W.counters[0], load their points' own data, wait until every chunk of the
-// preceding hyperplane has been counted in W.counters[2 + h], solve and count
-// their chunk.  A ticket is only taken by a running CTA, and every chunk a
-// CTA waits for has a lower ticket, so the waits end without any assumption
-// on how many CTAs are resident.  A wait that exceeds kSweepPolls polls sets
-// kStatusSweepTimeout and W.counters[1]; every CTA then leaves (the step's
-// result is invalid and the status word says so).
-template <int NS, int DIR>
-__global__ void __launch_bounds__(kSweepThreads) k_lusgs_sweep_all(const LusgsArgs L, const SweepWork W,
-                                                                   const __grid_constant__ ChemParams C) {
-  using Lane = LusgsLane<NS, DIR>;
-  __shared__ int sh_c, sh_abort;
-  volatile unsigned *vabort = W.counters + 1;
-  const int nv = 5 + SpecCount<NS>::n(C);
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const int t = (int)atomicAdd(W.counters, 1u);
-      sh_c = t < W.n_chunks ? (DIR > 0 ? t : W.n_chunks - 1 - t) : -1;
-    }
-    __syncthreads();
-    const int c = sh_c;
-    if (c < 0) return;
-    const int h = W.chunk_h[c];
-    const int64_t s = W.chunk_s0[c] + threadIdx.x / Lane::LP;
-    Lane pt;
-    pt.load(L, nv, (int)s, threadIdx.x % Lane::LP, s < W.h_end[h]);  // in flight while thread 0 waits
-    if (threadIdx.x == 0) {
-      int abort = *vabort != 0;
-      const int hw = h - DIR;  // hyperplane this chunk depends on
-      if (!abort && hw >= 0 && hw < W.H) {
-        const unsigned need = (unsigned)W.h_chunks[hw];
-        volatile unsigned *done = W.counters + 2 + hw;
-        long polls = 0;
-        while (*done < need) {
-          if (*vabort || ++polls > kSweepPolls) {
-            if (polls > kSweepPolls) atomicOr(W.status, kStatusSweepTimeout), atomicExch(W.counters + 1, 1u);
-            abort = 1;
-            break;
-          }
-          __nanosleep(32);
-        }
-        __threadfence();  // acquire: the counted chunks' stores are visible from here
-      }
-      sh_abort = abort;
-    }
-    __syncthreads();
-    if (sh_abort) return;
-    pt.template solve<true>(L, nv);
-    __threadfence();  // release this thread's stores before the chunk is counted
-    __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(W.counters + 2 + h, 1u);
-  }
+  pt.solve(L, nv);
 }
 
 // Q += dQ and the primitive recovery, transport and |V| of the new state

@@ -358,23 +358,6 @@ def test_lusgs_multiblock64_small_matches_oracle():
     assert not bad, errs
 
 
-def test_lusgs_one_launch_sweeps_equal_per_plane_launches(monkeypatch):
-    """The one-launch sweeps (chunk tickets, counted hyperplanes) give the
-    state of one launch per hyperplane bit for bit, on uneven blocks."""
-    case = _with_cfl(MB64_SMALL, 5.0)
-    out = []
-    for mode in ("planes", "one"):
-        monkeypatch.setenv("CC_LUSGS_SWEEP", mode)
-        d = cc.Driver.from_case(case, "fp64")
-        d.initialize_computation()
-        d.simulate(3, "lusgs")
-        assert d.status() == 0
-        out.append([d.field[b].get_state()[2] for b in range(len(case["blocks"]))])
-        d.close()
-    for a, b in zip(out[0], out[1]):
-        np.testing.assert_array_equal(a, b)
-
-
 def test_lusgs_graph_replay_equals_launches():
     case = _with_cfl(CASES["multiblock"], 5.0)
     out = []
