@@ -61,22 +61,46 @@ __device__ __forceinline__ void lusgs_jac_vec(int nv, const double (&Q)[NV], dou
     if (l < nv) dF[l] = dQ[l] * U + Q[l] * dU;
 }
 
+// Rows of 16 doubles for 32 points, one per lane, written to their sweep-order
+// positions: the lanes first put their rows into a per-warp shared-memory
+// buffer, then each store instruction writes two whole rows (two 128-byte
+// lines) instead of one word of 32 scattered rows.  Row element e of lane r
+// goes to dst[pos_r * stride + e]; lanes without a point pass pos = -1.
+__device__ __forceinline__ void lusgs_put_rows(double (*buf)[17], const double (&v)[16], int64_t pos, double *dst,
+                                               int stride) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) buf[lane][e] = v[e];
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    const int r = 2 * m + (lane >> 4), e = lane & 15;
+    const int64_t pr = __shfl_sync(0xffffffffu, pos, r);
+    if (pr >= 0) dst[pr * stride + e] = buf[r][e];
+  }
+  __syncwarp();
+}
+
 // Right-hand side, spectral radii, diagonal and the Jacobian inputs of every
 // interior point of the tiles (the split variant's face arena holds the
-// current fluxes), written in sweep order.
+// current fluxes), written in sweep order as whole rows (unused lanes zero).
 template <typename T, int NS>
 __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2) k_lusgs_rhs(const StageArgs<T> a, const LusgsArgs L,
-                                                      const __grid_constant__ ChemParams C) {
+                                                                             const __grid_constant__ ChemParams C) {
   constexpr int A = SpecCount<NS>::kArr;
   constexpr int NV = 5 + A;
+  static_assert(NV <= 16 || NS < 0, "rows are 16 doubles for the compiled species counts");
   const int ns = SpecCount<NS>::n(C);
   const int nv = 5 + ns;
+  __shared__ double sbuf[kTX * kTY / 32][32][17];
+  double (*buf)[17] = sbuf[(threadIdx.y * kTX + threadIdx.x) >> 5];
   const Tile t = a.tiles[blockIdx.x];
   const BlockInfo B = a.blocks[t.blk];
   const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
-  if (i >= B.mx || j >= B.my) return;
+  const bool act = i < B.mx && j < B.my;  // inactive lanes still take part in the row writes
   const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
   const int64_t S = L.S;
+  const int lp = L.lp;
   const bool three_d = B.mz > 1;
   const T *__restrict__ P = a.P;
   const T *__restrict__ G = a.G;
@@ -84,79 +108,122 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2) k_lusgs_rhs(
   const T *__restrict__ Fy = a.faces + (size_t)nv * N;
   const T *__restrict__ Fz = a.faces + (size_t)2 * nv * N;
   const T *rec = param_rec<T>(C);
-  const int col = (int)B.base + i + sj * j;
+  const int col = (int)B.base + (act ? i + sj * j : 0);
   for (int k = t.k0; k < t.k1; ++k) {
     const int p = col + sk * k;
-    const int64_t sp = L.pos[p];
-    double *row = L.pt + sp * kLuScalars;
+    const int64_t sp = act ? (int64_t)L.pos[p] : -1;
+    if (NV > 16) {  // runtime species count beyond 11: plain stores of the wider rows
+      if (act) {
 #pragma unroll
-    for (int l = 0; l < NV; ++l) {
-      if (l < nv) {
-        const int o = l * N + p;
-        T acc = Fx[o] - Fx[o - 1];
-        acc += Fy[o] - Fy[o - sj];
-        if (three_d) acc += Fz[o] - Fz[o - sk];
-        double dq = -(double)acc;
-        if (a.gcl && l >= 1 && l <= 3) dq -= C.p_ref * a.gcl[(l - 1) * N + p];
-        L.R[sp * L.lp + l] = dq;
-        L.Qs[sp * L.lp + l] = a.Qin[o];
+        for (int l = 0; l < NV; ++l) {
+          if (l < nv) {
+            const int o = l * N + p;
+            T acc = Fx[o] - Fx[o - 1];
+            acc += Fy[o] - Fy[o - sj];
+            if (three_d) acc += Fz[o] - Fz[o - sk];
+            double dq = -(double)acc;
+            if (a.gcl && l >= 1 && l <= 3) dq -= C.p_ref * a.gcl[(l - 1) * N + p];
+            L.R[sp * lp + l] = dq;
+            L.Qs[sp * lp + l] = a.Qin[o];
+          }
+        }
       }
+    } else {
+      double rv[16], qv[16];
+#pragma unroll
+      for (int l = 0; l < 16; ++l) {
+        rv[l] = qv[l] = 0.0;
+        if (act && l < nv) {
+          const int o = l * N + p;
+          T acc = Fx[o] - Fx[o - 1];
+          acc += Fy[o] - Fy[o - sj];
+          if (three_d) acc += Fz[o] - Fz[o - sk];
+          double dq = -(double)acc;
+          if (a.gcl && l >= 1 && l <= 3) dq -= C.p_ref * a.gcl[(l - 1) * N + p];
+          rv[l] = dq;
+          qv[l] = a.Qin[o];
+        }
+      }
+      lusgs_put_rows(buf, rv, lp == 16 ? sp : -1, L.R, 16);
+      lusgs_put_rows(buf, qv, lp == 16 ? sp : -1, L.Qs, 16);
+      if (lp != 16 && act)  // 8-lane rows (the air model)
+#pragma unroll
+        for (int l = 0; l < 8; ++l) L.R[sp * lp + l] = rv[l], L.Qs[sp * lp + l] = qv[l];
     }
-    {
+    double row[32];
+#pragma unroll
+    for (int e = 0; e < 32; ++e) row[e] = 0.0;
+    double psi[16];
+#pragma unroll
+    for (int l = 0; l < 16; ++l) psi[l] = 0.0;
+    if (act) {
       const double inv = 1.0 / a.Qin[p];
       row[kLuInv] = inv;
       row[kLuU] = a.Qin[N + p] * inv;
       row[kLuU + 1] = a.Qin[2 * N + p] * inv;
       row[kLuU + 2] = a.Qin[3 * N + p] * inv;
-    }
-    row[kLuP] = (double)P[4 * N + p] + C.p_ref;
-    T Y[A];
-#pragma unroll
-    for (int l = 0; l < A; ++l)
-      if (l < ns) Y[l] = P[(6 + l) * N + p];
-    T gam, c;
-    gamma_and_c<T, NS>(C, rec, P[5 * N + p], Y, gam, c);
-    const double rho = (double)P[p], u = (double)P[N + p], v = (double)P[2 * N + p], w = (double)P[3 * N + p];
-    const double mu = (double)a.Pr[p];
-    const double dt = local_time_step<T>(C, G, N, p, rho, u, v, w, (double)c, (double)gam, mu, three_d);
-    const double J = (double)G[p];
-    const double c1 = fmax((double)gam, 4.0 / 3.0);
-    const double c2 = mu / rho / C.Pr;
-    double D = J / dt;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      double r = 0;
-      const double m0 = (double)G[(1 + 3 * d) * N + p], m1 = (double)G[(2 + 3 * d) * N + p],
-                   m2 = (double)G[(3 + 3 * d) * N + p];
-      if (d < 2 || three_d) {
-        const double g = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
-        const double U = u * m0 + v * m1 + w * m2;
-        r = fabs(U) + (double)c * g;
-        if (C.viscous) r += 2.0 * c1 * c2 * g * g;
-        r *= J;
-        D += r;
-      }
-      row[kLuRad + d] = r;
-      row[kLuK + 3 * d] = J * m0;
-      row[kLuK + 3 * d + 1] = J * m1;
-      row[kLuK + 3 * d + 2] = J * m2;
-    }
-    row[kLuRD] = 1.0 / D;
-    row[kLuGam] = (double)gam;
-    const int id[3] = {i, j, k};
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-      if (id[d] == 0)  // no lower neighbour: nothing arrives in this slot during the lower sweep
-#pragma unroll
-        for (int l = 0; l < NV; ++l)
-          if (l < nv) L.Cn[(d * S + sp) * L.lp + l] = 0.0;
-    if (ns > 0) {
-      const double td = (double)P[5 * N + p], g1 = (double)gam - 1.0;
+      row[kLuP] = (double)P[4 * N + p] + C.p_ref;
+      T Y[A];
 #pragma unroll
       for (int l = 0; l < A; ++l)
-        if (l < ns)
-          L.psi[sp * L.lp + 5 + l] =
-              (double)gam * C.d.cv_shift[l] * td - g1 * nasa_h<double>(C.d, param_rec<double>(C), l, td);
+        if (l < ns) Y[l] = P[(6 + l) * N + p];
+      T gam, c;
+      gamma_and_c<T, NS>(C, rec, P[5 * N + p], Y, gam, c);
+      const double rho = (double)P[p], u = (double)P[N + p], v = (double)P[2 * N + p], w = (double)P[3 * N + p];
+      const double mu = (double)a.Pr[p];
+      const double dt = local_time_step<T>(C, G, N, p, rho, u, v, w, (double)c, (double)gam, mu, three_d);
+      const double J = (double)G[p];
+      const double c1 = fmax((double)gam, 4.0 / 3.0);
+      const double c2 = mu / rho / C.Pr;
+      double D = J / dt;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double r = 0;
+        const double m0 = (double)G[(1 + 3 * d) * N + p], m1 = (double)G[(2 + 3 * d) * N + p],
+                     m2 = (double)G[(3 + 3 * d) * N + p];
+        if (d < 2 || three_d) {
+          const double g = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+          const double U = u * m0 + v * m1 + w * m2;
+          r = fabs(U) + (double)c * g;
+          if (C.viscous) r += 2.0 * c1 * c2 * g * g;
+          r *= J;
+          D += r;
+        }
+        row[kLuRad + d] = r;
+        row[kLuK + 3 * d] = J * m0;
+        row[kLuK + 3 * d + 1] = J * m1;
+        row[kLuK + 3 * d + 2] = J * m2;
+      }
+      row[kLuRD] = 1.0 / D;
+      row[kLuGam] = (double)gam;
+      const int id[3] = {i, j, k};
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (id[d] == 0)  // no lower neighbour: nothing arrives in this row during the lower sweep
+          for (int l = 0; l < lp; ++l) L.Cn[(d * S + sp) * lp + l] = 0.0;
+      if (ns > 0) {
+        const double td = (double)P[5 * N + p], g1 = (double)gam - 1.0;
+#pragma unroll
+        for (int l = 0; l < A; ++l) {
+          if (l < ns) {
+            const double x = (double)gam * C.d.cv_shift[l] * td - g1 * nasa_h<double>(C.d, param_rec<double>(C), l, td);
+            if (NV <= 16)
+              psi[5 + l] = x;
+            else
+              L.psi[sp * lp + 5 + l] = x;
+          }
+        }
+      }
+    }
+    double half[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) half[e] = row[e];
+    lusgs_put_rows(buf, half, sp, L.pt, kLuScalars);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) half[e] = row[16 + e];
+    lusgs_put_rows(buf, half, sp, L.pt + 16, kLuScalars);
+    if (NV <= 16 && ns > 0) {
+      lusgs_put_rows(buf, psi, lp == 16 ? sp : -1, L.psi, 16);
     }
   }
 }
@@ -173,8 +240,8 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2) k_lusgs_rhs(
 // lanes by shuffles, and every lane evaluates the oracle's expressions in
 // its order.  In the lower sweep a point also clears the rows that no
 // neighbour fills in the upper sweep.  Every lane of the warp runs the
-// shuffles; lanes without a point or a variable only mask their memory
-// accesses.  Offsets are 32-bit (3 lp S < 2^31 is checked at allocation).
+// shuffles; lanes without a point mask their memory accesses, lanes without
+// a variable hold zeros and store them, so that every row is written whole.  Offsets are 32-bit (3 lp S < 2^31 is checked at allocation).
 template <int NS, int DIR>
 struct LusgsLane {
   static constexpr int A = SpecCount<NS>::kArr;
@@ -210,8 +277,8 @@ struct LusgsLane {
       if (var) acc += *c;
     }
     const double X = DIR > 0 ? acc * rD : R - acc * rD;
-    if (var) L.R[s * LP + l] = X;
-    if (DIR > 0 && var) {
+    if (act) L.R[s * LP + l] = X;  // whole rows: lanes without a variable store 0
+    if (DIR > 0 && act) {
 #pragma unroll
       for (int d = 0; d < 3; ++d)
         if (nb[d] < 0) Cn[((int64_t)d * S + s) * LP + l] = 0.0;
@@ -230,7 +297,7 @@ struct LusgsLane {
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      if (nb[d] < 0 || !var) continue;
+      if (nb[d] < 0 || !act) continue;
       const double k0 = kv[3 * d], k1 = kv[3 * d + 1], k2 = kv[3 * d + 2];
       const double U = k0 * u + k1 * v + k2 * w;
       const double dm = k0 * x1 + k1 * x2 + k2 * x3;
