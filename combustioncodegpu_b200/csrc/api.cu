@@ -725,11 +725,11 @@ int lusgs_and_halo(cc_ctx *c, StageArgs<T> a, int pn, int pc) {
   CK((Launch<T, NS>::lusgs_rhs(a, L, c->chem, nt, c->stream)));
   const int H = (int)c->lu_hb.size() - 1;
   for (int h = 0; h < H; ++h) {
-    L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1];
+    L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1], L.early = h > 0;
     CK((Launch<T, NS>::lusgs_sweep(L, c->chem, 1, c->stream)));
   }
   for (int h = H - 1; h >= 0; --h) {
-    L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1];
+    L.s0 = c->lu_hb[h], L.s1 = c->lu_hb[h + 1], L.early = h < H - 1;
     CK((Launch<T, NS>::lusgs_sweep(L, c->chem, -1, c->stream)));
   }
   a.gcl = nullptr;  // the geometric term is part of the right-hand side

@@ -173,6 +173,7 @@ struct LusgsArgs {
                      //             at this point's row (zero where the block has no such neighbour)
   double *pt;        // [S][kLuScalars]: the point's scalars, at the kLu* offsets
   int64_t s0, s1;    // sweep positions of one launch (one hyperplane)
+  int early;         // 1: the launch may read its points' own rows before waiting for its predecessor
 };
 
 // Offsets in a point's scalar row (LusgsArgs::pt): 1 / D (D = J / dt_local +

@@ -130,12 +130,18 @@ cudaError_t Launch<T, NS>::lusgs_sweep(const LusgsArgs &L, const ChemParams &C, 
   if (n <= 0) return cudaSuccess;
   if (L.lp != LusgsLane<NS, 1>::LP) return cudaErrorInvalidValue;  // rows laid out for another lane count
   const int pts = kSweepThreads / LusgsLane<NS, 1>::LP;
-  const unsigned grid = (unsigned)((n + pts - 1) / pts);
-  if (dir > 0)
-    k_lusgs_sweep<NS, 1><<<grid, kSweepThreads, 0, s>>>(L, C);
-  else
-    k_lusgs_sweep<NS, -1><<<grid, kSweepThreads, 0, s>>>(L, C);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)((n + pts - 1) / pts));
+  cfg.blockDim = dim3(kSweepThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // programmatic dependent launch
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (dir > 0) return cudaLaunchKernelEx(&cfg, k_lusgs_sweep<NS, 1>, L, C);
+  return cudaLaunchKernelEx(&cfg, k_lusgs_sweep<NS, -1>, L, C);
 }
 
 template <typename T, int NS>

@@ -27,7 +27,8 @@
 //
 // A point of sweep hyperplane h = i + j + k depends only on hyperplane h - 1
 // (h + 1 for the upper sweep), so each hyperplane is one launch over all
-// blocks, in order.  The sweeps read and write arrays in sweep order (points
+// blocks, in order, chained by programmatic dependent launch so that a
+// launch and its own loads overlap the previous hyperplane.  The sweeps read and write arrays in sweep order (points
 // sorted by hyperplane, block, k, j; LusgsArgs): the points of a hyperplane
 // are contiguous and the neighbours a warp reads in the adjacent hyperplane
 // are too.  The arithmetic of each point is the oracle's lexicographic sweep,
@@ -251,21 +252,24 @@ struct LusgsLane {
   bool act, var;  // the group has a point; this lane has a variable
   double R, Q, psi, kv[9], rad[3], rD, ps, gam, inv, u, v, w;
 
+  // All loads go through L2 (ld.global.cg): with programmatic dependent
+  // launch they may run while the preceding kernel is still finishing, and
+  // an L1 line of an earlier kernel on this SM must not be used.
   __device__ __forceinline__ void load(const LusgsArgs &L, int nv, int s_, int l_, bool act_) {
     s = s_, S = (int)L.S, l = l_, act = act_, var = act_ && l_ < nv;
     const int *__restrict__ next = DIR > 0 ? L.hi : L.lo;  // neighbours of the next hyperplane
     R = Q = psi = 0.0;
-    if (var) R = L.R[s * LP + l], Q = L.Qs[s * LP + l], psi = L.psi[s * LP + l];
+    if (var) R = __ldcg(L.R + s * LP + l), Q = __ldcg(L.Qs + s * LP + l), psi = __ldcg(L.psi + s * LP + l);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) nb[d] = act ? next[d * S + s] : -1;
+    for (int d = 0; d < 3; ++d) nb[d] = act ? __ldcg(next + d * S + s) : -1;
     const double *row = L.pt + (int64_t)(act ? s : 0) * kLuScalars;
 #pragma unroll
-    for (int e = 0; e < 9; ++e) kv[e] = act ? row[kLuK + e] : 0.0;
+    for (int e = 0; e < 9; ++e) kv[e] = act ? __ldcg(row + kLuK + e) : 0.0;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) rad[d] = act ? row[kLuRad + d] : 0.0;
-    rD = act ? row[kLuRD] : 0.0, ps = act ? row[kLuP] : 0.0, gam = act ? row[kLuGam] : 1.0;
-    inv = act ? row[kLuInv] : 0.0, u = act ? row[kLuU] : 0.0, v = act ? row[kLuU + 1] : 0.0;
-    w = act ? row[kLuU + 2] : 0.0;
+    for (int d = 0; d < 3; ++d) rad[d] = act ? __ldcg(row + kLuRad + d) : 0.0;
+    rD = act ? __ldcg(row + kLuRD) : 0.0, ps = act ? __ldcg(row + kLuP) : 0.0, gam = act ? __ldcg(row + kLuGam) : 1.0;
+    inv = act ? __ldcg(row + kLuInv) : 0.0, u = act ? __ldcg(row + kLuU) : 0.0;
+    v = act ? __ldcg(row + kLuU + 1) : 0.0, w = act ? __ldcg(row + kLuU + 2) : 0.0;
   }
 
   __device__ __forceinline__ void solve(const LusgsArgs &L, int nv) {
@@ -274,7 +278,7 @@ struct LusgsLane {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double *c = Cn + ((int64_t)d * S + s) * LP + l;
-      if (var) acc += *c;
+      if (var) acc += __ldcg(c);
     }
     const double X = DIR > 0 ? acc * rD : R - acc * rD;
     if (act) L.R[s * LP + l] = X;  // whole rows: lanes without a variable store 0
@@ -325,7 +329,17 @@ __global__ void __launch_bounds__(kSweepThreads) k_lusgs_sweep(const LusgsArgs L
   const int nv = 5 + SpecCount<NS>::n(C);
   const int64_t s = L.s0 + (int64_t)blockIdx.x * (kSweepThreads / Lane::LP) + threadIdx.x / Lane::LP;
   Lane pt;
-  pt.load(L, nv, (int)s, threadIdx.x % Lane::LP, s < L.s1);
+  // Programmatic dependent launch: this kernel may start while the previous
+  // hyperplane's is still running.  The point's own rows were written by the
+  // right-hand side kernel or the lower sweep, which completed before the
+  // previous launch passed its wait (it only lets this launch start after
+  // that), so they are read before waiting, except by the first launch of a
+  // sweep (L.early = 0), whose predecessor produced them.  The neighbour
+  // rows of L.Cn are written by the previous launch: read after the wait.
+  if (L.early) pt.load(L, nv, (int)s, threadIdx.x % Lane::LP, s < L.s1);
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (!L.early) pt.load(L, nv, (int)s, threadIdx.x % Lane::LP, s < L.s1);
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   pt.solve(L, nv);
 }
 
