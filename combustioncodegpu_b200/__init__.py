@@ -112,6 +112,11 @@ EXPORTS = {
     "cc_save_checkpoint": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
     "cc_load_checkpoint": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
     "cc_sync": ([ctypes.c_void_p], ctypes.c_int),
+    "cc_mlp_param_count": ([ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int64),
+    "cc_mlp_workspace_bytes": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int64),
+    "cc_mlp_grad": ([ctypes.c_int] * 4 + [ctypes.c_void_p] * 8, ctypes.c_int),
+    "cc_mlp_adam": ([ctypes.c_int64] + [ctypes.c_void_p] * 4 + [ctypes.c_float] * 4 + [ctypes.c_int, ctypes.c_void_p],
+                    ctypes.c_int),
     "cc_residual_rms_noalloc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
                                 ctypes.c_int),
 }

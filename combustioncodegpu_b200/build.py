@@ -16,7 +16,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcc_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = [
-    "api.cu", "misc.cu", "halo_plan.cpp", "noalloc.cu",
+    "api.cu", "misc.cu", "halo_plan.cpp", "noalloc.cu", "closure_train.cu",
     "inst_d0.cu", "inst_d9.cu", "inst_dn.cu", "inst_f0.cu", "inst_f9.cu", "inst_fn.cu",
 ]
 

@@ -11,12 +11,18 @@ targets are the library's own exact FP64 transport of those points
 the kernel: inputs as BF16 (hi, lo) pairs, BF16 weights and BF16 hidden
 activations (rounding with a straight-through gradient), FP32 accumulation,
 FP32 biases; the loss is the mean squared error of the log properties, i.e.
-of the relative error.  Training runs on the GPU with PyTorch (an offline
-step, not the hot path); the result is a dict that Driver.set_closure takes.
+of the relative error.  Training runs on the GPU with the library's own
+forward/backward and Adam kernels (cc_mlp_grad, cc_mlp_adam; an offline
+step, not the hot path), checked against the CPU restatement of the same
+math in oracle/closure_mlp.py; the result is a dict that Driver.set_closure
+takes.  ClosureNet is the plain PyTorch FP32 model of the same network with
+the same rounding points: the reference the inference kernel is tested
+against, and the evaluation of the trained weights.
 
   python -m combustioncodegpu_b200.closure --out closure_weights.npz
 """
 import argparse
+import ctypes
 import json
 import os
 import time
@@ -98,12 +104,34 @@ class ClosureNet:
         return d
 
 
+def one_cycle(step, total, max_lr, pct_start=0.05, div_factor=25.0, final_div_factor=1e4,
+              beta_lo=0.85, beta_hi=0.95):
+    """(lr, beta1) of the one-cycle policy (Smith & Topin, 2019) at step
+    (0-based) of total: cosine warm-up from max_lr / div_factor to max_lr over
+    pct_start of the steps while beta1 falls from beta_hi to beta_lo, then
+    cosine decay to max_lr / (div_factor * final_div_factor) while beta1
+    returns to beta_hi."""
+    lo_lr = max_lr / div_factor
+    end1 = pct_start * total - 1.0
+    cos = lambda a, b, t: b + (a - b) / 2.0 * (1.0 + np.cos(np.pi * t))
+    if step <= end1:
+        t = step / end1 if end1 > 0 else 1.0
+        return cos(lo_lr, max_lr, t), cos(beta_hi, beta_lo, t)
+    t = (step - end1) / max(1.0, (total - 1) - end1)
+    return cos(max_lr, lo_lr / final_div_factor, t), cos(beta_lo, beta_hi, t)
+
+
 def train(driver, species, n_samples=2_000_000, n_val=200_000, epochs=60, batch=4096, lr=2e-3, seed=7,
           device="cuda", log=print):
-    """Fit the closure to the exact transport of `driver`'s species tables.
+    """Fit the closure to the exact transport of `driver`'s species tables
+    with the library's training kernels (cc_mlp_grad: quantisation-aware
+    forward and backward; cc_mlp_adam).  PyTorch only holds the device
+    arrays, draws the initial weights and shuffles the batches.
     Returns (weights dict, report dict)."""
     import torch
+    from . import load_library
 
+    lib = load_library()
     t0 = time.time()
     T, Y, X = sample_states(n_samples + n_val, species, seed)
     tgt = np.log(driver.eval_transport(T, Y, "exact"))  # [2+ns][n]
@@ -116,32 +144,54 @@ def train(driver, species, n_samples=2_000_000, n_val=200_000, epochs=60, batch=
     y_all = torch.as_tensor(((tgt - mean[:, None]) / scale[:, None]).T, dtype=torch.float32, device=device)
     sc = torch.as_tensor(scale, dtype=torch.float32, device=device)
     xtr, ytr = x_all[:n_samples], y_all[:n_samples]
-    net = ClosureNet(n_in, n_out, device, seed)
-    opt = torch.optim.Adam(net.params, lr=lr)
+    net = ClosureNet(n_in, n_out, device, seed)  # initial weights
+    params = torch.cat([p.detach().reshape(-1) for p in net.params]).contiguous()
+    n_par = lib.cc_mlp_param_count(n_in, HIDDEN, n_out)
+    assert n_par == params.numel()
+    grad = torch.zeros_like(params)
+    m1 = torch.zeros_like(params)
+    m2 = torch.zeros_like(params)
+    work = torch.empty(lib.cc_mlp_workspace_bytes(n_in, HIDDEN, n_out, batch), dtype=torch.uint8, device=device)
+    loss = torch.zeros(1, dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream().cuda_stream
     steps = epochs * (n_samples // batch)
-    sched = torch.optim.lr_scheduler.OneCycleLR(opt, max_lr=lr, total_steps=steps, pct_start=0.05)
     gen = torch.Generator(device=device).manual_seed(seed)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
     t1 = time.time()
+    step = 0
     for ep in range(epochs):
         perm = torch.randperm(n_samples, device=device, generator=gen)
-        tot = 0.0
+        tot, cnt = 0.0, 0
         for b in range(n_samples // batch):
             idx = perm[b * batch:(b + 1) * batch]
-            err = (net.forward(xtr[idx]) - ytr[idx]) * sc  # error of the log properties
-            loss = (err * err).mean()
-            opt.zero_grad(set_to_none=True)
-            loss.backward()
-            opt.step()
-            sched.step()
-            tot += float(loss.detach()) if b % 50 == 0 else 0.0
+            xb, yb = xtr[idx].contiguous(), ytr[idx].contiguous()
+            rc = lib.cc_mlp_grad(n_in, HIDDEN, n_out, batch, vp(params), vp(xb), vp(yb), vp(sc), vp(grad), vp(loss),
+                                 vp(work), ctypes.c_void_p(stream))
+            if rc != 0:
+                raise RuntimeError(lib.cc_last_error().decode())
+            lr_t, beta1 = one_cycle(step, steps, lr)
+            step += 1
+            rc = lib.cc_mlp_adam(n_par, vp(params), vp(grad), vp(m1), vp(m2), lr_t, beta1, 0.999, 1e-8, step,
+                                 ctypes.c_void_p(stream))
+            if rc != 0:
+                raise RuntimeError(lib.cc_last_error().decode())
+            if b % 50 == 0:
+                tot, cnt = tot + float(loss), cnt + 1
         if ep % 10 == 0 or ep == epochs - 1:
-            log("epoch %d  loss(sampled) %.3e" % (ep, tot / max(1, (n_samples // batch) // 50)))
+            log("epoch %d  loss(sampled) %.3e" % (ep, tot / max(1, cnt)))
+    torch.cuda.synchronize()
     t_train = time.time() - t1
+    off = 0
+    for p in net.params:  # the trained weights back into the PyTorch model, for its evaluation below
+        with torch.no_grad():
+            p.copy_(params[off:off + p.numel()].view_as(p))
+        off += p.numel()
     w = net.export(mean, scale)
     with torch.no_grad():
-        o = net.forward(x_all[n_samples:]).cpu().numpy() * scale + mean  # torch model, log space
+        o = net.forward(x_all[n_samples:]).cpu().numpy() * scale + mean  # the trained model, log space
     rel_torch = np.abs(np.expm1(o.T - tgt[:, n_samples:]))
     report = {"n_samples": n_samples, "n_val": n_val, "epochs": epochs, "batch": batch, "seed": seed,
+              "trainer": "cc_mlp_grad + cc_mlp_adam (the library's kernels), one-cycle schedule",
               "seconds_data": t_data, "seconds_train": t_train,
               "torch_model_rel_err": _err_summary(rel_torch)}
     return w, report

@@ -241,6 +241,27 @@ int cc_load_checkpoint(cc_ctx *ctx, const char *path);
 /* Synchronises the context's stream. */
 int cc_sync(cc_ctx *ctx);
 
+/* Training of the learned transport closure (no counterpart in the
+ * reference): the 4-layer MLP n_in -> hidden -> hidden -> hidden -> n_out
+ * (SiLU) of cc_closure, trained with the inference kernel's rounding points
+ * (layer inputs and weights rounded to BF16 in the forward pass, passed
+ * through unchanged in the backward pass; FP32 master weights, biases and
+ * accumulation).  Widths at most 64.  params: one FP32 buffer W1 [hidden][n_in],
+ * b1, W2 [hidden][hidden], b2, W3, b3, W4 [n_out][hidden], b4 of
+ * cc_mlp_param_count floats.  All pointers are device memory owned by the
+ * caller; nothing is allocated; work is cc_mlp_workspace_bytes bytes.
+ * cc_mlp_grad: loss = mean over batch and outputs of ((mlp(x) - y) scale)^2
+ * (x [batch][n_in] holding BF16-representable values, y [batch][n_out],
+ * scale [n_out]) into *loss and its gradient into grad, enqueued on stream;
+ * sums run in a fixed order, so results are reproducible bit for bit.
+ * cc_mlp_adam: one Adam step (bias-corrected, step >= 1, no weight decay). */
+int64_t cc_mlp_param_count(int n_in, int hidden, int n_out);
+int64_t cc_mlp_workspace_bytes(int n_in, int hidden, int n_out, int batch);
+int cc_mlp_grad(int n_in, int hidden, int n_out, int batch, const float *params, const float *x, const float *y,
+                const float *out_scale, float *grad, float *loss, void *workspace, void *stream);
+int cc_mlp_adam(int64_t n, float *params, const float *grad, float *m, float *v, float lr, float beta1, float beta2,
+                float eps, int step, void *stream);
+
 /* No counterpart in the reference.  Residual norms without any allocation,
  * for callers that cannot call cudaMalloc where they need them (an
  * allocation-free loop, a host application that owns the device allocator):

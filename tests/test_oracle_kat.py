@@ -152,3 +152,34 @@ def test_renormalised_mass_fractions_sum_to_one(species):
     yk = o.state(0)[1]
     g = yk.reshape(species["n_spec"], 12, 12, 12)[:, 2:-2, 2:-2, 2:-2].sum(axis=0)
     np.testing.assert_allclose(g, 1.0, rtol=0, atol=1e-14)
+
+
+def test_closure_mlp_oracle_gradient_by_finite_difference():
+    """The oracle's backward pass (the checker of the training kernels),
+    without its BF16 rounding: central differences of the loss."""
+    from oracle import closure_mlp as om
+
+    rng = np.random.default_rng(4)
+    n_in, H, n_out, B = 5, 7, 3, 9
+    lay, n = om.layout(n_in, H, n_out)
+    p = rng.standard_normal(n) * 0.5
+    x, y = rng.standard_normal((B, n_in)), rng.standard_normal((B, n_out))
+    scale = rng.uniform(0.5, 2.0, n_out)
+    _, g = om.loss_and_grad(p, x, y, scale, n_in, H, n_out, quantized=False)
+    for e in rng.choice(n, 25, replace=False):
+        h = 1e-6
+        pp, pm = p.copy(), p.copy()
+        pp[e] += h
+        pm[e] -= h
+        fd = (om.loss_and_grad(pp, x, y, scale, n_in, H, n_out, quantized=False)[0]
+              - om.loss_and_grad(pm, x, y, scale, n_in, H, n_out, quantized=False)[0]) / (2 * h)
+        assert abs(fd - g[e]) <= 1e-6 * max(1.0, abs(g[e])), (e, fd, g[e])
+
+
+def test_bf16_rounding_ties_to_even():
+    from oracle import closure_mlp as om
+
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -1.0 - 2 ** -8, 1.0 + 2 ** -9, 3.14159], dtype=np.float32)
+    got = om.bf16(x)
+    np.testing.assert_array_equal(got[:5], np.array([1.0, 1.0, 1.0 + 2 ** -6, -1.0, 1.0], dtype=np.float32))
+    assert abs(got[5] - 3.140625) == 0.0
