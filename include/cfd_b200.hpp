@@ -44,6 +44,9 @@ class Parameter {
   bool get_bool(const std::string &key) const { return find(bools_, key); }
   const std::string &get_string(const std::string &key) const { return find(strings_, key); }
   bool has_int(const std::string &key) const { return ints_.count(key) != 0; }
+  bool has_real(const std::string &key) const { return reals_.count(key) != 0; }
+  bool has_bool(const std::string &key) const { return bools_.count(key) != 0; }
+  bool has_string(const std::string &key) const { return strings_.count(key) != 0; }
 
  private:
   template <typename M>
@@ -89,6 +92,7 @@ struct Mesh {
 // coefficient, and the Wilke factors [n][n].  n_spec = 0 selects the air model.
 struct Species {
   int n_spec = 0;
+  std::vector<std::string> names;  // mechanism order (ChemData.cpp:36-57)
   std::vector<double> mw, t_low, t_mid, t_high, low_temp_coeff, high_temp_coeff, LJ_potent_inv, vis_coeff,
       WjDivWi_to_One4th, sqrt_WiDivWjPl1Mul8;
 };
