@@ -167,7 +167,7 @@ cudaError_t Launch<T, NS>::halo_copies(const HaloArgs<T> &a, const ChemParams &C
   if (n <= 0) return cudaSuccess;
   const int ns = C.ns, np = 6 + ns, npr = 2 + ns, nq = 5 + ns;
   const int tpb = 256;
-  k_halo_copy_fields<T, NS><<<dim3((unsigned)((n + tpb - 1) / tpb), np + npr + nq), tpb, 0, s>>>(a, np, npr, nq);
+  k_halo_copy_fields<T, NS><<<dim3((unsigned)((n + tpb - 1) / tpb), 3), tpb, 0, s>>>(a, np, npr, nq);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !a.dt_next || a.n_icopies <= 0) return e;
   k_halo_copy_dt<T, NS><<<(unsigned)((a.n_icopies + tpb - 1) / tpb), tpb, 0, s>>>(a, C);

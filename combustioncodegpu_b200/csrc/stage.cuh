@@ -718,25 +718,44 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
   }
 }
 
-// Phase B: write every changed point from its resolved source, one thread
-// per (copy, field): consecutive threads move one field of consecutive
-// copies, so every thread issues one load and one store and the list's
-// destination order keeps them coalesced.
+// Phase B: write every changed point from its resolved source.  One thread
+// per (copy, array): grid y selects P, Pr or Q, and the thread moves all
+// fields of that array for its copy, loading them all before the first
+// store (the stores may alias the sources as far as the compiler knows).
+// Consecutive threads take consecutive copies, whose destinations (and
+// mostly sources) are consecutive, so every field access is coalesced; the
+// copy record is read once per array rather than once per field.
 template <typename T, int NS>
 __global__ void k_halo_copy_fields(const HaloArgs<T> a, int np, int npr, int nq) {
+  constexpr int A = SpecCount<NS>::kArr;
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // copy (grid x)
-  const int f = blockIdx.y;                                           // field (grid y)
   if (e >= a.end - a.begin) return;
   const HaloCopy c = a.copies[a.begin + e];
   const RefPtrs<T> r = resolve(a, c.src);
-  if (f < np) {
-    a.P[f * a.N + c.dst] = r.P[f * r.stride + r.idx];
-  } else if (f < np + npr) {
-    const int g = f - np;
-    a.Pr[g * a.N + c.dst] = r.Pr[g * r.stride + r.idx];
+  if (blockIdx.y == 0) {
+    T v[6 + A];
+#pragma unroll
+    for (int f = 0; f < 6 + A; ++f)
+      if (f < np) v[f] = r.P[f * r.stride + r.idx];
+#pragma unroll
+    for (int f = 0; f < 6 + A; ++f)
+      if (f < np) a.P[f * a.N + c.dst] = v[f];
+  } else if (blockIdx.y == 1) {
+    T v[2 + A];
+#pragma unroll
+    for (int f = 0; f < 2 + A; ++f)
+      if (f < npr) v[f] = r.Pr[f * r.stride + r.idx];
+#pragma unroll
+    for (int f = 0; f < 2 + A; ++f)
+      if (f < npr) a.Pr[f * a.N + c.dst] = v[f];
   } else {
-    const int g = f - np - npr;
-    a.Q[g * a.N + c.dst] = r.Q[g * r.stride + r.idx];
+    double v[5 + A];
+#pragma unroll
+    for (int f = 0; f < 5 + A; ++f)
+      if (f < nq) v[f] = r.Q[f * r.stride + r.idx];
+#pragma unroll
+    for (int f = 0; f < 5 + A; ++f)
+      if (f < nq) a.Q[f * a.N + c.dst] = v[f];
   }
 }
 
