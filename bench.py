@@ -47,7 +47,7 @@ def parse():
                          "box256_closure: 256^3 box, exact transport vs the learned closure; "
                          "box128_lusgs: LU-SGS steady steps on the 128^3 box")
     ap.add_argument("--study-steps", default="100,1000,2000", help="mixing_layer: error snapshot steps")
-    ap.add_argument("--variant", default="auto", choices=["auto", "l1", "tma", "split", "split-tma"],
+    ap.add_argument("--variant", default="auto", choices=["auto", "l1", "tma", "split", "split-tma", "split-tma-p"],
                     help="stage kernels: autotuned (default) or pinned (profiling runs, where the autotuner's "
                          "timings are distorted)")
     return ap.parse_args()
@@ -556,10 +556,10 @@ def main():
     bpp = algorithmic_bytes(9, "mixed")
     kt = mixed["kernels"]
     stage_ms = kt["stage_ms"]
-    split = mixed["tuning"]["variant"] in ("split", "split-tma")
+    split = mixed["tuning"]["variant"] in ("split", "split-tma", "split-tma-p")
     stage_achieved = bpp * mixed["npts"] / (stage_ms / 1e3) / 1e9
     if split:  # dominant kernel: the face kernel
-        tma = mixed["tuning"]["variant"] == "split-tma"
+        tma = mixed["tuning"]["variant"] in ("split-tma", "split-tma-p")
         kname = "k_faces_tma<float,9>" if tma else "k_faces<float,9>"
         kbpp, kms = face_kernel_bytes(9, "mixed"), kt["faces_ms"]
         traffic = ncu_traffic("faces_tma_kernel_box128_mixed" if tma else "faces_kernel_box128_mixed")
@@ -571,7 +571,7 @@ def main():
     levels = mixed["info"]["halo_levels"]
     # per stage: stage kernels, halo node levels, halo copies; per step: the
     # third stage's post-exchange dt of rewritten interior points, dt finalize
-    n_stage = {"l1": 1, "tma": 1, "split": 2, "split-tma": 3}[mixed["tuning"]["variant"]]
+    n_stage = {"l1": 1, "tma": 1, "split": 2, "split-tma": 3, "split-tma-p": 3}[mixed["tuning"]["variant"]]
     launches_per_step = 3 * (n_stage + levels + 1) + 2
     line = {
         "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,

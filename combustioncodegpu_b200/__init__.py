@@ -29,7 +29,7 @@ MAX_SPECIES = 16
 CC_FP64, CC_MIXED, CC_FP32 = 0, 1, 2
 CC_RK3, CC_STEADY_EULER, CC_STEADY_LUSGS = 0, 1, 2
 PRECISIONS = {"fp64": CC_FP64, "mixed": CC_MIXED, "fp32": CC_FP32}
-VARIANTS = ("l1", "tma", "split", "split-tma")  # stage-kernel variants, cc_tuning order
+VARIANTS = ("l1", "tma", "split", "split-tma", "split-tma-p")  # stage-kernel variants, cc_tuning order
 SCHEMES = {"rk3": CC_RK3, "steady": CC_STEADY_EULER, "lusgs": CC_STEADY_LUSGS}
 
 _dp = ctypes.POINTER(ctypes.c_double)

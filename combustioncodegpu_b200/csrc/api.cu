@@ -100,7 +100,7 @@ struct cc_ctx {
   uint32_t *d_skip_dt = nullptr;  // bitmask: interior points the halo rewrites
   int renorm = -1;                // Y renormalisation: -1 = by precision (mixed on, FP64 off)
   int variant = 0;                // stage kernels: 0 fused (L1 stencil reads), 1 fused TMA planes, 2 split faces/update,
-                                  // 3 split with TMA-staged face planes
+                                  // 3 split with TMA-staged face planes, 4 the same on persistent CTAs
   std::vector<Tile> hedges;       // split variant: tiles of the minus-side face layers
   std::vector<int> tile_begin, edge_begin;  // per block: first tile / edge tile (lists are block-ordered), + end
   bool per_block = false;         // cc_set_launch_mode: one launch per block per kernel instead of one per stage
@@ -116,6 +116,7 @@ struct cc_ctx {
   int kz = 1;                     // k-chunk of the stage tiles
   double tuned_ms = 0;            // stage-kernel time of the chosen configuration
   CUtensorMap *d_tmaps = nullptr; // [2][n_blocks]: primitive arenas P[0], P[1] per block
+  unsigned *d_ticket = nullptr;   // tile counter of the persistent face kernel
   LusgsArgs lu{};                 // LU-SGS work arrays (allocated by the first LU-SGS step)
   std::vector<int64_t> lu_hb;     // sweep positions where each hyperplane begins, + end
   int n_partials = 296;
@@ -407,6 +408,8 @@ int setup_device(cc_ctx *c) {
   }
   if (dev_alloc(c, &c->G, E * N * 10)) return CC_ERR_CUDA;
   if (dev_alloc(c, &c->faces, E * N * 3 * nv_of(c))) return CC_ERR_CUDA;
+  if (dev_alloc(c, &p, sizeof(unsigned))) return CC_ERR_CUDA;
+  c->d_ticket = (unsigned *)p;
   if (c->precision != CC_FP64) {
     if (dev_alloc(c, &p, sizeof(double) * 3 * N)) return CC_ERR_CUDA;
     c->d_gcl = (double *)p;
@@ -628,13 +631,13 @@ int prof_event(cc_ctx *c, std::vector<cudaEvent_t> &pool, size_t &next) {
   return 0;
 }
 
-const char *const kVariantName[4] = {"fused-l1", "fused-tma", "split", "split-tma"};
+const char *const kVariantName[5] = {"fused-l1", "fused-tma", "split", "split-tma", "split-tma-persistent"};
 
 // Variants this context can run: the TMA-staged ones need the tensor maps
 // (0 or 9 species); the fused TMA kernel's planes and flux planes fit in
 // shared memory in the FP32 bulk precision only.
 bool variant_ok(const cc_ctx *c, int v) {
-  if (v == 3) return c->tma_ok;
+  if (v == 3 || v == 4) return c->tma_ok;
   if (v == 1) return c->tma_ok && c->precision != CC_FP64;
   return v == 0 || v == 2;
 }
@@ -661,17 +664,21 @@ int launch_stage(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt) {
 
 template <typename T, int NS>
 int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge) {
-  if ((variant == 1 || variant == 3) && !c->d_tmaps)
+  if ((variant == 1 || variant == 3 || variant == 4) && !c->d_tmaps)
     return fail(CC_ERR_STATE, "TMA variant without tensor maps");
   if (variant == 1) {
     CK((Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
-  } else if (variant == 2 || variant == 3) {
+  } else if (variant == 2 || variant == 3 || variant == 4) {
     a.faces = (T *)c->faces;
     if (!a.edge_tiles) a.edge_tiles = c->d_edges;
     if (variant == 2) {
       CK((Launch<T, NS>::faces(a, c->chem, nt, n_edge, c->stream)));
-    } else {  // regular tiles from TMA-staged planes, edge tiles through L1
-      CK((Launch<T, NS>::faces_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
+    } else {  // regular tiles from TMA-staged planes (persistent CTAs for 4), edge tiles through L1
+      if (variant == 3)
+        CK((Launch<T, NS>::faces_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
+      else
+        CK((Launch<T, NS>::faces_tma_persistent(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt,
+                                                c->d_ticket, c->stream)));
       CK((Launch<T, NS>::faces(a, c->chem, 0, n_edge, c->stream)));
     }
     if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
@@ -852,7 +859,7 @@ int autotune(cc_ctx *c) {
   if (c->force_variant >= 0)
     variants.push_back(c->force_variant);
   else
-    for (int v : {0, 1, 2, 3})
+    for (int v : {0, 1, 2, 3, 4})
       if (variant_ok(c, v)) variants.push_back(v);
   for (int variant : variants) {
     for (int kz : kzs) {
@@ -1397,9 +1404,10 @@ int cc_tuning(cc_ctx *c, int *variant, int *kz, double *stage_ms) {
 
 int cc_set_tuning(cc_ctx *c, int variant, int kz) {
   if (int r = check_ctx(c)) return r;
-  if (variant < -1 || variant > 3)
+  if (variant < -1 || variant > 4)
     return fail(CC_ERR_ARG,
-                "variant must be -1 (autotune), 0 (fused, L1), 1 (fused, TMA), 2 (split) or 3 (split, TMA faces)");
+                "variant must be -1 (autotune), 0 (fused, L1), 1 (fused, TMA), 2 (split), 3 (split, TMA faces) or 4 "
+                "(split, TMA faces on persistent CTAs)");
   if (kz < 0) return fail(CC_ERR_ARG, "kz must be >= 0");
   c->force_variant = variant;
   c->force_kz = kz;

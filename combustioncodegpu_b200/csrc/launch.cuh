@@ -56,6 +56,28 @@ cudaError_t Launch<T, NS>::faces_tma(const StageArgs<T> &a, const void *maps, co
 }
 
 template <typename T, int NS>
+cudaError_t Launch<T, NS>::faces_tma_persistent(const StageArgs<T> &a, const void *maps, const ChemParams &C,
+                                                int n_tiles, unsigned *ticket, cudaStream_t s) {
+  if (n_tiles <= 0) return cudaSuccess;
+  if (faces_tma_smem() > 227 * 1024) return cudaErrorInvalidConfiguration;
+  static int per_sm = 0, n_sm = 0;
+  if (per_sm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_faces_tma_persistent<T, NS>, kTX * kTY,
+                                                  faces_tma_smem());
+    per_sm = std::max(1, per_sm);
+  }
+  cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  const int grid = std::min(n_tiles, n_sm * per_sm);
+  k_faces_tma_persistent<T, NS><<<grid, dim3(kTX, kTY), faces_tma_smem(), s>>>(a, (const CUtensorMap *)maps, C,
+                                                                              n_tiles, ticket);
+  return cudaGetLastError();
+}
+
+template <typename T, int NS>
 cudaError_t Launch<T, NS>::update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;
   k_update<T, NS><<<n_tiles, dim3(kTX, kTY), update_smem(), s>>>(a, C);
@@ -97,6 +119,9 @@ cudaError_t Launch<T, NS>::configure() {
     e = cudaFuncSetAttribute(k_stage_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_tma_smem());
   if (e == cudaSuccess && faces_tma_smem() <= 227 * 1024)
     e = cudaFuncSetAttribute(k_faces_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)faces_tma_smem());
+  if (e == cudaSuccess && faces_tma_smem() <= 227 * 1024)
+    e = cudaFuncSetAttribute(k_faces_tma_persistent<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)faces_tma_smem());
   return e;
 }
 

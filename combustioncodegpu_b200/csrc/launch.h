@@ -26,6 +26,9 @@ struct Launch {
   static size_t faces_tma_smem();
   static cudaError_t faces_tma(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
                                cudaStream_t s);
+  // persistent form: resident CTAs take the n_tiles regular tiles from *ticket (zeroed here)
+  static cudaError_t faces_tma_persistent(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
+                                          unsigned *ticket, cudaStream_t s);
   // learned transport closure (closure.cuh) over every arena point; cl is a ClosureDev
   static cudaError_t props_mlp(const T *P, T *Pr, int64_t N, const void *cl, unsigned *status, const ChemParams &C,
                                cudaStream_t s);

@@ -329,22 +329,23 @@ struct FacesTmaLayout {
   static constexpr size_t kBytes = 128 + 128 + kRing * kPlaneBytes + kRec;
 };
 
+// One regular tile of the face kernel: fill the ring with planes k0-1 ..
+// k0+2, then per plane k wait for k-1 .. k+2, compute the +z, +x, +y faces
+// of the tile's points and request plane k+3 into the slot of k-1.  pc0 is
+// the number of planes this CTA loaded before the tile: plane kp is the
+// CTA's (pc0 + kp - k0 + 1)-th load, in slot (that count mod 4) with the
+// slot's barrier at parity (count / 4) mod 2.  The mbarriers are initialised
+// by the caller.  Returns the planes loaded; *aborted is set (uniformly) when
+// a wait timed out, after the copies in flight have landed.
 template <typename T, int NS>
-__global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
-    k_faces_tma(const StageArgs<T> a, const CUtensorMap *__restrict__ maps, const __grid_constant__ ChemParams C) {
+__device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUtensorMap *map, const ChemParams &C,
+                                              uint64_t *bars, unsigned char *ring, const T *sRec, const Tile &t,
+                                              unsigned pc0, bool &aborted) {
   using L = FacesTmaLayout<T, NS>;
   constexpr int NV = 5 + SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   const int nv = 5 + ns;
-  extern __shared__ __align__(128) unsigned char smem_dyn[];
-  unsigned char *smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
-  unsigned char *ring = smem_raw + 128;
-  T *sRec = reinterpret_cast<T *>(ring + L::kRing * L::kPlaneBytes);
-
-  const Tile t = a.tiles[blockIdx.x];
   const BlockInfo B = a.blocks[t.blk];
-  const CUtensorMap *map = maps + t.blk;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
   const int i = t.i0 + tx, j = t.j0 + ty;
   const bool act = (i < B.mx) && (j < B.my);
@@ -355,30 +356,25 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   // tensor coordinates of plane kp: x = i0 - 2 + g, y = j0 - 2 + g, z = kp + g
   const int tx0 = t.i0 - 2 + B.g, ty0 = t.j0 - 2 + B.g;
   const int kfirst = t.k0 - 1, klast = t.k1 + 1;  // planes the sweep reads
-
-  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * kTY) sRec[e] = param_rec<T>(C)[e];
+  auto slot_of = [&](int kp) { return (int)((pc0 + (unsigned)(kp - kfirst)) & (L::kRing - 1)); };
+  auto parity_of = [&](int kp) { return ((pc0 + (unsigned)(kp - kfirst)) / L::kRing) & 1u; };
+  const int k_pro = min(klast, kfirst + L::kRing - 1);
   if (tid == 0) {
-    for (int b = 0; b < L::kRing; ++b) mbar_init(&bars[b], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
                  : "memory");
-  }
-  __syncthreads();
-  // plane kp lives in slot (kp - kfirst) % 4 as that slot's n-th load, n = (kp - kfirst) / 4
-  auto slot_of = [&](int kp) { return (kp - kfirst) & (L::kRing - 1); };
-  auto parity_of = [&](int kp) { return (unsigned)(((kp - kfirst) / L::kRing) & 1); };
-  const int k_pro = min(klast, kfirst + L::kRing - 1);
-  if (tid == 0)
+    // a previous tile's threads read these slots through the generic proxy
+    if (pc0 != 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     for (int kp = kfirst; kp <= k_pro; ++kp) {
       const int sl = slot_of(kp);
       mbar_arrive_expect_tx(&bars[sl], plane_bytes);
       tma_load_plane(ring + sl * L::kPlaneBytes, map, tx0, ty0, kp + B.g, &bars[sl]);
     }
+  }
   int k_issued = k_pro;
 
   const int q = (ty + 2) * kHX + (tx + 2);  // in-plane index of this thread's point
   T F[NV];
-  bool aborted = false;
+  aborted = false;
   for (int k = t.k0; k < t.k1; ++k) {
     bool late = false;
     for (int kp = k - 1; kp <= k + 2; ++kp) {
@@ -423,7 +419,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
     }
   }
   if (aborted) {
-    // let this CTA's copies in flight land before it exits (bounded)
+    // let this CTA's copies in flight land before it leaves (bounded)
     if (tid == 0)
       for (int kp = max(kfirst, k_issued - L::kRing + 1); kp <= k_issued; ++kp) {
         long spins = 0;
@@ -431,6 +427,64 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
         }
       }
     __syncthreads();
+  }
+  return klast - kfirst + 1;
+}
+
+template <typename T, int NS>
+__global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
+    k_faces_tma(const StageArgs<T> a, const CUtensorMap *__restrict__ maps, const __grid_constant__ ChemParams C) {
+  using L = FacesTmaLayout<T, NS>;
+  const int ns = SpecCount<NS>::n(C);
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char *smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  unsigned char *ring = smem_raw + 128;
+  T *sRec = reinterpret_cast<T *>(ring + L::kRing * L::kPlaneBytes);
+  const int tid = threadIdx.y * kTX + threadIdx.x;
+  const Tile t = a.tiles[blockIdx.x];
+  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * kTY) sRec[e] = param_rec<T>(C)[e];
+  if (tid == 0) {
+    for (int b = 0; b < L::kRing; ++b) mbar_init(&bars[b], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  bool aborted;
+  faces_tma_tile<T, NS>(a, maps + t.blk, C, bars, ring, sRec, t, 0u, aborted);
+}
+
+// Persistent form of k_faces_tma: as many CTAs as fit on the GPU take the
+// regular tiles in order from a device counter (zeroed before the launch),
+// initialising the NASA records and the mbarriers once; the plane count
+// carries the mbarrier phases from one tile to the next.
+template <typename T, int NS>
+__global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
+    k_faces_tma_persistent(const StageArgs<T> a, const CUtensorMap *__restrict__ maps,
+                           const __grid_constant__ ChemParams C, int n_tiles, unsigned *ticket) {
+  using L = FacesTmaLayout<T, NS>;
+  const int ns = SpecCount<NS>::n(C);
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char *smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  unsigned char *ring = smem_raw + 128;
+  T *sRec = reinterpret_cast<T *>(ring + L::kRing * L::kPlaneBytes);
+  __shared__ int sh_tile;
+  const int tid = threadIdx.y * kTX + threadIdx.x;
+  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * kTY) sRec[e] = param_rec<T>(C)[e];
+  if (tid == 0) {
+    for (int b = 0; b < L::kRing; ++b) mbar_init(&bars[b], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  unsigned pc = 0;
+  for (;;) {
+    if (tid == 0) sh_tile = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int ti = sh_tile;
+    __syncthreads();  // every thread has its tile index before the next ticket
+    if (ti >= n_tiles) break;
+    bool aborted;
+    pc += (unsigned)faces_tma_tile<T, NS>(a, maps + a.tiles[ti].blk, C, bars, ring, sRec, a.tiles[ti], pc, aborted);
+    if (aborted) break;
   }
 }
 

@@ -182,7 +182,8 @@ int cc_time_kernels(cc_ctx *ctx, int n_steps, int scheme, double out_ms[6]);
  * first cc_init, or pinned by cc_set_tuning) and its measured time per
  * stage: variant 0 = fused stage kernel with L1 stencil reads, 1 = fused
  * with TMA-staged primitive planes, 2 = split (face kernel, then update
- * kernel), 3 = split with TMA-staged planes in the face kernel; kz =
+ * kernel), 3 = split with TMA-staged planes in the face kernel, 4 = as 3
+ * with the face kernel on persistent CTAs taking tiles from a counter; kz =
  * k-planes per tile.  CC_AUTOTUNE=0 keeps the heuristic. */
 int cc_tuning(cc_ctx *ctx, int *variant, int *kz, double *stage_ms);
 /* No counterpart in the reference (its launch shapes are fixed).  Pins the

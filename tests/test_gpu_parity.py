@@ -103,7 +103,7 @@ def test_mixed_close_to_oracle(name, scheme):
 # Every stage-kernel variant on every case, with k-chunks that split the
 # sweep (kz=3) and that do not (kz=64).  The TMA variants exist for 0 or 9
 # species; the fused one for the FP32 bulk precision only.
-@pytest.mark.parametrize("variant", ["tma", "split-tma"])
+@pytest.mark.parametrize("variant", ["tma", "split-tma", "split-tma-p"])
 @pytest.mark.parametrize("kz", [3, 64])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_tma_variant_close_to_oracle(name, kz, variant):
@@ -114,7 +114,7 @@ def test_tma_variant_close_to_oracle(name, kz, variant):
     assert not bad, errs
 
 
-@pytest.mark.parametrize("variant", ["split", "split-tma"])
+@pytest.mark.parametrize("variant", ["split", "split-tma", "split-tma-p"])
 @pytest.mark.parametrize("scheme", ["steady", "rk3"])
 @pytest.mark.parametrize("kz", [3, 64])
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -134,7 +134,7 @@ def test_split_variant_mixed_close_to_oracle(name):
     assert not bad, errs
 
 
-@pytest.mark.parametrize("variant", ["l1", "split", "split-tma"])
+@pytest.mark.parametrize("variant", ["l1", "split", "split-tma", "split-tma-p"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_k_chunking_is_bit_identical(precision, variant):
     """A face at a k-chunk boundary is computed by both chunks through the
@@ -160,7 +160,7 @@ def test_variants_agree_at_64(precision):
     split-variant edge tiles span several CTAs per face layer) after two
     RK3 steps: FP64 to 1e-13, mixed to 1e-6 relative per field."""
     case = cases.case_box(64, species=cases.synthetic_species(), seed=5)
-    variants = ["l1", "split", "split-tma"] + (["tma"] if precision == "mixed" else [])
+    variants = ["l1", "split", "split-tma", "split-tma-p"] + (["tma"] if precision == "mixed" else [])
     out = {}
     for v in variants:
         d = cc.Driver.from_case(case, precision)
@@ -403,7 +403,7 @@ def test_tma_variants_refused_without_tensor_maps():
     """Tensor maps exist for 0 or 9 species only: pinning a TMA variant on a
     context with another species count fails at cc_init."""
     case = cases.case_box(8, species=SP4, seed=2)
-    for variant in ("tma", "split-tma"):
+    for variant in ("tma", "split-tma", "split-tma-p"):
         d = cc.Driver.from_case(case, "mixed")
         d.set_tuning(variant, 4)
         with pytest.raises(RuntimeError, match="TMA variants"):
