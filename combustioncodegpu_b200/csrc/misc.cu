@@ -115,8 +115,17 @@ __global__ void k_store_last(const BlockInfo *blocks, int nblocks, const T *P, c
   last[3 * n_int + g] = P[5 * N + p];
 }
 
-// compute_square_of_dbv + per-CTA sums (fixed order), then one CTA sums the
-// partials in fixed order: the result does not depend on scheduling.
+// Sum over a warp by shuffles in a fixed tree (the result does not depend on
+// scheduling); lane 0 holds the sum.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// compute_square_of_dbv + per-CTA sums (warp shuffles, then the warps' sums
+// by the first warp, fixed order), then one warp sums the partials: the
+// result does not depend on scheduling.
 template <typename T>
 __global__ void k_residual_partial(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
                                    int64_t n_int, const double *last, double *partials) {
@@ -129,24 +138,33 @@ __global__ void k_residual_partial(const BlockInfo *blocks, int nblocks, const T
     const double d3 = (double)P[5 * N + p] - last[3 * n_int + g];
     acc[0] += d0 * d0, acc[1] += d1 * d1, acc[2] += d2 * d2, acc[3] += d3 * d3;
   }
-  __shared__ double sh[4][256];
-  for (int l = 0; l < 4; ++l) sh[l][threadIdx.x] = acc[l];
-  __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if ((int)threadIdx.x < st)
-      for (int l = 0; l < 4; ++l) sh[l][threadIdx.x] += sh[l][threadIdx.x + st];
-    __syncthreads();
+  __shared__ double sh[4][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    const double w = warp_sum(acc[l]);
+    if (lane == 0) sh[l][warp] = w;
   }
-  if (threadIdx.x == 0)
-    for (int l = 0; l < 4; ++l) partials[4 * blockIdx.x + l] = sh[l][0];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const double w = warp_sum(lane < n_warps ? sh[l][lane] : 0.0);
+      if (lane == 0) partials[4 * blockIdx.x + l] = w;
+    }
+  }
 }
 
 __global__ void k_residual_final(const double *partials, int n_partials, int64_t n_int, double *res) {
-  if (threadIdx.x != 0) return;
+  const int lane = threadIdx.x & 31;
   double r[4] = {0, 0, 0, 0};
-  for (int b = 0; b < n_partials; ++b)
+  for (int b = lane; b < n_partials; b += 32)  // each lane in fixed order, then a fixed tree
     for (int l = 0; l < 4; ++l) r[l] += partials[4 * b + l];
-  for (int l = 0; l < 4; ++l) res[l] = sqrt(r[l] / (double)n_int);
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    const double w = warp_sum(r[l]);
+    if (lane == 0) res[l] = sqrt(w / (double)n_int);
+  }
 }
 
 template <typename T>
