@@ -372,6 +372,42 @@ def test_lusgs_graph_replay_equals_launches():
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("name", ["box", "channel", "sod"])
+def test_lusgs_fp32_close_to_oracle(name):
+    """LU-SGS in the full-FP32 precision (conserved state rounded to FP32):
+    at the FP32 level of the RK3 test."""
+    errs, status = compare(_with_cfl(CASES[name], 5.0), "lusgs", 3, "fp32")
+    assert status == 0
+    tol = {"res": 5e-2, "dt": 1e-4}
+    bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-3)}
+    assert not bad, errs
+
+
+def test_lusgs_with_learned_closure():
+    """LU-SGS steps with the transport of each new state from the learned
+    closure: after five CFL-5 steps (ten times the time an RK3 step at CFL
+    0.5 advances) the state stays within a few times the closure's ~1e-3
+    transport error of the steps with the exact transport."""
+    from combustioncodegpu_b200 import closure
+
+    w, _ = closure.load()
+    case = _with_cfl(cases.case_box(16, species=cases.synthetic_species(), seed=4), 5.0)
+    out = {}
+    for mode in ("exact", "closure"):
+        d = cc.Driver.from_case(case, "mixed")
+        if mode == "closure":
+            d.set_closure(w)
+            d.use_closure(True)
+        d.initialize_computation()
+        d.simulate(5, "lusgs")
+        assert d.status() == 0
+        out[mode] = d.field[0].get_state()[0]
+        d.close()
+    for f in (0, 4, 5):  # rho, p, T
+        rel = np.abs(out["closure"][f] - out["exact"][f]).max() / np.abs(out["exact"][f]).max()
+        assert rel < 5e-3, (f, rel)
+
+
 # A species count without a compiled specialisation (4: H2, O2, H2O, N2) runs
 # the kernels' runtime-count path.
 SP4 = cases.synthetic_species([cases.H2O2_N2_SPECIES[i] for i in (0, 1, 2, 8)])
