@@ -229,6 +229,8 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
   const T *__restrict__ G = a.G;
   const double dtj = dt / (double)G[p];
   double q[NV];
+  // all loads first, then the stores: Qout may alias Qin, so a store between
+  // two loads would keep the compiler from issuing the loads together
 #pragma unroll
   for (int l = 0; l < NV; ++l) {
     if (l < nv) {
@@ -239,9 +241,11 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
       if (l == 3 && !three_d) qs = 0;
       q[l] = (a.a != 0.0) ? a.a * a.Qn[l * N + p] + a.b * qs : qs;
       if (a.q32) q[l] = (double)(float)q[l];  // full-FP32 study: FP32 conserved state
-      a.Qout[l * N + p] = q[l];
     }
   }
+#pragma unroll
+  for (int l = 0; l < NV; ++l)
+    if (l < nv) a.Qout[l * N + p] = q[l];
   // primitives (TimeAdvanceFunc.cu:266-289), FP64
   const double rho = q[0];
   const double inv = 1.0 / rho;
