@@ -113,6 +113,19 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2) k_lusgs_rhs(
   for (int k = t.k0; k < t.k1; ++k) {
     const int p = col + sk * k;
     const int64_t sp = act ? (int64_t)L.pos[p] : -1;
+    // the point's primitives, viscosity and geometry, read together with the
+    // faces below: read after the row stores they would wait for a second
+    // round trip, since the compiler cannot move loads above stores that may
+    // alias them
+    T pv[6 + A], mu_t = T(0), gv[10];
+#pragma unroll
+    for (int f = 0; f < 6 + A; ++f) pv[f] = (act && f < 6 + ns) ? P[f * N + p] : T(0);
+#pragma unroll
+    for (int r = 0; r < 10; ++r) gv[r] = act ? G[r * N + p] : T(0);
+    if (act) mu_t = a.Pr[p];
+    double qc[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) qc[f] = act ? a.Qin[f * N + p] : 0.0;
     if (NV > 16) {  // runtime species count beyond 11: plain stores of the wider rows
       if (act) {
 #pragma unroll
@@ -158,30 +171,32 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2) k_lusgs_rhs(
 #pragma unroll
     for (int l = 0; l < 16; ++l) psi[l] = 0.0;
     if (act) {
-      const double inv = 1.0 / a.Qin[p];
+      const double inv = 1.0 / qc[0];
       row[kLuInv] = inv;
-      row[kLuU] = a.Qin[N + p] * inv;
-      row[kLuU + 1] = a.Qin[2 * N + p] * inv;
-      row[kLuU + 2] = a.Qin[3 * N + p] * inv;
-      row[kLuP] = (double)P[4 * N + p] + C.p_ref;
+      row[kLuU] = qc[1] * inv;
+      row[kLuU + 1] = qc[2] * inv;
+      row[kLuU + 2] = qc[3] * inv;
+      row[kLuP] = (double)pv[4] + C.p_ref;
       T Y[A];
 #pragma unroll
       for (int l = 0; l < A; ++l)
-        if (l < ns) Y[l] = P[(6 + l) * N + p];
+        if (l < ns) Y[l] = pv[6 + l];
       T gam, c;
-      gamma_and_c<T, NS>(C, rec, P[5 * N + p], Y, gam, c);
-      const double rho = (double)P[p], u = (double)P[N + p], v = (double)P[2 * N + p], w = (double)P[3 * N + p];
-      const double mu = (double)a.Pr[p];
-      const double dt = local_time_step<T>(C, G, N, p, rho, u, v, w, (double)c, (double)gam, mu, three_d);
-      const double J = (double)G[p];
+      gamma_and_c<T, NS>(C, rec, pv[5], Y, gam, c);
+      const double rho = (double)pv[0], u = (double)pv[1], v = (double)pv[2], w = (double)pv[3];
+      const double mu = (double)mu_t;
+      double mt[9];
+#pragma unroll
+      for (int r = 0; r < 9; ++r) mt[r] = (double)gv[1 + r];
+      const double dt = local_time_step_m(C, mt, rho, u, v, w, (double)c, (double)gam, mu, three_d);
+      const double J = (double)gv[0];
       const double c1 = fmax((double)gam, 4.0 / 3.0);
       const double c2 = mu / rho / C.Pr;
       double D = J / dt;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         double r = 0;
-        const double m0 = (double)G[(1 + 3 * d) * N + p], m1 = (double)G[(2 + 3 * d) * N + p],
-                     m2 = (double)G[(3 + 3 * d) * N + p];
+        const double m0 = mt[3 * d], m1 = mt[3 * d + 1], m2 = mt[3 * d + 2];
         if (d < 2 || three_d) {
           const double g = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
           const double U = u * m0 + v * m1 + w * m2;
@@ -203,7 +218,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2) k_lusgs_rhs(
         if (id[d] == 0)  // no lower neighbour: nothing arrives in this row during the lower sweep
           for (int l = 0; l < lp; ++l) L.Cn[(d * S + sp) * lp + l] = 0.0;
       if (ns > 0) {
-        const double td = (double)P[5 * N + p], g1 = (double)gam - 1.0;
+        const double td = (double)pv[5], g1 = (double)gam - 1.0;
 #pragma unroll
         for (int l = 0; l < A; ++l) {
           if (l < ns) {

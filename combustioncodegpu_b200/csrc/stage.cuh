@@ -28,14 +28,11 @@ __device__ __forceinline__ void atomic_min_pos_double(unsigned long long *dst, d
   atomicMin(dst, (unsigned long long)__double_as_longlong(v));
 }
 
-// TemporalScheme.cu:11-43: CFL / (inviscid + viscous spectral radius).
-template <typename T>
-__device__ __forceinline__ double local_time_step(const ChemParams &C, const T *G, int64_t N, int64_t p, double rho,
-                                                  double u, double v, double w, double c, double gamma, double mu,
-                                                  bool three_d) {
-  double m[9];
-#pragma unroll
-  for (int r = 0; r < 9; ++r) m[r] = (double)G[(1 + r) * N + p];
+// TemporalScheme.cu:11-43: CFL / (inviscid + viscous spectral radius), from
+// the point's metrics m[3 d + c] = d xi_d / d x_c.
+__device__ __forceinline__ double local_time_step_m(const ChemParams &C, const double (&m)[9], double rho, double u,
+                                                    double v, double w, double c, double gamma, double mu,
+                                                    bool three_d) {
   const double gxi = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
   const double get = sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
   const double gze = sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
@@ -50,6 +47,17 @@ __device__ __forceinline__ double local_time_step(const ChemParams &C, const T *
   if (three_d) srv += gze * gze;
   srv *= c1 * c2;
   return C.cfl / (sri + srv);
+}
+
+// The same with the metrics read from the geometry arena G.
+template <typename T>
+__device__ __forceinline__ double local_time_step(const ChemParams &C, const T *G, int64_t N, int64_t p, double rho,
+                                                  double u, double v, double w, double c, double gamma, double mu,
+                                                  bool three_d) {
+  double m[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) m[r] = (double)G[(1 + r) * N + p];
+  return local_time_step_m(C, m, rho, u, v, w, c, gamma, mu, three_d);
 }
 
 // Stencil access of the primitives around one face (point p0 and its
