@@ -337,6 +337,24 @@ struct FacesTmaLayout {
 // slot's barrier at parity (count / 4) mod 2.  The mbarriers are initialised
 // by the caller.  Returns the planes loaded; *aborted is set (uniformly) when
 // a wait timed out, after the copies in flight have landed.
+// While plane k is processed, bring into L2 the transport and geometry rows
+// of plane kp = k + 2 (1-point halo in j, the tile's i span plus one point
+// on each side), which the faces of plane k + 1 read for the first time
+// through L1.  Rows are spread over the CTA's threads; a hint nothing waits on.
+template <typename T>
+__device__ __forceinline__ void prefetch_props_geometry(const StageArgs<T> &a, const BlockInfo &B, const Tile &t,
+                                                        int kp, int npr, int tid) {
+  const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
+  const int j_lo = max(t.j0 - 1, -B.g), j_hi = min(t.j0 + kTY + 1, B.my + B.g), nr = j_hi - j_lo;
+  const int n = (npr + 10) * nr;
+  for (int e = tid; e < n; e += kTX * kTY) {
+    const int f = e / nr, j = j_lo + e % nr;
+    const T *base = f < npr ? a.Pr + (size_t)f * N : a.G + (size_t)(f - npr) * N;
+    const int row = (int)B.base + sk * kp + sj * j;
+    l2_prefetch(base, N, row + t.i0 - 1, row + t.i0 + kTX + 1);
+  }
+}
+
 template <typename T, int NS>
 __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUtensorMap *map, const ChemParams &C,
                                               uint64_t *bars, unsigned char *ring, const T *sRec, const Tile &t,
@@ -395,6 +413,9 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
     const T *pl1 = reinterpret_cast<const T *>(ring + slot_of(k + 1) * L::kPlaneBytes);
     const T *pl2 = reinterpret_cast<const T *>(ring + slot_of(k + 2) * L::kPlaneBytes);
     const int p = col + sk * k;
+    // (FP64 only: measured faster there, slower in FP32, whose smaller rows
+    // stay in L2 without it)
+    if (sizeof(T) == 8 && k + 2 <= B.mz - 1 + B.g) prefetch_props_geometry<T>(a, B, t, k + 2, 2 + ns, tid);
     if (act) {
 #pragma unroll 1
       for (int it = three_d ? 0 : 1; it < 3; ++it) {
