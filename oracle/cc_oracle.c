@@ -1,7 +1,8 @@
 /*
  * cc_oracle.c -- CPU FP64 restatement of CombustionCodeGPU's per-timestep
- * residual path.  TEST INFRASTRUCTURE ONLY (the checker and the timed CPU
- * baseline); the CUDA product never links or calls it.
+ * residual path.  TEST INFRASTRUCTURE ONLY (what the tests compare the CUDA
+ * results against, and the timed CPU baseline); the CUDA product never links
+ * or calls it.
  *
  * Each routine names the reference file:line it follows.  The arithmetic is
  * written in the reference's evaluation order so that the restatement agrees

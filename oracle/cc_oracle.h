@@ -1,7 +1,7 @@
 /*
  * cc_oracle.h -- CPU FP64 restatement of CombustionCodeGPU's per-timestep
- * residual path.  TEST INFRASTRUCTURE ONLY: this is the checker that the
- * CUDA product is compared against, and the timed CPU baseline.  Nothing in
+ * residual path.  TEST INFRASTRUCTURE ONLY: this is what the tests compare
+ * the CUDA product against, and the timed CPU baseline.  Nothing in
  * the product links, loads or calls it.
  *
  * Every function in cc_oracle.c cites the reference file:line it restates.

@@ -1,5 +1,5 @@
 """CPU restatement (numpy, FP64 arithmetic) of the closure MLP's training
-math -- TEST INFRASTRUCTURE ONLY, the checker of the training kernels
+math -- TEST INFRASTRUCTURE ONLY, what the training kernels are tested against
 (combustioncodegpu_b200/csrc/closure_train.cu); the product never calls it.
 
 Network: n_in -> H -> H -> H -> n_out, SiLU on the hidden layers.

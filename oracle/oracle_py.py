@@ -1,7 +1,7 @@
 """ctypes driver of the CPU FP64 oracle (cc_oracle.c).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
-the checker, and by bench.py for the CPU baseline.  The product never uses it.
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() to
+check its CUDA result, and by bench.py for the CPU baseline.  The product never uses it.
 """
 import ctypes
 import os

@@ -155,7 +155,7 @@ def test_renormalised_mass_fractions_sum_to_one(species):
 
 
 def test_closure_mlp_oracle_gradient_by_finite_difference():
-    """The oracle's backward pass (the checker of the training kernels),
+    """The oracle's backward pass (what the training kernels are tested against),
     without its BF16 rounding: central differences of the loss."""
     from oracle import closure_mlp as om
 
