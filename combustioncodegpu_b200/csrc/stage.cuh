@@ -236,6 +236,9 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
   const int nv = 5 + ns;
   const T *__restrict__ G = a.G;
   const double dtj = dt / (double)G[p];
+  // whether this point's step enters the next global time step, read with
+  // the state rather than behind the stores below
+  const bool want_dt = a.dt_next && !((a.skip_dt[p >> 5] >> (p & 31)) & 1u);
   double q[NV];
   // all loads first, then the stores: Qout may alias Qin, so a store between
   // two loads would keep the compiler from issuing the loads together
@@ -335,7 +338,7 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
 #pragma unroll
   for (int l = 0; l < A; ++l)
     if (l < ns) Prn[(2 + l) * N + p] = rd[l];
-  if (a.dt_next && !((a.skip_dt[p >> 5] >> (p & 31)) & 1u)) {
+  if (want_dt) {
     const double dtl = local_time_step<T>(C, G, N, p, rho, u, v, w, (double)c, (double)gam, (double)mu, three_d);
     dt_min = fmin(dt_min, dtl);
   }
