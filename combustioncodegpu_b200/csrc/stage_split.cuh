@@ -113,6 +113,9 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 2 : 3)
   double dt_min = 1e300;
   if (act) {
     const int col = (int)B.base + i + sj * j;
+    // the global step, read once (inside the loop it would follow the
+    // previous point's stores)
+    const double dt_global = a.local_dt ? 0.0 : *a.dt;
     for (int k = t.k0; k < t.k1; ++k) {
       const int p = col + sk * k;
       // dq = -(sum over directions of F(+1/2) - F(-1/2)), the fused kernel's order
@@ -138,7 +141,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 2 : 3)
         dt = local_time_step<T>(C, a.G, N, p, (double)P[p], (double)P[N + p], (double)P[2 * N + p],
                                 (double)P[3 * N + p], (double)c, (double)gam, (double)a.Pr[p], three_d);
       } else {
-        dt = *a.dt;
+        dt = dt_global;
       }
       point_update<T, NS>(C, sRec, sRecD, a, p, N, dq, dt, (double)P[5 * N + p], three_d, flags, dt_min);
     }
