@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--variant", default="auto", choices=["auto", "l1", "tma", "split", "split-tma", "split-tma-p"],
                     help="stage kernels: autotuned (default) or pinned (profiling runs, where the autotuner's "
                          "timings are distorted)")
+    ap.add_argument("--kz", type=int, default=4, help="k-planes per tile when --variant pins the stage kernels")
     return ap.parse_args()
 
 
@@ -189,7 +190,7 @@ def run_ours(args, rank, world, dist):
     for prec in ("fp64", "mixed"):
         d = cc.Driver.from_case(case, prec)
         if args.variant != "auto":  # the fused TMA variant exists in the FP32 bulk precision only
-            d.set_tuning("l1" if prec == "fp64" and args.variant == "tma" else args.variant, 4)
+            d.set_tuning("l1" if prec == "fp64" and args.variant == "tma" else args.variant, args.kz)
         d.initialize_computation()
         s = torch.cuda.ExternalStream(d.stream())
         info = d.info()
@@ -244,7 +245,7 @@ def run_ours(args, rank, world, dist):
         bv_h, yk_h = pin(blk["bv"]), pin(blk["yk"])
         d = cc.Driver.from_case(case, "mixed")
         if args.variant != "auto":
-            d.set_tuning(args.variant, 4)
+            d.set_tuning(args.variant, args.kz)
         d.initialize_computation()
         d.simulate(2)
         d.sync()
