@@ -112,6 +112,10 @@ EXPORTS = {
     "cc_save_checkpoint": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
     "cc_load_checkpoint": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
     "cc_sync": ([ctypes.c_void_p], ctypes.c_int),
+    "cc_halo_dependencies": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                              ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+    "cc_block_arena": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
+                        ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "cc_mlp_param_count": ([ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int64),
     "cc_mlp_workspace_bytes": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int64),
     "cc_mlp_grad": ([ctypes.c_int] * 4 + [ctypes.c_void_p] * 8, ctypes.c_int),
@@ -424,6 +428,25 @@ class Driver:
         """"batched": one launch per stage kernel over all blocks;
         "per_block": one launch per block per kernel (the reference's way)."""
         _check(self.lib.cc_set_launch_mode(self.ctx, {"batched": 0, "per_block": 1}[mode]))
+
+    def halo_dependencies(self):
+        """(dst, src, which) int64/int64/int32 arrays: arena point src of the
+        current (which 0) or previous (1) state that the halo program's final
+        value of point dst is computed from (cc_halo_dependencies; host only)."""
+        n = ctypes.c_int64(0)
+        _check(self.lib.cc_halo_dependencies(self.ctx, None, None, None, 0, ctypes.byref(n)))
+        dst = np.empty(n.value, dtype=np.int64)
+        src = np.empty(n.value, dtype=np.int64)
+        which = np.empty(n.value, dtype=np.int32)
+        _check(self.lib.cc_halo_dependencies(self.ctx, dst.ctypes.data, src.ctypes.data, which.ctypes.data,
+                                             n.value, ctypes.byref(n)))
+        return dst, src, which
+
+    def block_arena(self, block):
+        """(first, count): the arena points of a block's ghosted box (cc_block_arena)."""
+        first, count = ctypes.c_int64(0), ctypes.c_int64(0)
+        _check(self.lib.cc_block_arena(self.ctx, int(block), ctypes.byref(first), ctypes.byref(count)))
+        return first.value, count.value
 
     def save_checkpoint(self, path):
         """The current state, bit for bit (cc_save_checkpoint)."""

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -358,16 +359,15 @@ int build_tensor_maps(cc_ctx *c) {
   return 0;
 }
 
-// Layout, device allocation, halo program, geometry.  Runs once.
-int setup_device(cc_ctx *c) {
-  const int ns = c->chem.ns;
-  c->elem = c->precision == CC_FP64 ? 8 : 4;
-  c->ns_key = ns == 0 ? 0 : (ns == 9 ? 9 : -1);
-  // arena layout: rows padded to 32 points, every block starts on a 32-point boundary
-  int64_t end = 0, n_int = 0;
-  c->hblocks.clear();
-  for (auto &b : c->blocks) {
-    b.g = c->ngg;
+// Arena layout: rows padded to 32 points, every block starting on a
+// 32-point boundary.  Fills each block's extents and offsets and its
+// BlockInfo; returns the arena size (a multiple of 32 points).
+int64_t layout_blocks(std::vector<HostBlock> &blocks, int ngg, std::vector<BlockInfo> &info, int64_t &n_int) {
+  int64_t end = 0;
+  n_int = 0;
+  info.clear();
+  for (auto &b : blocks) {
+    b.g = ngg;
     b.nx = ((b.mx + 2 * b.g + 31) / 32) * 32;
     b.ny = b.my + 2 * b.g;
     b.nz = b.mz + 2 * b.g;
@@ -379,9 +379,18 @@ int setup_device(cc_ctx *c) {
     bi.mx = b.mx, bi.my = b.my, bi.mz = b.mz, bi.g = b.g, bi.nx = b.nx, bi.ny = b.ny, bi.nz = b.nz;
     bi.base = b.base, bi.off = b.off, bi.ng = (int64_t)b.nx * b.ny * b.nz, bi.interior_off = n_int;
     n_int += (int64_t)b.mx * b.my * b.mz;
-    c->hblocks.push_back(bi);
+    info.push_back(bi);
   }
-  c->N = ((end + 31) / 32) * 32;
+  return ((end + 31) / 32) * 32;
+}
+
+// Layout, device allocation, halo program, geometry.  Runs once.
+int setup_device(cc_ctx *c) {
+  const int ns = c->chem.ns;
+  c->elem = c->precision == CC_FP64 ? 8 : 4;
+  c->ns_key = ns == 0 ? 0 : (ns == 9 ? 9 : -1);
+  int64_t n_int = 0;
+  c->N = layout_blocks(c->blocks, c->ngg, c->hblocks, n_int);
   c->n_int = n_int;
   if ((double)c->N * (6 + kMaxSpec) >= 2147483647.0)
     return fail(CC_ERR_ARG, "grid too large for one context (32-bit field offsets); split it over contexts");
@@ -1659,6 +1668,60 @@ int cc_set_launch_mode(cc_ctx *c, int per_block) {
   if (int r = check_ctx(c)) return r;
   c->per_block = per_block != 0;
   destroy_graphs(c);
+  return 0;
+}
+
+int cc_halo_dependencies(cc_ctx *c, int64_t *dst, int64_t *src, int *which, int64_t cap, int64_t *n) {
+  if (int r = check_ctx(c)) return r;
+  if (!n || cap < 0) return fail(CC_ERR_ARG, "cc_halo_dependencies: n is null or cap < 0");
+  if (c->blocks.empty()) return fail(CC_ERR_STATE, "no blocks");
+  std::vector<HostBlock> blocks = c->blocks;  // the context's own layout is set by cc_init
+  std::vector<BlockInfo> info;
+  int64_t n_int = 0;
+  layout_blocks(blocks, c->ngg, info, n_int);
+  HaloPlan plan;
+  if (!build_halo_plan(blocks, c->bcs, plan)) return fail(CC_ERR_TOPOLOGY, "halo program: " + plan.error);
+  // the points of the current (kind 0) or previous (kind 1) state that a
+  // reference resolves to, through the scratch nodes it reads
+  std::vector<std::pair<int64_t, int>> found;
+  std::function<void(const HaloRef &)> walk = [&](const HaloRef &r) {
+    if (r.kind == 0 || r.kind == 1) {
+      found.push_back({r.idx, r.kind});
+      return;
+    }
+    const HaloNode &nd = plan.nodes.at((size_t)r.idx);
+    if (nd.op == kHaloInflow || nd.op == kHaloKeep) return;
+    walk(nd.a);
+    if (nd.op == kHaloAvg || nd.op == kHaloWallGhost) walk(nd.b);
+  };
+  int64_t k = 0;
+  for (const HaloCopy &hc : plan.copies) {
+    found.clear();
+    walk(hc.src);
+    std::sort(found.begin(), found.end());
+    found.erase(std::unique(found.begin(), found.end()), found.end());
+    for (const auto &f : found) {
+      if (k < cap) {
+        if (dst) dst[k] = hc.dst;
+        if (src) src[k] = f.first;
+        if (which) which[k] = f.second;
+      }
+      ++k;
+    }
+  }
+  *n = k;
+  return 0;
+}
+
+int cc_block_arena(cc_ctx *c, int block, int64_t *first, int64_t *count) {
+  if (int r = check_ctx(c)) return r;
+  if (block < 0 || block >= (int)c->blocks.size()) return fail(CC_ERR_ARG, "cc_block_arena: no such block");
+  std::vector<HostBlock> blocks = c->blocks;
+  std::vector<BlockInfo> info;
+  int64_t n_int = 0;
+  layout_blocks(blocks, c->ngg, info, n_int);
+  if (first) *first = info[(size_t)block].off;
+  if (count) *count = info[(size_t)block].ng;
   return 0;
 }
 

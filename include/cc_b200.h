@@ -239,6 +239,21 @@ int cc_eval_transport(cc_ctx *ctx, int64_t n, const double *T, const double *Y, 
  * needs a context initialised with the same blocks, species and precision. */
 int cc_save_checkpoint(cc_ctx *ctx, const char *path);
 int cc_load_checkpoint(cc_ctx *ctx, const char *path);
+/* No counterpart in the reference, whose multi-process exchange
+ * (ParallelFace, Mesh.h:62-102) is unfinished.  Host-side query for a run in
+ * which each process computes some of the blocks: the halo program's
+ * dependencies as triples (dst[k], src[k], which[k]), one for every arena
+ * point src[k] of the current (which 0) or previous (which 1) state that the
+ * final value of the changed point dst[k] is computed from (a copied point,
+ * or a source of an interface average, wall or inflow node), so that a
+ * process can fetch from their owners the sources of its own blocks' halo
+ * before running it.  Needs no device and may be called before cc_init, once
+ * the blocks, faces and conditions are added.  Writes at most cap triples
+ * (any of dst, src, which may be null) and the total count to *n. */
+int cc_halo_dependencies(cc_ctx *ctx, int64_t *dst, int64_t *src, int *which, int64_t cap, int64_t *n);
+/* Arena index of the first point of block b's ghosted box and its point
+ * count, in the layout of cc_halo_dependencies (no device needed). */
+int cc_block_arena(cc_ctx *ctx, int block, int64_t *first, int64_t *count);
 /* Synchronises the context's stream. */
 int cc_sync(cc_ctx *ctx);
 
