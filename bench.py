@@ -29,6 +29,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "box128_9sp_viscous_rk3"
+E_STEPS = 1000  # steps of the workload's job (the end-to-end leg runs the whole job)
 METRIC = "Mcell-updates/s per RK stage, mixed vs FP64 plain, at stated L2 err vs FP64"
 
 
@@ -235,9 +236,14 @@ def run_ours(args, rank, world, dist):
         errs.update(field_errors(b32, b64))
         errs["l2_Y"] = l2(y32, y64)
         errs["linf_Y"] = li(y32, y64)
-    # end-to-end through the C ABI with host buffers (mixed): upload of the
-    # state from pinned memory, K steps each reading back the residual, and the
-    # download of the final state
+        for k, nm in enumerate(sp["names"]):
+            errs["l2_Y_" + nm] = l2(y32[k], y64[k])
+            errs["linf_Y_" + nm] = li(y32[k], y64[k])
+    # end to end through the C ABI with host buffers (mixed), as a caller of
+    # the workload runs it: the initial state uploaded from pinned host memory,
+    # the workload's E_STEPS steps, each computing the residual and copying it
+    # into pinned host memory without waiting (cc_residual_async), and the
+    # final state downloaded.  The job length is the workload's, not --steps.
     e2e = None
     if rank == 0:
         blk = case["blocks"][0]
@@ -253,19 +259,23 @@ def run_ours(args, rank, world, dist):
         bv_o = pin(np.empty_like(bv_h))
         yk_o = pin(np.empty_like(yk_h))
         cv_o = pin(np.empty((14, ng)))
-        K = args.steps
+        K = E_STEPS
+        res_h = pin(np.zeros((K, 4)))
         t0 = time.perf_counter()
         d.field[0].set_state(bv_h, yk_h)
-        for _ in range(K):
+        for s in range(K):
             d.simulate(1, residual=True)
-            d.residual()
-        cc._check(d.lib.cc_get_state(d.ctx, 0, cc._ptr(bv_o), cc._ptr(yk_o), cc._ptr(cv_o)))
+            cc._check(d.lib.cc_residual_async(d.ctx, res_h[s].ctypes.data_as(cc._dp)))
+        cc._check(d.lib.cc_get_state(d.ctx, 0, cc._ptr(bv_o), cc._ptr(yk_o), cc._ptr(cv_o), 0))
         dt = time.perf_counter() - t0
+        assert np.isfinite(res_h).all() and (res_h[:, 0] > 0).all()
         npts = out["mixed"]["npts"]
         up = bv_h.nbytes + yk_h.nbytes
-        down = bv_o.nbytes + yk_o.nbytes + cv_o.nbytes + 32 * K
+        down = bv_o.nbytes + yk_o.nbytes + cv_o.nbytes + res_h.nbytes
         e2e = {"value": npts * 3 * K / dt / 1e6, "unit": "Mcell-updates/s", "h2d_bytes_per_step": up / K,
-               "d2h_bytes_per_step": down / K, "timing": "host wall clock, synchronised, whole job"}
+               "d2h_bytes_per_step": down / K, "steps": K,
+               "timing": "host wall clock around the whole job: state upload from pinned memory, %d steps with "
+                         "the residual of every step copied to pinned memory asynchronously, state download" % K}
         d.close()
     return out, errs, e2e
 

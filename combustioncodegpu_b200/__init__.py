@@ -87,11 +87,11 @@ EXPORTS = {
     "cc_add_boundary": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(CCBoundary)], ctypes.c_int),
     "cc_add_inner_face": ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(CCInnerFace)], ctypes.c_int),
     "cc_add_bc": ([ctypes.c_void_p, ctypes.POINTER(CCBc)], ctypes.c_int),
-    "cc_set_state": ([ctypes.c_void_p, ctypes.c_int, _dp, _dp], ctypes.c_int),
+    "cc_set_state": ([ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int], ctypes.c_int),
     "cc_init": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_step": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "cc_residual": ([ctypes.c_void_p, _dp], ctypes.c_int),
-    "cc_get_state": ([ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp], ctypes.c_int),
+    "cc_get_state": ([ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int], ctypes.c_int),
     "cc_get_props": ([ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp], ctypes.c_int),
     "cc_last_dt": ([ctypes.c_void_p, _dp], ctypes.c_int),
     "cc_status": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint)], ctypes.c_int),
@@ -99,6 +99,9 @@ EXPORTS = {
     "cc_get_stream": ([ctypes.c_void_p], ctypes.c_void_p),
     "cc_use_graph": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_set_renormalize": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "cc_residual_async": ([ctypes.c_void_p, _dp], ctypes.c_int),
+    "cc_set_wait_limit": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "cc_set_newton_max_iter": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_info": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "cc_time_kernels": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp], ctypes.c_int),
@@ -241,20 +244,31 @@ class Mesh(list):
         return sum(b.mx * b.my * b.mz for b in self)
 
 
+def _layout(name):
+    """CC_LAYOUT_FIELD_MAJOR (0) for "field", CC_LAYOUT_POINT_MAJOR (1) for "point"."""
+    if name not in ("field", "point"):
+        raise ValueError("layout must be 'field' or 'point'")
+    return 1 if name == "point" else 0
+
+
 class Field:
     """cfd::Field (Field.h:67-82): one block's state on the device."""
 
     def __init__(self, driver, index, block):
         self.driver, self.index, self.block = driver, index, block
 
-    def get_state(self):
-        """(bv [6][Ng], yk [n_spec][Ng], cv [n_var][Ng]) as FP64 host arrays."""
+    def get_state(self, layout="field"):
+        """(bv, yk, cv) as FP64 host arrays: [6][Ng], [n_spec][Ng],
+        [n_var][Ng] (layout "field"), or [Ng][6], [Ng][n_spec], [Ng][n_var]
+        (layout "point", the reference's VectorField3D order)."""
         d = self.driver
         ng = self.block.n_ghosted(d.ngg)
-        bv = np.empty((6, ng))
-        yk = np.empty((max(d.n_spec, 0), ng))
-        cv = np.empty((5 + d.n_spec, ng))
-        _check(d.lib.cc_get_state(d.ctx, self.index, _ptr(bv), _ptr(yk) if d.n_spec else None, _ptr(cv)))
+        pm = _layout(layout)
+        shape = (lambda nf: (ng, nf)) if pm else (lambda nf: (nf, ng))
+        bv = np.empty(shape(6))
+        yk = np.empty(shape(max(d.n_spec, 0)))
+        cv = np.empty(shape(5 + d.n_spec))
+        _check(d.lib.cc_get_state(d.ctx, self.index, _ptr(bv), _ptr(yk) if d.n_spec else None, _ptr(cv), pm))
         return bv, yk, cv
 
     def get_props(self):
@@ -266,11 +280,13 @@ class Field:
         _check(d.lib.cc_get_props(d.ctx, self.index, _ptr(mul), _ptr(cond), _ptr(rd) if d.n_spec else None))
         return mul, cond, rd
 
-    def set_state(self, bv, yk=None):
+    def set_state(self, bv, yk=None, layout="field"):
+        """bv (and yk) in layout "field" ([n_field][Ng]) or "point"
+        ([Ng][n_field])."""
         d = self.driver
         bv = np.ascontiguousarray(bv, dtype=np.float64)
         yk = np.ascontiguousarray(yk, dtype=np.float64) if d.n_spec else None
-        _check(d.lib.cc_set_state(d.ctx, self.index, _ptr(bv), _ptr(yk)))
+        _check(d.lib.cc_set_state(d.ctx, self.index, _ptr(bv), _ptr(yk), _layout(layout)))
 
 
 def make_params(parameter, species):
@@ -388,6 +404,16 @@ class Driver:
         """Y renormalisation after each update: True/False, or None for the
         precision's default (mixed on, FP64 off)."""
         _check(self.lib.cc_set_renormalize(self.ctx, -1 if enable is None else (1 if enable else 0)))
+
+    def set_wait_limit(self, spins=0):
+        """Polls of a device-side wait before the kernel gives up and sets its
+        status bit; 0 restores the default."""
+        _check(self.lib.cc_set_wait_limit(self.ctx, int(spins)))
+
+    def set_newton_max_iter(self, n=0):
+        """Iteration cap of the temperature Newton; 0 restores the
+        reference's 1000."""
+        _check(self.lib.cc_set_newton_max_iter(self.ctx, int(n)))
 
     def use_graph(self, enable=True):
         _check(self.lib.cc_use_graph(self.ctx, 1 if enable else 0))

@@ -242,6 +242,19 @@ int from64(cc_ctx *c, const double *src, void *dst, int64_t count) {
   return 0;
 }
 
+// nf fields of ng points between point-major ([ng][nf], from_point_major)
+// and field-major ([nf][ng]) host order.
+void transpose_fields(const double *src, int64_t ng, int nf, std::vector<double> &dst, bool from_point_major) {
+  dst.resize((size_t)(ng * nf));
+  for (int64_t p = 0; p < ng; ++p)
+    for (int f = 0; f < nf; ++f) {
+      if (from_point_major)
+        dst[(size_t)(f * ng + p)] = src[p * nf + f];
+      else
+        dst[(size_t)(p * nf + f)] = src[f * ng + p];
+    }
+}
+
 // Stage-kernel work list: kTX x kTY columns, k split into chunks of kz.
 void build_tiles_kz(cc_ctx *c, int kz) {
   c->htiles.clear();
@@ -1035,6 +1048,8 @@ int cc_create(const cc_params *params, cc_ctx **out) {
   c->chem.cfl = params->cfl;
   c->chem.Sc = params->n_spec > 0 ? params->schmidt_number : 1.0;
   c->chem.p_ref = 0.0;  // set at the first cc_init for the FP32 bulk precisions
+  c->chem.max_spins = kDefaultWaitSpins;
+  c->chem.newton_max_iter = 1000;
   fill_tables(c->chem.d, params);
   fill_tables(c->chem.f, params);
   *out = c;
@@ -1134,12 +1149,23 @@ int cc_add_bc(cc_ctx *c, const cc_bc *bc) {
   return 0;
 }
 
-int cc_set_state(cc_ctx *c, int block, const double *bv, const double *yk) {
+int cc_set_state(cc_ctx *c, int block, const double *bv, const double *yk, int layout) {
   if (int r = check_ctx(c)) return r;
   if (block < 0 || block >= (int)c->blocks.size()) return fail(CC_ERR_ARG, "bad block");
   if (!bv || (c->chem.ns > 0 && !yk)) return fail(CC_ERR_ARG, "bv (and yk when n_spec > 0) required");
+  if (layout != CC_LAYOUT_FIELD_MAJOR && layout != CC_LAYOUT_POINT_MAJOR)
+    return fail(CC_ERR_ARG, "layout must be CC_LAYOUT_FIELD_MAJOR or CC_LAYOUT_POINT_MAJOR");
   const HostBlock &b = c->blocks[block];
   const int64_t ng = ng_user(b);
+  std::vector<double> bv_fm, yk_fm;  // field-major copies of point-major input
+  if (layout == CC_LAYOUT_POINT_MAJOR) {
+    transpose_fields(bv, ng, 6, bv_fm, true);
+    bv = bv_fm.data();
+    if (c->chem.ns > 0) {
+      transpose_fields(yk, ng, c->chem.ns, yk_fm, true);
+      yk = yk_fm.data();
+    }
+  }
   if (!c->initialized) {
     c->pend_bv[block].assign(bv, bv + 6 * ng);
     if (c->chem.ns > 0) c->pend_yk[block].assign(yk, yk + c->chem.ns * ng);
@@ -1247,10 +1273,33 @@ int cc_residual(cc_ctx *c, double out[4]) {
   return 0;
 }
 
-int cc_get_state(cc_ctx *c, int block, double *bv, double *yk, double *cv) {
+int cc_residual_async(cc_ctx *c, double *out) {
+  if (int r = check_ctx(c)) return r;
+  if (!c->initialized) return fail(CC_ERR_STATE, "cc_residual_async before cc_init");
+  if (!out) return fail(CC_ERR_ARG, "out is null");
+  CK(cudaMemcpyAsync(out, c->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return 0;
+}
+
+int cc_get_state(cc_ctx *c, int block, double *bv, double *yk, double *cv, int layout) {
   if (int r = check_ctx(c)) return r;
   if (!c->initialized) return fail(CC_ERR_STATE, "cc_get_state before cc_init");
   if (block < 0 || block >= (int)c->blocks.size()) return fail(CC_ERR_ARG, "bad block");
+  if (layout != CC_LAYOUT_FIELD_MAJOR && layout != CC_LAYOUT_POINT_MAJOR)
+    return fail(CC_ERR_ARG, "layout must be CC_LAYOUT_FIELD_MAJOR or CC_LAYOUT_POINT_MAJOR");
+  if (layout == CC_LAYOUT_POINT_MAJOR) {  // field-major into scratch, then transposed
+    const int64_t ng = ng_user(c->blocks[block]);
+    const int ns = c->chem.ns, nv = nv_of(c);
+    std::vector<double> fb(bv ? 6 * ng : 0), fy(yk && ns ? ns * ng : 0), fc(cv ? nv * ng : 0);
+    if (int r = cc_get_state(c, block, bv ? fb.data() : nullptr, yk && ns ? fy.data() : nullptr,
+                             cv ? fc.data() : nullptr, CC_LAYOUT_FIELD_MAJOR))
+      return r;
+    std::vector<double> t;
+    if (bv) transpose_fields(fb.data(), ng, 6, t, false), std::copy(t.begin(), t.end(), bv);
+    if (yk && ns) transpose_fields(fy.data(), ng, ns, t, false), std::copy(t.begin(), t.end(), yk);
+    if (cv) transpose_fields(fc.data(), ng, nv, t, false), std::copy(t.begin(), t.end(), cv);
+    return 0;
+  }
   if (c->state_dirty) {
     destroy_graphs(c);
     int r = dispatch(c, [&](auto tt, auto nn) { return derive_state<typename decltype(tt)::type, decltype(nn)::value>(c); });
@@ -1330,6 +1379,20 @@ void *cc_get_stream(cc_ctx *c) { return c ? (void *)c->stream : nullptr; }
 int cc_set_renormalize(cc_ctx *c, int enable) {
   if (int r = check_ctx(c)) return r;
   c->renorm = enable < 0 ? -1 : (enable != 0);
+  destroy_graphs(c);
+  return 0;
+}
+
+int cc_set_wait_limit(cc_ctx *c, int64_t spins) {
+  if (int r = check_ctx(c)) return r;
+  c->chem.max_spins = spins > 0 ? (long long)spins : kDefaultWaitSpins;
+  destroy_graphs(c);  // the captured launches carry the parameters by value
+  return 0;
+}
+
+int cc_set_newton_max_iter(cc_ctx *c, int n) {
+  if (int r = check_ctx(c)) return r;
+  c->chem.newton_max_iter = n > 0 ? n : 1000;
   destroy_graphs(c);
   return 0;
 }
@@ -1684,13 +1747,20 @@ int cc_halo_dependencies(cc_ctx *c, int64_t *dst, int64_t *src, int *which, int6
   // the points of the current (kind 0) or previous (kind 1) state that a
   // reference resolves to, through the scratch nodes it reads
   std::vector<std::pair<int64_t, int>> found;
+  bool unknown_op = false;
   std::function<void(const HaloRef &)> walk = [&](const HaloRef &r) {
     if (r.kind == 0 || r.kind == 1) {
       found.push_back({r.idx, r.kind});
       return;
     }
     const HaloNode &nd = plan.nodes.at((size_t)r.idx);
-    if (nd.op == kHaloInflow || nd.op == kHaloKeep) return;
+    if (nd.op == kHaloInflow) return;  // a constant state: no source point
+    if (nd.op != kHaloCopy && nd.op != kHaloAvg && nd.op != kHaloWallFace && nd.op != kHaloWallGhost) {
+      // an op without a rule here (kHaloKeep is reserved and never emitted):
+      // refuse rather than drop its sources silently
+      unknown_op = true;
+      return;
+    }
     walk(nd.a);
     if (nd.op == kHaloAvg || nd.op == kHaloWallGhost) walk(nd.b);
   };
@@ -1698,6 +1768,7 @@ int cc_halo_dependencies(cc_ctx *c, int64_t *dst, int64_t *src, int *which, int6
   for (const HaloCopy &hc : plan.copies) {
     found.clear();
     walk(hc.src);
+    if (unknown_op) return fail(CC_ERR_STATE, "cc_halo_dependencies: halo node op without a dependency rule");
     std::sort(found.begin(), found.end());
     found.erase(std::unique(found.begin(), found.end()), found.end());
     for (const auto &f : found) {

@@ -12,6 +12,7 @@ constexpr int kMaxSpec = 16;           // species supported by one context
 constexpr int kTX = 32;                // stage tile: points along i (one warp)
 constexpr int kTY = 8;                 // stage tile: points along j (warps)
 constexpr int kRecLen = 12;            // values per NASA-7 record (cp, h, pad)
+constexpr long long kDefaultWaitSpins = 1LL << 22;  // polls of a device wait before it gives up
 
 // Per-precision species tables, passed to every kernel by value (constant
 // bank).  Horner-form NASA-7 coefficients: for T >= t_mid the `hi` set.
@@ -44,6 +45,14 @@ struct ChemParams {
   // the FP64 path), and the momentum face fluxes carry p - p_ref, so that
   // FP32 rounding acts on the pressure variations, not on ~1e5 Pa
   double p_ref;
+  // polls of a device wait (TMA plane, tensor-core completion) before the
+  // kernel gives up on it and sets its status bit (cc_set_wait_limit); the
+  // drain of copies in flight after such an abort keeps its own fixed bound
+  long long max_spins;
+  // iteration cap of the temperature Newton (Thermo.cu:103-121 stops after
+  // 1000; cc_set_newton_max_iter)
+  int newton_max_iter;
+  int pad_;
   SpecTables<double> d;
   SpecTables<float> f;
 };
@@ -99,7 +108,7 @@ enum HaloOp : int {
   kHaloInflow = 2,     // dst <- inflow state bc
   kHaloWallFace = 3,   // wall point: p, Y from src (i-dir), T_wall or T(src)
   kHaloWallGhost = 4,  // mirror of src; T reference from src2 (i-dir)
-  kHaloKeep = 5,       // dst <- previous buffer value of dst
+  kHaloKeep = 5,       // reserved (dst <- previous buffer value of dst): never emitted by the builder
 };
 
 struct BcDevice {

@@ -32,7 +32,7 @@ namespace ccb {
 constexpr int kMlpSmem = kMlpWBytes + kMlpXBytes + kMlpHBytes + kMlpBias * 4 + 64;
 constexpr int kMlpTmemCols = 64;
 constexpr unsigned kStatusMlpTimeout = 16u;  // an MMA completion wait gave up
-constexpr long kMlpMaxSpins = 1L << 22;
+constexpr long long kMlpMaxSpins = kDefaultWaitSpins;  // bound of the drain after an abort
 constexpr float kMlpPureX = 0.998f;  // mole fraction above which the exact transport is used
 
 __device__ __forceinline__ uint32_t mlp_smem_u32(const void *p) {
@@ -200,11 +200,11 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
                          mlp_smem_u32(bar))
                      : "memory");
       }
-      long spins = 0;
+      long long spins = 0;
       while (!mlp_try_wait(bar, phase))
-        if (++spins > kMlpMaxSpins) break;
+        if (++spins > C.max_spins) break;
       phase ^= 1u;
-      if (__syncthreads_or(spins > kMlpMaxSpins)) {
+      if (__syncthreads_or(spins > C.max_spins)) {
         late = true;
         break;
       }

@@ -11,10 +11,15 @@
 // the library holds it until the process exits.  Host code must not take its
 // address directly: in host code the symbol is only a stand-in, so the first
 // call on each device looks up the device address with cudaGetSymbolAddress
-// (that first call should therefore come before any stream capture).  Every
-// call shares the array and it keeps the previous call's contents; each call
-// writes every partial it later reads, so nothing needs clearing, but two
-// calls whose work overlaps on the GPU race on it.
+// (that first call should therefore come before any stream capture).  The
+// address belongs to the device's current context: if that context is
+// destroyed and a new one made (cudaDeviceReset, or a host application that
+// resets the device), the module is loaded again at another address, so the
+// cached address is keyed on the context's unique id and looked up again when
+// the id changes.  Every call shares the array and it keeps the previous
+// call's contents; each call writes every partial it later reads, so nothing
+// needs clearing, but two calls whose work overlaps on the GPU race on it.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -67,7 +72,39 @@ __global__ void k_final(const double *partials, int n_partials, int64_t n, doubl
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-double *g_scratch[kMaxDevices] = {nullptr};
+struct Scratch {
+  unsigned long long ctx_id;  // context the address belongs to
+  double *ptr;
+};
+Scratch g_scratch[kMaxDevices] = {};
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// Unique id of the calling thread's current context (0 when it cannot be
+// read).  The driver entry points are looked up once.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(fn);
+    looked_up = true;
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 int fail(int code, const std::string &msg) {
   ccb_set_last_error(msg);
@@ -85,22 +122,29 @@ extern "C" int cc_residual_rms_noalloc(const double *cur, const double *last, in
                                 "]: the fixed scratch holds one partial sum per 4096 points");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+  if (e != cudaSuccess)
     return fail(CC_ERR_CUDA, std::string("cc_residual_rms_noalloc: no current device: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return fail(CC_ERR_ARG, "cc_residual_rms_noalloc: device index " + std::to_string(dev) + " is not below " +
+                                std::to_string(kMaxDevices) + ", the devices this entry point keeps an address for");
   double *scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch[dev]) {
-      // once per device, with that device current: the device address of the
-      // static array (its host-side name is not a device address)
+    const unsigned long long id = current_context_id();
+    Scratch &sc = g_scratch[dev];
+    if (!sc.ptr || id == 0 || sc.ctx_id != id) {
+      // once per device and context, with that device current: the device
+      // address of the static array (its host-side name is not a device
+      // address)
       void *p = nullptr;
       e = cudaGetSymbolAddress(&p, g_partials);
       if (e != cudaSuccess || !p)
         return fail(CC_ERR_CUDA,
                     std::string("cc_residual_rms_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-      g_scratch[dev] = static_cast<double *>(p);
+      sc.ptr = static_cast<double *>(p);
+      sc.ctx_id = id;
     }
-    scratch = g_scratch[dev];
+    scratch = sc.ptr;
   }
   const int grid = (int)((n + kPointsPerCta - 1) / kPointsPerCta);
   cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -221,7 +221,8 @@ __device__ __forceinline__ void point_props(const ChemParams &C, const T *rec, T
 }
 
 // Temperature from internal energy by Newton iteration (tolerance 1e-3 on
-// |1 - T1/T|, at most 1000 iterations, warm start t), in the precision W:
+// |1 - T1/T|, at most C.newton_max_iter iterations (1000 by default, as the
+// reference), warm start t), in the precision W:
 // FP64 for the plain and mixed paths, FP32 for the full-FP32 study.
 template <typename W, int NS>
 __device__ __forceinline__ W newton_temperature_w(const ChemParams &C, const W *rec, W e, const W *Y, W gas_const,
@@ -231,7 +232,7 @@ __device__ __forceinline__ W newton_temperature_w(const ChemParams &C, const W *
   const int ns = SpecCount<NS>::n(C);
   W err = 1;
   int iter = 0;
-  while (err > W(1e-3) && iter++ < 1000) {
+  while (err > W(1e-3) && iter++ < C.newton_max_iter) {
     W cp_tot = 0, h = 0;
 #pragma unroll
     for (int l = 0; l < A; ++l) {

@@ -11,8 +11,9 @@
 // done, so copies run two planes ahead of the sweep and overlap the point
 // updates.  Transport properties and geometry are read through L1.
 //
-// Waits are bounded: a CTA whose plane does not arrive within kMaxSpins
-// polls sets kStatusTmaTimeout in the status word and leaves the sweep.
+// Waits are bounded: a CTA whose plane does not arrive within C.max_spins
+// polls sets kStatusTmaTimeout in the status word, waits (at most kMaxSpins
+// polls each) for the copies it has in flight and leaves the sweep.
 #pragma once
 #include <cuda.h>
 
@@ -25,7 +26,7 @@ constexpr int kHY = kTY + 4;               // staged points along j
 constexpr int kPlaneVals = kHX * kHY;      // values per field and plane
 constexpr int kSlots = 5;                  // planes in flight: k-1 .. k+3
 constexpr unsigned kStatusTmaTimeout = 8u;
-constexpr long kMaxSpins = 1L << 22;
+constexpr long long kMaxSpins = kDefaultWaitSpins;  // bound of the drain after an abort
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -181,9 +182,9 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
     // planes k-1 .. k+2 must be resident
     bool late = false;
     for (int kp = k - 1; kp <= k + 2; ++kp) {
-      long spins = 0;
+      long long spins = 0;
       while (!mbar_try_wait(&bars[slot_of(kp)], parity_of(kp))) {
-        if (++spins > kMaxSpins) {
+        if (++spins > C.max_spins) {
           late = true;
           break;
         }
@@ -396,9 +397,9 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
   for (int k = t.k0; k < t.k1; ++k) {
     bool late = false;
     for (int kp = k - 1; kp <= k + 2; ++kp) {
-      long spins = 0;
+      long long spins = 0;
       while (!mbar_try_wait(&bars[slot_of(kp)], parity_of(kp)))
-        if (++spins > kMaxSpins) {
+        if (++spins > C.max_spins) {
           late = true;
           break;
         }

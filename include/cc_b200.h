@@ -138,11 +138,19 @@ int cc_add_inner_face(cc_ctx *ctx, int block, const cc_inner_face *f);
  * (outflow, inflow, wall; BoundCond.cu:251-313), then the block interfaces. */
 int cc_add_bc(cc_ctx *ctx, const cc_bc *bc);
 
+/* Host layout of the state arrays of cc_set_state / cc_get_state:
+ * FIELD_MAJOR = one field after another, [n_field][Ng], i fastest within a
+ * field; POINT_MAJOR = the reference's VectorField3D order (Field.h:36-63,
+ * indexed point * n_field + l as in Driver.cu:341-344), [Ng][n_field], the
+ * component fastest.  Ng runs over the ghosted box, i fastest, then j, k. */
+#define CC_LAYOUT_FIELD_MAJOR 0
+#define CC_LAYOUT_POINT_MAJOR 1
 /* HZone::bv / HZone::yk (Field.h:13-32), copied host -> device:
- * bv [6][Ng] = rho,u,v,w,p,T;  yk [n_spec][Ng].  Before cc_init it sets the
- * initial field; afterwards it replaces the state (primitives, conserved
- * variables and properties are re-derived as by cc_init). */
-int cc_set_state(cc_ctx *ctx, int block, const double *bv, const double *yk);
+ * bv = rho,u,v,w,p,T (6 fields);  yk = n_spec fields, in `layout`.  Before
+ * cc_init it sets the initial field; afterwards it replaces the state
+ * (primitives, conserved variables and properties are re-derived as by
+ * cc_init). */
+int cc_set_state(cc_ctx *ctx, int block, const double *bv, const double *yk, int layout);
 /* Driver::initialize_computation (Driver.cu:59-97). */
 int cc_init(cc_ctx *ctx, int precision);
 /* Driver::simulate: n_steps steps of the chosen scheme (Driver.cu:113-192).
@@ -151,15 +159,32 @@ int cc_step(cc_ctx *ctx, int n_steps, int scheme, int want_residual);
 /* Driver::compute_residual (Driver.cu:219-277): RMS change of rho, |V|, p, T
  * over the last step, before the res_scale normalisation. */
 int cc_residual(cc_ctx *ctx, double out[4]);
-/* Device -> host: bv [6][Ng], yk [n_spec][Ng], cv [n_var][Ng]; null skips. */
-int cc_get_state(cc_ctx *ctx, int block, double *bv, double *yk, double *cv);
+/* The same four values copied into out[4] on the context's stream without
+ * waiting (out should be pinned host memory); they are there once the stream
+ * has reached the copy (cc_sync, or an event recorded after the call). */
+int cc_residual_async(cc_ctx *ctx, double *out);
+/* Device -> host: bv (6 fields), yk (n_spec), cv (n_var) in `layout`; null
+ * skips an array. */
+int cc_get_state(cc_ctx *ctx, int block, double *bv, double *yk, double *cv, int layout);
 /* DZone::mul / conductivity / rho_D (Field.h:52-56): [Ng], [Ng], [n_spec][Ng]. */
 int cc_get_props(cc_ctx *ctx, int block, double *mul, double *conductivity, double *rho_d);
 /* Time step of the last completed step (RK3). */
 int cc_last_dt(cc_ctx *ctx, double *dt);
 /* Device status word: bit 0 Newton iteration cap hit, bit 1 non-finite or
- * non-positive rho/p/T, bit 2 invalid time step.  Cleared by the call. */
+ * non-positive rho/p/T, bit 2 invalid time step, bit 3 a TMA plane wait gave
+ * up, bit 4 a tensor-core completion wait of the closure gave up.  Cleared by
+ * the call.  The reference checks none of these (its Newton, Thermo.cu:103-121,
+ * stops silently after 1000 iterations). */
 int cc_status(cc_ctx *ctx, unsigned *flags);
+/* No counterpart in the reference.  Polls of a device-side wait (a TMA plane,
+ * a tensor-core completion) before the kernel gives up on it, sets its status
+ * bit (3 or 4) and returns; the context stays usable.  spins <= 0 restores the
+ * default (2^22).  Takes effect at the next cc_step. */
+int cc_set_wait_limit(cc_ctx *ctx, int64_t spins);
+/* Iteration cap of the temperature Newton (Thermo.cu:103-121: 1000); a point
+ * that reaches it sets status bit 0.  n <= 0 restores 1000.  Takes effect at
+ * the next cc_step. */
+int cc_set_newton_max_iter(cc_ctx *ctx, int n);
 /* Stream used by every launch of the context (default: a private stream). */
 int cc_set_stream(cc_ctx *ctx, void *cuda_stream);
 void *cc_get_stream(cc_ctx *ctx);
@@ -286,8 +311,10 @@ int cc_mlp_adam(int64_t n, float *params, const float *grad, float *m, float *v,
  * scratch is a fixed 64 KiB array inside the library (held by every device
  * that loads it), so n is limited to CC_NOALLOC_MAX_POINTS; larger n is
  * rejected with CC_ERR_ARG.  The first call on a device looks up that
- * array's device address, so make it before any stream capture.  Calls share
- * the array: calls that overlap on the GPU race. */
+ * array's device address, so make it before any stream capture; the address
+ * is kept per device and context, and looked up again on the first call in a
+ * new context (after a device reset).  Calls share the array: calls that
+ * overlap on the GPU race. */
 #define CC_NOALLOC_MAX_POINTS 8388608
 int cc_residual_rms_noalloc(const double *cur, const double *last, int64_t n, double *out, void *stream);
 

@@ -106,11 +106,14 @@ class Driver;
 class Field {
  public:
   Field(Driver *d, int id, const Block *b) : driver_(d), id_(id), block_(b) {}
-  // bv [6][Ng], yk [n_spec][Ng], cv [n_var][Ng] (HZone::bv/yk, DZone::cv)
-  void get_state(std::vector<double> &bv, std::vector<double> &yk, std::vector<double> &cv) const;
+  // bv (6 fields), yk (n_spec), cv (n_var) over the Ng ghosted points
+  // (HZone::bv/yk, DZone::cv): field-major [field][Ng] by default, or
+  // CC_LAYOUT_POINT_MAJOR, the VectorField3D order [Ng][field]
+  void get_state(std::vector<double> &bv, std::vector<double> &yk, std::vector<double> &cv,
+                 int layout = CC_LAYOUT_FIELD_MAJOR) const;
   // DZone::mul, conductivity, rho_D
   void get_props(std::vector<double> &mul, std::vector<double> &cond, std::vector<double> &rho_d) const;
-  void set_state(const std::vector<double> &bv, const std::vector<double> &yk);
+  void set_state(const std::vector<double> &bv, const std::vector<double> &yk, int layout = CC_LAYOUT_FIELD_MAJOR);
   int id() const { return id_; }
 
  private:
@@ -205,13 +208,15 @@ class Driver {
   cc_ctx *ctx_ = nullptr;
 };
 
-inline void Field::get_state(std::vector<double> &bv, std::vector<double> &yk, std::vector<double> &cv) const {
+inline void Field::get_state(std::vector<double> &bv, std::vector<double> &yk, std::vector<double> &cv,
+                             int layout) const {
   const int64_t ng = block_->n_ghosted(driver_->ngg());
   const int ns = driver_->n_spec();
   bv.assign(6 * ng, 0.0);
   yk.assign(ns * ng, 0.0);
   cv.assign((5 + ns) * ng, 0.0);
-  check(cc_get_state(driver_->context(), id_, bv.data(), ns ? yk.data() : nullptr, cv.data()), "cc_get_state");
+  check(cc_get_state(driver_->context(), id_, bv.data(), ns ? yk.data() : nullptr, cv.data(), layout),
+        "cc_get_state");
 }
 
 inline void Field::get_props(std::vector<double> &mul, std::vector<double> &cond, std::vector<double> &rho_d) const {
@@ -224,8 +229,8 @@ inline void Field::get_props(std::vector<double> &mul, std::vector<double> &cond
         "cc_get_props");
 }
 
-inline void Field::set_state(const std::vector<double> &bv, const std::vector<double> &yk) {
-  check(cc_set_state(driver_->context(), id_, bv.data(), yk.empty() ? nullptr : yk.data()), "cc_set_state");
+inline void Field::set_state(const std::vector<double> &bv, const std::vector<double> &yk, int layout) {
+  check(cc_set_state(driver_->context(), id_, bv.data(), yk.empty() ? nullptr : yk.data(), layout), "cc_set_state");
 }
 
 }  // namespace cfd

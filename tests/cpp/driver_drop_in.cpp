@@ -6,15 +6,33 @@
 // ("mx my mz n_boundary n_inner" and the raw face records), block_<b>.bin
 // (jacobian, metric, bv, yk), bcs.bin (cc_bc records).
 //
-//   driver_drop_in <case_dir> <out.bin> <precision 0|1|2> <scheme 0|1|2> <n_steps>
+//   driver_drop_in <case_dir> <out.bin> <precision 0|1|2> <scheme 0|1|2> <n_steps> [layout 0|1]
 //
-// out.bin: per block bv, yk, cv (doubles), then the residual of the last step.
+// layout 1 hands the state to the library and reads it back in the
+// reference's VectorField3D order (component fastest, CC_LAYOUT_POINT_MAJOR):
+// the initial state is set again that way before initialize_computation.
+// out.bin: per block bv, yk, cv (doubles, field-major), then the residual of
+// the last step.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
 #include <sstream>
 
 #include "cfd_b200.hpp"
+
+// [nf][ng] <-> [ng][nf]
+static std::vector<double> transpose(const std::vector<double> &a, size_t nf, bool to_point_major) {
+  const size_t ng = nf ? a.size() / nf : 0;
+  std::vector<double> t(a.size());
+  for (size_t p = 0; p < ng; ++p)
+    for (size_t f = 0; f < nf; ++f) {
+      if (to_point_major)
+        t[p * nf + f] = a[f * ng + p];
+      else
+        t[f * ng + p] = a[p * nf + f];
+    }
+  return t;
+}
 
 static std::vector<double> read_doubles(std::ifstream &f, size_t n) {
   std::vector<double> v(n);
@@ -24,10 +42,11 @@ static std::vector<double> read_doubles(std::ifstream &f, size_t n) {
 }
 
 int main(int argc, char **argv) {
-  if (argc != 6) {
-    std::fprintf(stderr, "usage: %s case_dir out.bin precision scheme n_steps\n", argv[0]);
+  if (argc != 6 && argc != 7) {
+    std::fprintf(stderr, "usage: %s case_dir out.bin precision scheme n_steps [layout]\n", argv[0]);
     return 2;
   }
+  const int layout = argc == 7 ? std::atoi(argv[6]) : CC_LAYOUT_FIELD_MAJOR;
   const std::string dir = argv[1];
   try {
     cfd::Parameter parameter;
@@ -86,6 +105,10 @@ int main(int argc, char **argv) {
     }
 
     cfd::Driver driver(parameter, mesh, chem, std::atoi(argv[3]));
+    if (layout == CC_LAYOUT_POINT_MAJOR)
+      for (size_t b = 0; b < mesh.blocks.size(); ++b)
+        driver.field[b].set_state(transpose(mesh.blocks[b].bv, 6, true), transpose(mesh.blocks[b].yk, ns, true),
+                                  CC_LAYOUT_POINT_MAJOR);
     driver.initialize_computation();
     driver.simulate(std::atoi(argv[5]), std::atoi(argv[4]), true);
     if (driver.status() != 0) throw std::runtime_error("device status word set");
@@ -93,7 +116,12 @@ int main(int argc, char **argv) {
     std::ofstream out(argv[2], std::ios::binary);
     std::vector<double> bv, yk, cv;
     for (auto &fld : driver.field) {
-      fld.get_state(bv, yk, cv);
+      fld.get_state(bv, yk, cv, layout);
+      if (layout == CC_LAYOUT_POINT_MAJOR) {
+        bv = transpose(bv, 6, false);
+        yk = transpose(yk, ns, false);
+        cv = transpose(cv, 5 + ns, false);
+      }
       out.write(reinterpret_cast<const char *>(bv.data()), (std::streamsize)(bv.size() * sizeof(double)));
       out.write(reinterpret_cast<const char *>(yk.data()), (std::streamsize)(yk.size() * sizeof(double)));
       out.write(reinterpret_cast<const char *>(cv.data()), (std::streamsize)(cv.size() * sizeof(double)));

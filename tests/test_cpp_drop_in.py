@@ -73,15 +73,19 @@ CASES = {
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision,scheme", [("fp64", "rk3"), ("mixed", "lusgs"), ("fp64", "steady")])
+@pytest.mark.parametrize("precision,scheme,layout",
+                         [("fp64", "rk3", 0), ("mixed", "lusgs", 0), ("fp64", "steady", 0), ("mixed", "rk3", 1)])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_cpp_driver_equals_python_driver(name, precision, scheme, tmp_path):
+def test_cpp_driver_equals_python_driver(name, precision, scheme, layout, tmp_path):
+    """layout 1: the C++ program sets and reads the state in the reference's
+    VectorField3D order (CC_LAYOUT_POINT_MAJOR) and must still get the Python
+    driver's field-major state bit for bit."""
     case = CASES[name]()
     exe = compile_driver(tmp_path)
     dump_case(case, str(tmp_path / "case"))
     out = str(tmp_path / "out.bin")
-    r = subprocess.run([exe, str(tmp_path / "case"), out, str(cc.PRECISIONS[precision]), str(cc.SCHEMES[scheme]), "3"],
-                       capture_output=True, text=True, timeout=600)
+    r = subprocess.run([exe, str(tmp_path / "case"), out, str(cc.PRECISIONS[precision]), str(cc.SCHEMES[scheme]), "3",
+                        str(layout)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     got = np.fromfile(out, dtype=np.float64)
     d = cc.Driver.from_case(case, precision)

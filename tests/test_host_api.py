@@ -76,7 +76,26 @@ def test_invalid_parameters_are_rejected(cclib):
     bid = ctypes.c_int()
     assert cclib.cc_add_block(ctx, 0, 4, 4, cc._ptr(jac), cc._ptr(met), ctypes.byref(bid)) == -1
     assert cclib.cc_step(ctx, 1, 0, 0) == -2  # before cc_init
+    # a state layout that is neither field- nor point-major
+    assert cclib.cc_add_block(ctx, 4, 4, 4, cc._ptr(jac), cc._ptr(met), ctypes.byref(bid)) == 0
+    bv = np.ones(6 * 8 * 8 * 8)
+    assert cclib.cc_set_state(ctx, bid.value, cc._ptr(bv), None, 2) == -1
+    assert b"layout" in cclib.cc_last_error()
+    assert cclib.cc_set_state(ctx, bid.value, cc._ptr(bv), None, 1) == 0
     assert cclib.cc_destroy(ctx) == 0
+
+
+def test_state_layout_names(cclib):
+    """The Python mirror takes the layout by name: "field" ([n_field][Ng]) or
+    "point" ([Ng][n_field], the reference's VectorField3D order); the
+    point-major arrays reach the library before cc_init without a device."""
+    case = cases.case_sod(8, 5, 5)
+    blk = case["blocks"][0]
+    d = cc.Driver.from_case(case)
+    d.field[0].set_state(np.ascontiguousarray(blk["bv"].T), None, layout="point")
+    with pytest.raises(ValueError):
+        d.field[0].set_state(blk["bv"], None, layout="aos")
+    d.close()
 
 
 def test_struct_layouts_match_reference_pods():
