@@ -405,10 +405,11 @@ class Driver:
         precision's default (mixed on, FP64 off)."""
         _check(self.lib.cc_set_renormalize(self.ctx, -1 if enable is None else (1 if enable else 0)))
 
-    def set_wait_limit(self, spins=0):
-        """Polls of a device-side wait before the kernel gives up and sets its
-        status bit; 0 restores the default."""
-        _check(self.lib.cc_set_wait_limit(self.ctx, int(spins)))
+    def set_wait_limit(self, spins=None):
+        """Polls of a device-side wait (after one non-blocking check) before
+        the kernel gives up and sets its status bit; None restores the
+        default."""
+        _check(self.lib.cc_set_wait_limit(self.ctx, -1 if spins is None else int(spins)))
 
     def set_newton_max_iter(self, n=0):
         """Iteration cap of the temperature Newton; 0 restores the

@@ -1385,7 +1385,7 @@ int cc_set_renormalize(cc_ctx *c, int enable) {
 
 int cc_set_wait_limit(cc_ctx *c, int64_t spins) {
   if (int r = check_ctx(c)) return r;
-  c->chem.max_spins = spins > 0 ? (long long)spins : kDefaultWaitSpins;
+  c->chem.max_spins = spins >= 0 ? (long long)spins : kDefaultWaitSpins;
   destroy_graphs(c);  // the captured launches carry the parameters by value
   return 0;
 }

@@ -80,6 +80,17 @@ __device__ __forceinline__ bool mlp_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
+// non-blocking check of the same phase
+__device__ __forceinline__ bool mlp_test_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mlp_smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // x * sigmoid(x) with the hardware exponential and division (relative error
 // ~1e-7, far below the BF16 rounding of the activations that follows)
 __device__ __forceinline__ float mlp_silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
@@ -200,11 +211,10 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
                          mlp_smem_u32(bar))
                      : "memory");
       }
-      long long spins = 0;
-      while (!mlp_try_wait(bar, phase))
-        if (++spins > C.max_spins) break;
+      bool ok = mlp_test_wait(bar, phase);
+      for (long long s = 0; !ok && s < C.max_spins; ++s) ok = mlp_try_wait(bar, phase);
       phase ^= 1u;
-      if (__syncthreads_or(spins > C.max_spins)) {
+      if (__syncthreads_or(!ok)) {
         late = true;
         break;
       }

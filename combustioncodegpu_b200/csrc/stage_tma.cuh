@@ -53,6 +53,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
   return ok != 0;
 }
 
+// Non-blocking check of the same phase (no suspension).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for a phase: one non-blocking check, then at most max_polls
+// potentially suspending polls (a limit of 0 gives up unless the phase has
+// already completed).  Returns false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, long long max_polls) {
+  bool ok = mbar_test_wait(bar, parity);
+  for (long long s = 0; !ok && s < max_polls; ++s) ok = mbar_try_wait(bar, parity);
+  return ok;
+}
+
 // One plane: box {kHX, kHY, 1, nf} at (x, y, z, 0) of the block's tensor map.
 __device__ __forceinline__ void tma_load_plane(void *dst, const CUtensorMap *map, int x, int y, int z,
                                                uint64_t *bar) {
@@ -181,15 +203,8 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
   for (int k = t.k0 - 1; k < t.k1; ++k) {
     // planes k-1 .. k+2 must be resident
     bool late = false;
-    for (int kp = k - 1; kp <= k + 2; ++kp) {
-      long long spins = 0;
-      while (!mbar_try_wait(&bars[slot_of(kp)], parity_of(kp))) {
-        if (++spins > C.max_spins) {
-          late = true;
-          break;
-        }
-      }
-    }
+    for (int kp = k - 1; kp <= k + 2 && !late; ++kp)
+      late = !mbar_wait_bounded(&bars[slot_of(kp)], parity_of(kp), C.max_spins);
     if (__syncthreads_or(late)) {
       if (tid == 0) atomicOr(a.status, kStatusTmaTimeout);
       aborted = true;
@@ -396,14 +411,8 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
   aborted = false;
   for (int k = t.k0; k < t.k1; ++k) {
     bool late = false;
-    for (int kp = k - 1; kp <= k + 2; ++kp) {
-      long long spins = 0;
-      while (!mbar_try_wait(&bars[slot_of(kp)], parity_of(kp)))
-        if (++spins > C.max_spins) {
-          late = true;
-          break;
-        }
-    }
+    for (int kp = k - 1; kp <= k + 2 && !late; ++kp)
+      late = !mbar_wait_bounded(&bars[slot_of(kp)], parity_of(kp), C.max_spins);
     if (__syncthreads_or(late)) {
       if (tid == 0) atomicOr(a.status, kStatusTmaTimeout);
       aborted = true;

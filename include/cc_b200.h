@@ -177,9 +177,11 @@ int cc_last_dt(cc_ctx *ctx, double *dt);
  * stops silently after 1000 iterations). */
 int cc_status(cc_ctx *ctx, unsigned *flags);
 /* No counterpart in the reference.  Polls of a device-side wait (a TMA plane,
- * a tensor-core completion) before the kernel gives up on it, sets its status
- * bit (3 or 4) and returns; the context stays usable.  spins <= 0 restores the
- * default (2^22).  Takes effect at the next cc_step. */
+ * a tensor-core completion) after its first non-blocking check, before the
+ * kernel gives up on it, sets its status bit (3 or 4) and returns; the
+ * context stays usable.  0 = give up unless the first check finds the data
+ * there; spins < 0 restores the default (2^22).  Takes effect at the next
+ * cc_step. */
 int cc_set_wait_limit(cc_ctx *ctx, int64_t spins);
 /* Iteration cap of the temperature Newton (Thermo.cu:103-121: 1000); a point
  * that reaches it sets status bit 0.  n <= 0 restores 1000.  Takes effect at
