@@ -48,10 +48,12 @@ def parse():
                          "box256_closure: 256^3 box, exact transport vs the learned closure; "
                          "box128_lusgs: LU-SGS steady steps on the 128^3 box")
     ap.add_argument("--study-steps", default="100,1000,2000", help="mixing_layer: error snapshot steps")
-    ap.add_argument("--variant", default="auto", choices=["auto", "l1", "tma", "split", "split-tma", "split-tma-p"],
+    ap.add_argument("--variant", default="auto",
+                    choices=["auto", "l1", "tma", "split", "split-tma", "split-tma-p", "dq-tma"],
                     help="stage kernels: autotuned (default) or pinned (profiling runs, where the autotuner's "
                          "timings are distorted)")
     ap.add_argument("--kz", type=int, default=4, help="k-planes per tile when --variant pins the stage kernels")
+    ap.add_argument("--tile-j", type=int, default=0, help="points along j of the dq-tma tile when --variant pins it")
     return ap.parse_args()
 
 
@@ -141,12 +143,13 @@ def field_errors(b, b0):
     return out
 
 
-def face_kernel_bytes(ns, precision):
-    """Bytes per point of the split variant's face kernel: it reads the
-    primitives (6+ns), transport (2+ns) and geometry (10) once and writes three
-    faces of n_var fluxes, all at the bulk width."""
+def face_kernel_bytes(ns, precision, dq=False):
+    """Bytes per point of the face kernel: it reads the primitives (6+ns),
+    transport (2+ns) and geometry (10) once and writes three faces of n_var
+    fluxes (split variants) or the point's residual of n_var values (the dq
+    variant, which differences the faces inside its tile), at the bulk width."""
     w = 8 if precision == "fp64" else 4
-    return ((6 + ns) + (2 + ns) + 10 + 3 * (5 + ns)) * w
+    return ((6 + ns) + (2 + ns) + 10 + (1 if dq else 3) * (5 + ns)) * w
 
 
 def ncu_traffic(kernel_tag):
@@ -190,8 +193,9 @@ def run_ours(args, rank, world, dist):
     states = {}
     for prec in ("fp64", "mixed"):
         d = cc.Driver.from_case(case, prec)
-        if args.variant != "auto":  # the fused TMA variant exists in the FP32 bulk precision only
-            d.set_tuning("l1" if prec == "fp64" and args.variant == "tma" else args.variant, args.kz)
+        if args.variant != "auto":  # the fused TMA and dq variants exist in the FP32 bulk precision only
+            fp32_only = args.variant in ("tma", "dq-tma")
+            d.set_tuning("split-tma-p" if prec == "fp64" and fp32_only else args.variant, args.kz, args.tile_j)
         d.initialize_computation()
         s = torch.cuda.ExternalStream(d.stream())
         info = d.info()
@@ -251,7 +255,7 @@ def run_ours(args, rank, world, dist):
         bv_h, yk_h = pin(blk["bv"]), pin(blk["yk"])
         d = cc.Driver.from_case(case, "mixed")
         if args.variant != "auto":
-            d.set_tuning(args.variant, args.kz)
+            d.set_tuning(args.variant, args.kz, args.tile_j)
         d.initialize_computation()
         d.simulate(2)
         d.sync()
@@ -567,10 +571,16 @@ def main():
     bpp = algorithmic_bytes(9, "mixed")
     kt = mixed["kernels"]
     stage_ms = kt["stage_ms"]
-    split = mixed["tuning"]["variant"] in ("split", "split-tma", "split-tma-p")
+    variant = mixed["tuning"]["variant"]
+    split = variant in ("split", "split-tma", "split-tma-p", "dq-tma")
     stage_achieved = bpp * mixed["npts"] / (stage_ms / 1e3) / 1e9
-    if split:  # dominant kernel: the face kernel
-        tma = mixed["tuning"]["variant"] in ("split-tma", "split-tma-p")
+    if variant == "dq-tma":  # dominant kernel: the face kernel that writes dq
+        ty = mixed["tuning"]["tile"][1]
+        kname = "k_faces_dq<float,9,%d,%d>" % (ty, {4: 2, 8: 3, 16: 1}[ty])
+        kbpp, kms = face_kernel_bytes(9, "mixed", dq=True), kt["faces_ms"]
+        traffic = ncu_traffic("faces_dq_kernel_box128_mixed")
+    elif split:  # dominant kernel: the face kernel
+        tma = variant in ("split-tma", "split-tma-p")
         kname = "k_faces_tma<float,9>" if tma else "k_faces<float,9>"
         kbpp, kms = face_kernel_bytes(9, "mixed"), kt["faces_ms"]
         traffic = ncu_traffic("faces_tma_kernel_box128_mixed" if tma else "faces_kernel_box128_mixed")
@@ -582,7 +592,7 @@ def main():
     levels = mixed["info"]["halo_levels"]
     # per stage: stage kernels, halo node levels, halo copies; per step: the
     # third stage's post-exchange dt of rewritten interior points, dt finalize
-    n_stage = {"l1": 1, "tma": 1, "split": 2, "split-tma": 3, "split-tma-p": 3}[mixed["tuning"]["variant"]]
+    n_stage = {"l1": 1, "tma": 1, "split": 2, "split-tma": 3, "split-tma-p": 3, "dq-tma": 2}[variant]
     launches_per_step = 3 * (n_stage + levels + 1) + 2
     line = {
         "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,

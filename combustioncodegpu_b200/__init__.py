@@ -29,7 +29,7 @@ MAX_SPECIES = 16
 CC_FP64, CC_MIXED, CC_FP32 = 0, 1, 2
 CC_RK3, CC_STEADY_EULER, CC_STEADY_LUSGS = 0, 1, 2
 PRECISIONS = {"fp64": CC_FP64, "mixed": CC_MIXED, "fp32": CC_FP32}
-VARIANTS = ("l1", "tma", "split", "split-tma", "split-tma-p")  # stage-kernel variants, cc_tuning order
+VARIANTS = ("l1", "tma", "split", "split-tma", "split-tma-p", "dq-tma")  # stage-kernel variants, cc_tuning order
 SCHEMES = {"rk3": CC_RK3, "steady": CC_STEADY_EULER, "lusgs": CC_STEADY_LUSGS}
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -105,8 +105,9 @@ EXPORTS = {
     "cc_info": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "cc_time_kernels": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp], ctypes.c_int),
-    "cc_tuning": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _dp], ctypes.c_int),
-    "cc_set_tuning": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "cc_tuning": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _dp,
+                   ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "cc_set_tuning": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "cc_set_launch_mode": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_set_closure": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "cc_use_closure": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
@@ -440,16 +441,20 @@ class Driver:
         """Stage-kernel configuration in use: variant ("l1" fused with L1
         stencil reads, "tma" fused with TMA-staged planes, "split" face and
         update kernels, "split-tma" the same with TMA-staged planes in the
-        face kernel), k-planes per tile, measured ms per stage."""
+        face kernel, "split-tma-p" on persistent CTAs, "dq-tma" a face kernel
+        that differences the faces inside its tile), k-planes per tile, the
+        face kernel's tile (i, j, k) in points, measured ms per stage."""
         v, kz, ms = ctypes.c_int(), ctypes.c_int(), np.zeros(1)
-        _check(self.lib.cc_tuning(self.ctx, ctypes.byref(v), ctypes.byref(kz), _ptr(ms)))
-        return {"variant": VARIANTS[v.value], "kz": kz.value, "stage_ms": float(ms[0])}
+        tile = (ctypes.c_int * 3)()
+        _check(self.lib.cc_tuning(self.ctx, ctypes.byref(v), ctypes.byref(kz), _ptr(ms), tile))
+        return {"variant": VARIANTS[v.value], "kz": kz.value, "stage_ms": float(ms[0]), "tile": tuple(tile)}
 
-    def set_tuning(self, variant="auto", kz=0):
-        """Pin the stage-kernel configuration: variant "auto", "l1", "tma",
-        "split" or "split-tma"; kz k-planes per tile (0 = autotune)."""
+    def set_tuning(self, variant="auto", kz=0, tile_j=0):
+        """Pin the stage-kernel configuration: variant "auto" or one of
+        VARIANTS; kz k-planes per tile (0 = autotune); tile_j points along j
+        of the "dq-tma" tile (4, 8, 16; 0 = autotune)."""
         v = (-1 if variant == "auto" else VARIANTS.index(variant)) if isinstance(variant, str) else int(variant)
-        _check(self.lib.cc_set_tuning(self.ctx, v, int(kz)))
+        _check(self.lib.cc_set_tuning(self.ctx, v, int(kz), int(tile_j)))
 
     def set_launch_mode(self, mode="batched"):
         """"batched": one launch per stage kernel over all blocks;

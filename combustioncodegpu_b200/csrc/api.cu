@@ -101,7 +101,13 @@ struct cc_ctx {
   uint32_t *d_skip_dt = nullptr;  // bitmask: interior points the halo rewrites
   int renorm = -1;                // Y renormalisation: -1 = by precision (mixed on, FP64 off)
   int variant = 0;                // stage kernels: 0 fused (L1 stencil reads), 1 fused TMA planes, 2 split faces/update,
-                                  // 3 split with TMA-staged face planes, 4 the same on persistent CTAs
+                                  // 3 split with TMA-staged face planes, 4 the same on persistent CTAs,
+                                  // 5 face kernel differencing in the tile (dq) + update
+  int dq_ty = 8;                  // variant 5: tile height of the dq face kernel (32 x dq_ty points x kz)
+  int force_ty = 0;               // cc_set_tuning: dq tile height, 0 = autotune
+  std::vector<Tile> hdq;          // variant 5: tiles of the dq face kernel
+  std::vector<int> dq_begin;      // per block: first dq tile (block-ordered list), + end
+  Tile *d_dqtiles = nullptr;
   std::vector<Tile> hedges;       // split variant: tiles of the minus-side face layers
   std::vector<int> tile_begin, edge_begin;  // per block: first tile / edge tile (lists are block-ordered), + end
   bool per_block = false;         // cc_set_launch_mode: one launch per block per kernel instead of one per stage
@@ -116,7 +122,8 @@ struct cc_ctx {
   double *d_gcl = nullptr;        // [3][N] geometric term of the gauge-pressure momentum fluxes
   int kz = 1;                     // k-chunk of the stage tiles
   double tuned_ms = 0;            // stage-kernel time of the chosen configuration
-  CUtensorMap *d_tmaps = nullptr; // [2][n_blocks]: primitive arenas P[0], P[1] per block
+  CUtensorMap *d_tmaps = nullptr; // [3][2][n_blocks]: plane boxes of tile height 8, 4, 16 (kTmaRows) for the
+                                  // primitive arenas P[0], P[1] per block
   unsigned *d_ticket = nullptr;   // tile counter of the persistent face kernel
   LusgsArgs lu{};                 // LU-SGS work arrays (allocated by the first LU-SGS step)
   std::vector<int64_t> lu_hb;     // sweep positions where each hyperplane begins, + end
@@ -255,6 +262,37 @@ void transpose_fields(const double *src, int64_t ng, int nf, std::vector<double>
     }
 }
 
+// Tensor-map plane boxes: tile heights 8 (the kTY tiles of the split and
+// fused kernels, and the dq kernel), 4 and 16 (dq kernel), each plus the
+// 2-point halo on both sides.
+constexpr int kTmaTileRows[3] = {8, 4, 16};
+int tma_shape(int ty) { return ty == 4 ? 1 : (ty == 16 ? 2 : 0); }
+
+// Work list of the dq face kernel: 32 x ty columns, k split into chunks of kz.
+void build_dq_tiles(cc_ctx *c, int ty, int kz) {
+  c->hdq.clear();
+  c->dq_begin.clear();
+  for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
+    c->dq_begin.push_back((int)c->hdq.size());
+    const auto &b = c->blocks[bi];
+    for (int k0 = 0; k0 < b.mz; k0 += kz)
+      for (int j0 = 0; j0 < b.my; j0 += ty)
+        for (int i0 = 0; i0 < b.mx; i0 += 32) {
+          Tile t{};
+          t.blk = bi, t.i0 = i0, t.j0 = j0, t.k0 = k0, t.k1 = std::min(b.mz, k0 + kz);
+          c->hdq.push_back(t);
+        }
+  }
+  c->dq_begin.push_back((int)c->hdq.size());
+  c->dq_ty = ty;
+}
+
+int max_dq_tiles(cc_ctx *c) {
+  int64_t n = 0;
+  for (const auto &b : c->blocks) n += (int64_t)((b.mx + 31) / 32) * ((b.my + 3) / 4) * b.mz;
+  return (int)n;
+}
+
 // Stage-kernel work list: kTX x kTY columns, k split into chunks of kz.
 void build_tiles_kz(cc_ctx *c, int kz) {
   c->htiles.clear();
@@ -348,17 +386,19 @@ int build_tensor_maps(cc_ctx *c) {
   if (!fn || q != cudaDriverEntryPointSuccess) return fail(CC_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   auto encode = reinterpret_cast<EncodeTiledFn>(fn);
   const int nb = (int)c->blocks.size();
-  std::vector<CUtensorMap> maps(2 * (size_t)nb);
+  std::vector<CUtensorMap> maps(3 * 2 * (size_t)nb);
   const size_t E = c->elem;
+  for (int shape = 0; shape < 3; ++shape)
   for (int buf = 0; buf < 2; ++buf)
     for (int b = 0; b < nb; ++b) {
       const HostBlock &h = c->blocks[b];
       const cuuint64_t dims[4] = {(cuuint64_t)h.nx, (cuuint64_t)h.ny, (cuuint64_t)h.nz, (cuuint64_t)np_of(c)};
       const cuuint64_t strides[3] = {(cuuint64_t)h.nx * E, (cuuint64_t)h.nx * h.ny * E, (cuuint64_t)c->N * E};
-      const cuuint32_t box[4] = {(cuuint32_t)(kTX + 4), (cuuint32_t)(kTY + 4), 1u, (cuuint32_t)np_of(c)};
+      const cuuint32_t box[4] = {(cuuint32_t)(kTX + 4), (cuuint32_t)(kTmaTileRows[shape] + 4), 1u,
+                                 (cuuint32_t)np_of(c)};
       const cuuint32_t estr[4] = {1, 1, 1, 1};
       void *base = (char *)c->P[buf] + (size_t)h.off * E;
-      CUresult r = encode(&maps[(size_t)buf * nb + b],
+      CUresult r = encode(&maps[((size_t)shape * 2 + buf) * nb + b],
                           E == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -422,6 +462,10 @@ int setup_device(cc_ctx *c) {
   c->d_blocks = (BlockInfo *)p;
   if (dev_alloc(c, &p, sizeof(Tile) * (size_t)std::max(1, max_tiles(c)))) return CC_ERR_CUDA;
   c->d_tiles = (Tile *)p;
+  if (dev_alloc(c, &p, sizeof(Tile) * (size_t)std::max(1, max_dq_tiles(c)))) return CC_ERR_CUDA;
+  c->d_dqtiles = (Tile *)p;
+  build_dq_tiles(c, c->dq_ty, c->kz);
+  CK(cudaMemcpyAsync(c->d_dqtiles, c->hdq.data(), sizeof(Tile) * c->hdq.size(), cudaMemcpyHostToDevice, c->stream));
   for (int b = 0; b < 2; ++b) {
     if (dev_alloc(c, &c->P[b], E * N * np_of(c))) return CC_ERR_CUDA;
     if (dev_alloc(c, &c->Pr[b], E * N * npr_of(c))) return CC_ERR_CUDA;
@@ -653,41 +697,56 @@ int prof_event(cc_ctx *c, std::vector<cudaEvent_t> &pool, size_t &next) {
   return 0;
 }
 
-const char *const kVariantName[5] = {"fused-l1", "fused-tma", "split", "split-tma", "split-tma-persistent"};
+const char *const kVariantName[6] = {"fused-l1", "fused-tma", "split", "split-tma", "split-tma-persistent",
+                                     "dq-tma"};
 
 // Variants this context can run: the TMA-staged ones need the tensor maps
 // (0 or 9 species); the fused TMA kernel's planes and flux planes fit in
 // shared memory in the FP32 bulk precision only.
 bool variant_ok(const cc_ctx *c, int v) {
   if (v == 3 || v == 4) return c->tma_ok;
-  if (v == 1) return c->tma_ok && c->precision != CC_FP64;
+  if (v == 1 || v == 5) return c->tma_ok && c->precision != CC_FP64;
   return v == 0 || v == 2;
 }
 
 // One stage's kernels of the given variant over the current tile list:
 // one launch per kernel over all blocks, or (per_block) one per block.
 template <typename T, int NS>
-int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge);
+int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge, const Tile *dq_tiles,
+                       int n_dq);
 
 template <typename T, int NS>
 int launch_stage(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt) {
   if (!c->per_block || c->tile_begin.size() != c->blocks.size() + 1)
-    return launch_stage_range<T, NS>(c, a, pc, variant, nt, (int)c->hedges.size());
+    return launch_stage_range<T, NS>(c, a, pc, variant, nt, (int)c->hedges.size(), c->d_dqtiles,
+                                     (int)c->hdq.size());
   const Tile *tiles = a.tiles;
   for (size_t b = 0; b < c->blocks.size(); ++b) {
     a.tiles = tiles + c->tile_begin[b];
     a.edge_tiles = c->d_edges + c->edge_begin[b];
     if (int r = launch_stage_range<T, NS>(c, a, pc, variant, c->tile_begin[b + 1] - c->tile_begin[b],
-                                          c->edge_begin[b + 1] - c->edge_begin[b]))
+                                          c->edge_begin[b + 1] - c->edge_begin[b], c->d_dqtiles + c->dq_begin[b],
+                                          c->dq_begin[b + 1] - c->dq_begin[b]))
       return r;
   }
   return 0;
 }
 
 template <typename T, int NS>
-int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge) {
-  if ((variant == 1 || variant == 3 || variant == 4) && !c->d_tmaps)
+int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge, const Tile *dq_tiles,
+                       int n_dq) {
+  if ((variant == 1 || variant == 3 || variant == 4 || variant == 5) && !c->d_tmaps)
     return fail(CC_ERR_STATE, "TMA variant without tensor maps");
+  if (variant == 5) {  // faces differenced in the tile (dq), then the update
+    a.faces = (T *)c->faces;
+    a.dq_direct = 1;
+    const size_t nb = c->blocks.size();
+    CK((Launch<T, NS>::faces_dq(a, dq_tiles, c->d_tmaps + ((size_t)tma_shape(c->dq_ty) * 2 + pc) * nb, c->chem,
+                                n_dq, c->dq_ty, c->stream)));
+    if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
+    CK((Launch<T, NS>::update(a, c->chem, nt, c->stream)));
+    return 0;
+  }
   if (variant == 1) {
     CK((Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
   } else if (variant == 2 || variant == 3 || variant == 4) {
@@ -873,39 +932,52 @@ int autotune(cc_ctx *c) {
   double best = 1e300;
   int best_kz = c->kz;
   int best_variant = 0;
+  int best_ty = c->dq_ty;
   if (c->force_kz > 0) kzs.assign(1, c->force_kz);
   std::vector<int> variants;
   if (c->force_variant >= 0 && !variant_ok(c, c->force_variant))
-    return fail(CC_ERR_ARG, "the TMA variants need 0 or 9 species, the fused one also the FP32 bulk precision "
-                            "(cc_set_tuning)");
+    return fail(CC_ERR_ARG, "the TMA variants need 0 or 9 species, the fused and dq ones also the FP32 bulk "
+                            "precision (cc_set_tuning)");
   if (c->force_variant >= 0)
     variants.push_back(c->force_variant);
   else
-    for (int v : {0, 1, 2, 3, 4})
+    for (int v : {0, 1, 2, 3, 4, 5})
       if (variant_ok(c, v)) variants.push_back(v);
+  // tile heights of the dq face kernel (variant 5; the other variants' tiles are 32 x 8)
+  std::vector<int> tys = {4, 8, 16};
+  if (c->force_ty > 0) tys.assign(1, c->force_ty);
   for (int variant : variants) {
-    for (int kz : kzs) {
-      build_tiles_kz(c, kz);
-      CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
-                         c->stream));
-      const int nt = (int)c->htiles.size();
-      if (int r = launch_stage<T, NS>(c, a, pc, variant, nt)) return r;
-      CK(cudaEventRecord(e0, c->stream));
-      for (int r = 0; r < 3; ++r)
-        if (int rr = launch_stage<T, NS>(c, a, pc, variant, nt)) return rr;
-      CK(cudaEventRecord(e1, c->stream));
-      CK(cudaEventSynchronize(e1));
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, e0, e1));
-      if (verbose)
-        std::fprintf(stderr, "cc autotune: %s kz=%d tiles=%d %.4f ms\n", kVariantName[variant], kz, nt, ms / 3);
-      if (ms / 3 < best) best = ms / 3, best_kz = kz, best_variant = variant;
+    for (int ty : (variant == 5 ? tys : std::vector<int>{8})) {
+      for (int kz : kzs) {
+        build_tiles_kz(c, kz);
+        CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
+                           c->stream));
+        build_dq_tiles(c, ty, kz);
+        CK(cudaMemcpyAsync(c->d_dqtiles, c->hdq.data(), sizeof(Tile) * c->hdq.size(), cudaMemcpyHostToDevice,
+                           c->stream));
+        const int nt = (int)c->htiles.size();
+        if (int r = launch_stage<T, NS>(c, a, pc, variant, nt)) return r;
+        CK(cudaEventRecord(e0, c->stream));
+        for (int r = 0; r < 3; ++r)
+          if (int rr = launch_stage<T, NS>(c, a, pc, variant, nt)) return rr;
+        CK(cudaEventRecord(e1, c->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (verbose)
+          std::fprintf(stderr, "cc autotune: %s tile 32x%dx%d tiles=%d %.4f ms\n", kVariantName[variant],
+                       variant == 5 ? ty : kTY, kz, variant == 5 ? (int)c->hdq.size() : nt, ms / 3);
+        if (ms / 3 < best) best = ms / 3, best_kz = kz, best_variant = variant, best_ty = ty;
+      }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   build_tiles_kz(c, best_kz);
   CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
+                     c->stream));
+  build_dq_tiles(c, best_variant == 5 ? best_ty : 8, best_kz);
+  CK(cudaMemcpyAsync(c->d_dqtiles, c->hdq.data(), sizeof(Tile) * c->hdq.size(), cudaMemcpyHostToDevice,
                      c->stream));
   c->variant = best_variant;
   c->tuned_ms = best;
@@ -1466,26 +1538,34 @@ int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[6]) {
   return 0;
 }
 
-int cc_tuning(cc_ctx *c, int *variant, int *kz, double *stage_ms) {
+int cc_tuning(cc_ctx *c, int *variant, int *kz, double *stage_ms, int tile[3]) {
   if (int r = check_ctx(c)) return r;
   if (variant) *variant = c->variant;
   if (kz) *kz = c->kz;
   if (stage_ms) *stage_ms = c->tuned_ms;
+  if (tile) {
+    tile[0] = kTX;
+    tile[1] = c->variant == 5 ? c->dq_ty : kTY;
+    tile[2] = c->kz;
+  }
   return 0;
 }
 
-int cc_set_tuning(cc_ctx *c, int variant, int kz) {
+int cc_set_tuning(cc_ctx *c, int variant, int kz, int tile_j) {
   if (int r = check_ctx(c)) return r;
-  if (variant < -1 || variant > 4)
+  if (variant < -1 || variant > 5)
     return fail(CC_ERR_ARG,
-                "variant must be -1 (autotune), 0 (fused, L1), 1 (fused, TMA), 2 (split), 3 (split, TMA faces) or 4 "
-                "(split, TMA faces on persistent CTAs)");
+                "variant must be -1 (autotune), 0 (fused, L1), 1 (fused, TMA), 2 (split), 3 (split, TMA faces), 4 "
+                "(split, TMA faces on persistent CTAs) or 5 (faces differenced in the tile)");
   if (kz < 0) return fail(CC_ERR_ARG, "kz must be >= 0");
+  if (tile_j != 0 && tile_j != 4 && tile_j != 8 && tile_j != 16)
+    return fail(CC_ERR_ARG, "tile_j must be 0 (autotune), 4, 8 or 16");
   c->force_variant = variant;
   c->force_kz = kz;
+  c->force_ty = tile_j;
   if (!c->initialized) return 0;
   if (!variant_ok(c, variant))
-    return fail(CC_ERR_ARG, "the TMA variants need 0 or 9 species, the fused one also the FP32 bulk precision");
+    return fail(CC_ERR_ARG, "the TMA variants need 0 or 9 species, the fused and dq ones also the FP32 bulk precision");
   destroy_graphs(c);
   int r = dispatch(c, [&](auto tt, auto nn) { return autotune<typename decltype(tt)::type, decltype(nn)::value>(c); });
   if (r) return r;

@@ -159,6 +159,9 @@ struct StageArgs {
   T *faces;
   const Tile *edge_tiles;
   int n_regular;
+  // 1: `faces` holds the residual dq [n_var][N] of every interior point
+  // (k_faces_dq), which k_update reads as it is instead of differencing faces
+  int dq_direct;
 };
 
 // Work arrays of the LU-SGS steady step (lusgs.cuh), in sweep order: the

@@ -6,6 +6,7 @@
 #include "stage.cuh"
 #include "stage_tma.cuh"
 #include "stage_split.cuh"
+#include "stage_dq.cuh"
 #include "closure.cuh"
 #include "lusgs.cuh"
 
@@ -53,6 +54,40 @@ cudaError_t Launch<T, NS>::faces_tma(const StageArgs<T> &a, const void *maps, co
   if (faces_tma_smem() > 227 * 1024) return cudaErrorInvalidConfiguration;
   k_faces_tma<T, NS><<<n_tiles, dim3(kTX, kTY), faces_tma_smem(), s>>>(a, (const CUtensorMap *)maps, C);
   return cudaGetLastError();
+}
+
+// y-exchange rounds of the dq face kernel per tile height (shared memory)
+template <int TY>
+struct DqChunks {
+  static constexpr int value = TY == 4 ? 2 : (TY == 8 ? 3 : 1);
+};
+
+template <typename T, int NS>
+size_t Launch<T, NS>::faces_dq_smem(int ty) {
+  if (ty == 4) return FacesDqLayout<T, NS, 4, DqChunks<4>::value>::kBytes;
+  if (ty == 8) return FacesDqLayout<T, NS, 8, DqChunks<8>::value>::kBytes;
+  return FacesDqLayout<T, NS, 16, DqChunks<16>::value>::kBytes;
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::faces_dq(const StageArgs<T> &a, const Tile *tiles, const void *maps, const ChemParams &C,
+                                    int n_tiles, int ty, cudaStream_t s) {
+  if constexpr (sizeof(T) != 4 || NS < 0) {
+    return cudaErrorInvalidValue;  // FP32 bulk precision, compiled species counts only
+  } else {
+    if (n_tiles <= 0) return cudaSuccess;
+    if (faces_dq_smem(ty) > 227 * 1024) return cudaErrorInvalidConfiguration;
+    const CUtensorMap *m = (const CUtensorMap *)maps;
+    if (ty == 4)
+      k_faces_dq<T, NS, 4, DqChunks<4>::value><<<n_tiles, dim3(32, 4), faces_dq_smem(4), s>>>(a, tiles, m, C);
+    else if (ty == 8)
+      k_faces_dq<T, NS, 8, DqChunks<8>::value><<<n_tiles, dim3(32, 8), faces_dq_smem(8), s>>>(a, tiles, m, C);
+    else if (ty == 16)
+      k_faces_dq<T, NS, 16, DqChunks<16>::value><<<n_tiles, dim3(32, 16), faces_dq_smem(16), s>>>(a, tiles, m, C);
+    else
+      return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
 }
 
 template <typename T, int NS>
@@ -122,6 +157,17 @@ cudaError_t Launch<T, NS>::configure() {
   if (e == cudaSuccess && faces_tma_smem() <= 227 * 1024)
     e = cudaFuncSetAttribute(k_faces_tma_persistent<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)faces_tma_smem());
+  if constexpr (sizeof(T) == 4 && NS >= 0) {
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_faces_dq<T, NS, 4, DqChunks<4>::value>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)faces_dq_smem(4));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_faces_dq<T, NS, 8, DqChunks<8>::value>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)faces_dq_smem(8));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_faces_dq<T, NS, 16, DqChunks<16>::value>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)faces_dq_smem(16));
+  }
   return e;
 }
 

@@ -27,6 +27,12 @@ struct Launch {
   static cudaError_t faces_tma(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
                                cudaStream_t s);
   // persistent form: resident CTAs take the n_tiles regular tiles from *ticket (zeroed here)
+  // face kernel that differences the faces in the tile and writes dq
+  // (stage_dq.cuh): tiles of 32 x ty points (ty = 4, 8, 16), FP32 bulk
+  // precision with 0 or 9 species only
+  static size_t faces_dq_smem(int ty);
+  static cudaError_t faces_dq(const StageArgs<T> &a, const Tile *tiles, const void *maps, const ChemParams &C,
+                              int n_tiles, int ty, cudaStream_t s);
   static cudaError_t faces_tma_persistent(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
                                           unsigned *ticket, cudaStream_t s);
   // learned transport closure (closure.cuh) over every arena point; cl is a ClosureDev

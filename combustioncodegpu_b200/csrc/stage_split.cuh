@@ -120,14 +120,20 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 2 : 3)
       const int p = col + sk * k;
       // dq = -(sum over directions of F(+1/2) - F(-1/2)), the fused kernel's order
       double dq[NV];
+      if (a.dq_direct) {  // dq differenced by the face kernel (k_faces_dq)
 #pragma unroll
-      for (int l = 0; l < NV; ++l) {
-        if (l < nv) {
-          const int o = l * N + p;
-          T acc = Fx[o] - Fx[o - 1];
-          acc += Fy[o] - Fy[o - sj];
-          if (three_d) acc += Fz[o] - Fz[o - sk];
-          dq[l] = -(double)acc;
+        for (int l = 0; l < NV; ++l)
+          if (l < nv) dq[l] = (double)Fx[l * N + p];
+      } else {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          if (l < nv) {
+            const int o = l * N + p;
+            T acc = Fx[o] - Fx[o - 1];
+            acc += Fy[o] - Fy[o - sj];
+            if (three_d) acc += Fz[o] - Fz[o - sk];
+            dq[l] = -(double)acc;
+          }
         }
       }
       double dt;

@@ -210,17 +210,22 @@ int cc_time_kernels(cc_ctx *ctx, int n_steps, int scheme, double out_ms[6]);
  * stage: variant 0 = fused stage kernel with L1 stencil reads, 1 = fused
  * with TMA-staged primitive planes, 2 = split (face kernel, then update
  * kernel), 3 = split with TMA-staged planes in the face kernel, 4 = as 3
- * with the face kernel on persistent CTAs taking tiles from a counter; kz =
- * k-planes per tile.  CC_AUTOTUNE=0 keeps the heuristic. */
-int cc_tuning(cc_ctx *ctx, int *variant, int *kz, double *stage_ms);
-/* No counterpart in the reference (its launch shapes are fixed).  Pins the
- * stage-kernel configuration instead of autotuning it: variant -1 = autotune,
- * 0 = fused with L1 stencil reads, 1 = fused with TMA-staged planes, 2 =
- * split faces / update, 3 = split with TMA-staged face planes (1 and 3: FP32
- * bulk precision with 0 or 9 species); kz = k-planes per tile, 0 = autotune.  Before cc_init it applies to
- * the first cc_init; after it, the new configuration is timed and used from
- * the next cc_step on. */
-int cc_set_tuning(cc_ctx *ctx, int variant, int kz);
+ * with the face kernel on persistent CTAs taking tiles from a counter, 5 =
+ * face kernel that differences the faces inside its tile and writes dq, then
+ * the update kernel; kz = k-planes per tile; tile (may be null) = the face
+ * kernel's tile {i, j, k} in points.  CC_AUTOTUNE=0 keeps the heuristic. */
+int cc_tuning(cc_ctx *ctx, int *variant, int *kz, double *stage_ms, int tile[3]);
+/* No counterpart in the reference (its launch shapes are fixed: 64-point
+ * pencils, TimeAdvanceFunc.cu:44-57).  Pins the stage-kernel configuration
+ * instead of autotuning it: variant -1 = autotune, 0 = fused with L1 stencil
+ * reads, 1 = fused with TMA-staged planes, 2 = split faces / update, 3 =
+ * split with TMA-staged face planes, 4 = as 3 on persistent CTAs, 5 = faces
+ * differenced in the tile (TMA variants: 0 or 9 species; 1 and 5: FP32 bulk
+ * precision); kz = k-planes per tile, 0 = autotune; tile_j = points along j
+ * of the variant-5 tile (4, 8 or 16; 0 = autotune; the other variants' tiles
+ * are 32 x 8).  Before cc_init it applies to the first cc_init; after it,
+ * the new configuration is timed and used from the next cc_step on. */
+int cc_set_tuning(cc_ctx *ctx, int variant, int kz, int tile_j);
 /* Launch granularity of the stage kernels: 0 (default) = one launch per
  * kernel over the tiles of every block; 1 = one launch per block per kernel,
  * the reference's granularity (Driver.cu:144-177 launches per block), kept for

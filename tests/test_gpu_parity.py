@@ -41,12 +41,12 @@ def _cases():
 CASES = _cases()
 
 
-def compare(case, scheme, n, precision, variant="auto", kz=0):
+def compare(case, scheme, n, precision, variant="auto", kz=0, tile_j=0):
     renorm = precision in ("mixed", "fp32") and case["params"].get("species") is not None
     o = Oracle(case)
     o.init()
     d = cc.Driver.from_case(case, precision)
-    d.set_tuning(variant, kz)
+    d.set_tuning(variant, kz, tile_j)
     d.initialize_computation()
     if variant != "auto":
         assert d.tuning()["variant"] == variant
@@ -102,8 +102,8 @@ def test_mixed_close_to_oracle(name, scheme):
 
 # Every stage-kernel variant on every case, with k-chunks that split the
 # sweep (kz=3) and that do not (kz=64).  The TMA variants exist for 0 or 9
-# species; the fused one for the FP32 bulk precision only.
-@pytest.mark.parametrize("variant", ["tma", "split-tma", "split-tma-p"])
+# species; the fused one and the dq one for the FP32 bulk precision only.
+@pytest.mark.parametrize("variant", ["tma", "split-tma", "split-tma-p", "dq-tma"])
 @pytest.mark.parametrize("kz", [3, 64])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_tma_variant_close_to_oracle(name, kz, variant):
@@ -134,6 +134,40 @@ def test_split_variant_mixed_close_to_oracle(name):
     assert not bad, errs
 
 
+@pytest.mark.parametrize("tile_j", [4, 8, 16])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_dq_variant_tile_shapes_close_to_oracle(name, tile_j):
+    """The face kernel that differences the faces inside its tile, at every
+    tile height (32 x 4, 32 x 8, 32 x 16 points, k-chunks of 3), steady and
+    RK3 steps against the oracle."""
+    for scheme in ("steady", "rk3"):
+        errs, status = compare(CASES[name], scheme, 2, "mixed", "dq-tma", 3, tile_j)
+        assert status == 0
+        tol = {"res": 5e-3, "dt": 1e-5}
+        bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-4)}
+        assert not bad, (scheme, errs)
+
+
+def test_dq_variant_tile_shape_and_chunking_are_bit_identical():
+    """Every face the dq kernel computes goes through one call site and every
+    point's residual is summed in one order, whichever tile or k-chunk the
+    point and its faces fall in: the state after two steps is the same for
+    every tile height and k-chunk, bit for bit."""
+    case = CASES["multiblock"]
+    out = []
+    for tile_j, kz in ((8, 1), (4, 2), (16, 64), (8, 3)):
+        d = cc.Driver.from_case(case, "mixed")
+        d.set_tuning("dq-tma", kz, tile_j)
+        d.initialize_computation()
+        assert d.tuning()["tile"] == (32, tile_j, kz)
+        d.simulate(2, "rk3")
+        out.append([d.field[b].get_state()[2] for b in range(len(case["blocks"]))])
+        d.close()
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            np.testing.assert_array_equal(a, b)
+
+
 @pytest.mark.parametrize("variant", ["l1", "split", "split-tma", "split-tma-p"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_k_chunking_is_bit_identical(precision, variant):
@@ -160,7 +194,7 @@ def test_variants_agree_at_64(precision):
     split-variant edge tiles span several CTAs per face layer) after two
     RK3 steps: FP64 to 1e-13, mixed to 1e-6 relative per field."""
     case = cases.case_box(64, species=cases.synthetic_species(), seed=5)
-    variants = ["l1", "split", "split-tma", "split-tma-p"] + (["tma"] if precision == "mixed" else [])
+    variants = ["l1", "split", "split-tma", "split-tma-p"] + (["tma", "dq-tma"] if precision == "mixed" else [])
     out = {}
     for v in variants:
         d = cc.Driver.from_case(case, precision)
@@ -202,8 +236,8 @@ def test_multiblock64_small_fp64_matches_oracle(variant):
     assert not bad, errs
 
 
-@pytest.mark.parametrize("variant", ["l1", "split"])
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("variant,precision", [("l1", "fp64"), ("l1", "mixed"), ("split", "fp64"),
+                                               ("split", "mixed"), ("dq-tma", "mixed")])
 def test_per_block_launches_equal_batched(precision, variant):
     """One launch per block per kernel (the reference's granularity) gives
     bit-identical states to the batched launch over all blocks."""
@@ -428,18 +462,19 @@ def test_fused_tma_variant_refused_in_fp64():
     """The fused TMA variant exists in the FP32 bulk precision only (its FP64
     planes do not fit in shared memory): pinning it on an FP64 context fails
     at cc_init, before any kernel runs."""
-    d = cc.Driver.from_case(CASES["box"], "fp64")
-    d.set_tuning("tma", 4)
-    with pytest.raises(RuntimeError, match="TMA variants"):
-        d.initialize_computation()
-    d.close()
+    for variant in ("tma", "dq-tma"):
+        d = cc.Driver.from_case(CASES["box"], "fp64")
+        d.set_tuning(variant, 4)
+        with pytest.raises(RuntimeError, match="TMA variants"):
+            d.initialize_computation()
+        d.close()
 
 
 def test_tma_variants_refused_without_tensor_maps():
     """Tensor maps exist for 0 or 9 species only: pinning a TMA variant on a
     context with another species count fails at cc_init."""
     case = cases.case_box(8, species=SP4, seed=2)
-    for variant in ("tma", "split-tma", "split-tma-p"):
+    for variant in ("tma", "split-tma", "split-tma-p", "dq-tma"):
         d = cc.Driver.from_case(case, "mixed")
         d.set_tuning(variant, 4)
         with pytest.raises(RuntimeError, match="TMA variants"):
