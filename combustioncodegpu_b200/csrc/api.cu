@@ -103,11 +103,11 @@ struct cc_ctx {
   int variant = 0;                // stage kernels: 0 fused (L1 stencil reads), 1 fused TMA planes, 2 split faces/update,
                                   // 3 split with TMA-staged face planes, 4 the same on persistent CTAs,
                                   // 5 face kernel differencing in the tile (dq) + update
-  int dq_ty = 8;                  // variant 5: tile height of the dq face kernel (32 x dq_ty points x kz)
-  int force_ty = 0;               // cc_set_tuning: dq tile height, 0 = autotune
-  std::vector<Tile> hdq;          // variant 5: tiles of the dq face kernel
-  std::vector<int> dq_begin;      // per block: first dq tile (block-ordered list), + end
-  Tile *d_dqtiles = nullptr;
+  int face_ty = 8;                // variants 3-5: tile height of the TMA face kernel (32 x face_ty x kz points)
+  int force_ty = 0;               // cc_set_tuning: face tile height, 0 = autotune
+  std::vector<Tile> hftiles;      // variants 3-5: tiles of the TMA face kernel
+  std::vector<int> ft_begin;      // per block: first face tile (block-ordered list), + end
+  Tile *d_ftiles = nullptr;
   std::vector<Tile> hedges;       // split variant: tiles of the minus-side face layers
   std::vector<int> tile_begin, edge_begin;  // per block: first tile / edge tile (lists are block-ordered), + end
   bool per_block = false;         // cc_set_launch_mode: one launch per block per kernel instead of one per stage
@@ -125,6 +125,8 @@ struct cc_ctx {
   CUtensorMap *d_tmaps = nullptr; // [3][2][n_blocks]: plane boxes of tile height 8, 4, 16 (kTmaRows) for the
                                   // primitive arenas P[0], P[1] per block
   unsigned *d_ticket = nullptr;   // tile counter of the persistent face kernel
+  GridBarrier *d_gridbar = nullptr;  // grid-wide barrier of the single-launch halo program
+  bool halo_coop = false;         // the device takes cooperative launches (single-launch halo program)
   LusgsArgs lu{};                 // LU-SGS work arrays (allocated by the first LU-SGS step)
   std::vector<int64_t> lu_hb;     // sweep positions where each hyperplane begins, + end
   int n_partials = 296;
@@ -268,26 +270,26 @@ void transpose_fields(const double *src, int64_t ng, int nf, std::vector<double>
 constexpr int kTmaTileRows[3] = {8, 4, 16};
 int tma_shape(int ty) { return ty == 4 ? 1 : (ty == 16 ? 2 : 0); }
 
-// Work list of the dq face kernel: 32 x ty columns, k split into chunks of kz.
-void build_dq_tiles(cc_ctx *c, int ty, int kz) {
-  c->hdq.clear();
-  c->dq_begin.clear();
+// Work list of the TMA face kernels: 32 x ty columns, k split into chunks of kz.
+void build_face_tiles(cc_ctx *c, int ty, int kz) {
+  c->hftiles.clear();
+  c->ft_begin.clear();
   for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
-    c->dq_begin.push_back((int)c->hdq.size());
+    c->ft_begin.push_back((int)c->hftiles.size());
     const auto &b = c->blocks[bi];
     for (int k0 = 0; k0 < b.mz; k0 += kz)
       for (int j0 = 0; j0 < b.my; j0 += ty)
         for (int i0 = 0; i0 < b.mx; i0 += 32) {
           Tile t{};
           t.blk = bi, t.i0 = i0, t.j0 = j0, t.k0 = k0, t.k1 = std::min(b.mz, k0 + kz);
-          c->hdq.push_back(t);
+          c->hftiles.push_back(t);
         }
   }
-  c->dq_begin.push_back((int)c->hdq.size());
-  c->dq_ty = ty;
+  c->ft_begin.push_back((int)c->hftiles.size());
+  c->face_ty = ty;
 }
 
-int max_dq_tiles(cc_ctx *c) {
+int max_face_tiles(cc_ctx *c) {
   int64_t n = 0;
   for (const auto &b : c->blocks) n += (int64_t)((b.mx + 31) / 32) * ((b.my + 3) / 4) * b.mz;
   return (int)n;
@@ -462,10 +464,10 @@ int setup_device(cc_ctx *c) {
   c->d_blocks = (BlockInfo *)p;
   if (dev_alloc(c, &p, sizeof(Tile) * (size_t)std::max(1, max_tiles(c)))) return CC_ERR_CUDA;
   c->d_tiles = (Tile *)p;
-  if (dev_alloc(c, &p, sizeof(Tile) * (size_t)std::max(1, max_dq_tiles(c)))) return CC_ERR_CUDA;
-  c->d_dqtiles = (Tile *)p;
-  build_dq_tiles(c, c->dq_ty, c->kz);
-  CK(cudaMemcpyAsync(c->d_dqtiles, c->hdq.data(), sizeof(Tile) * c->hdq.size(), cudaMemcpyHostToDevice, c->stream));
+  if (dev_alloc(c, &p, sizeof(Tile) * (size_t)std::max(1, max_face_tiles(c)))) return CC_ERR_CUDA;
+  c->d_ftiles = (Tile *)p;
+  build_face_tiles(c, c->face_ty, c->kz);
+  CK(cudaMemcpyAsync(c->d_ftiles, c->hftiles.data(), sizeof(Tile) * c->hftiles.size(), cudaMemcpyHostToDevice, c->stream));
   for (int b = 0; b < 2; ++b) {
     if (dev_alloc(c, &c->P[b], E * N * np_of(c))) return CC_ERR_CUDA;
     if (dev_alloc(c, &c->Pr[b], E * N * npr_of(c))) return CC_ERR_CUDA;
@@ -476,6 +478,14 @@ int setup_device(cc_ctx *c) {
   if (dev_alloc(c, &c->faces, E * N * 3 * nv_of(c))) return CC_ERR_CUDA;
   if (dev_alloc(c, &p, sizeof(unsigned))) return CC_ERR_CUDA;
   c->d_ticket = (unsigned *)p;
+  if (dev_alloc(c, &p, sizeof(GridBarrier))) return CC_ERR_CUDA;
+  c->d_gridbar = (GridBarrier *)p;
+  {
+    int dev = 0, coop = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    c->halo_coop = coop != 0;
+  }
   if (c->precision != CC_FP64) {
     if (dev_alloc(c, &p, sizeof(double) * 3 * N)) return CC_ERR_CUDA;
     c->d_gcl = (double *)p;
@@ -588,18 +598,36 @@ HaloArgs<T> halo_args(cc_ctx *c, int pn, int pp, double *qn, const double *qp) {
   return h;
 }
 
+// The halo program after a stage: one cooperative launch of the whole
+// program (node levels, copies, the zeroing of |V| at wall faces when vel is
+// given, the post-exchange time step), or, in the per-block launch mode (the
+// reference's granularity) and for programs of more than kHaloMaxLevels node
+// levels, one launch per level, one for the copies (and time step) and one for
+// |V|.  Both run the same device functions: identical results.
 template <typename T, int NS>
-int run_halo(cc_ctx *c, int pn, int pp, double *qn, const double *qp, unsigned long long *dt_next = nullptr) {
+int run_halo(cc_ctx *c, int pn, int pp, double *qn, const double *qp, unsigned long long *dt_next = nullptr,
+             double *vel = nullptr) {
   HaloArgs<T> h = halo_args<T, NS>(c, pn, pp, qn, qp);
   h.G = (const T *)c->G;
   h.dt_next = dt_next;
   const auto &lb = c->plan.level_begin;
+  const int n_levels = lb.empty() ? 0 : (int)lb.size() - 1;
+  if (!c->per_block && c->halo_coop && n_levels <= kHaloMaxLevels) {
+    HaloLevels lv{};
+    lv.n = n_levels;
+    for (int l = 0; l <= n_levels; ++l) lv.begin[l] = lb[l];
+    h.begin = 0, h.end = (int64_t)c->plan.copies.size();
+    CK((Launch<T, NS>::halo_all(h, c->chem, lv, vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->d_gridbar,
+                                c->d_status, c->stream)));
+    return 0;
+  }
   for (size_t l = 0; l + 1 < lb.size(); ++l) {
     h.begin = lb[l], h.end = lb[l + 1];
     CK((Launch<T, NS>::halo_nodes(h, c->chem, c->stream)));
   }
   h.begin = 0, h.end = (int64_t)c->plan.copies.size();
   CK((Launch<T, NS>::halo_copies(h, c->chem, c->stream)));
+  if (vel) CK(launch_zero_points(vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream));
   return 0;
 }
 
@@ -611,6 +639,7 @@ int derive_state(cc_ctx *c) {
   const int64_t N = c->N;
   c->qcur = 0;
   CK((Launch<T, NS>::configure()));
+  CK(cudaMemsetAsync(c->d_gridbar, 0, sizeof(GridBarrier), c->stream));
   CK((Launch<T, NS>::cv_from_bv(c->chem, c->stage64, c->Q[0], N, c->d_vel, c->stream)));
   CK(cudaMemcpyAsync(c->Q[1], c->Q[0], sizeof(double) * N * nv_of(c), cudaMemcpyDeviceToDevice, c->stream));
   if (int r = from64(c, c->stage64, c->P[0], N * np_of(c))) return r;
@@ -712,37 +741,37 @@ bool variant_ok(const cc_ctx *c, int v) {
 // One stage's kernels of the given variant over the current tile list:
 // one launch per kernel over all blocks, or (per_block) one per block.
 template <typename T, int NS>
-int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge, const Tile *dq_tiles,
-                       int n_dq);
+int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge, const Tile *face_tiles,
+                       int n_ft);
 
 template <typename T, int NS>
 int launch_stage(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt) {
   if (!c->per_block || c->tile_begin.size() != c->blocks.size() + 1)
-    return launch_stage_range<T, NS>(c, a, pc, variant, nt, (int)c->hedges.size(), c->d_dqtiles,
-                                     (int)c->hdq.size());
+    return launch_stage_range<T, NS>(c, a, pc, variant, nt, (int)c->hedges.size(), c->d_ftiles,
+                                     (int)c->hftiles.size());
   const Tile *tiles = a.tiles;
   for (size_t b = 0; b < c->blocks.size(); ++b) {
     a.tiles = tiles + c->tile_begin[b];
     a.edge_tiles = c->d_edges + c->edge_begin[b];
     if (int r = launch_stage_range<T, NS>(c, a, pc, variant, c->tile_begin[b + 1] - c->tile_begin[b],
-                                          c->edge_begin[b + 1] - c->edge_begin[b], c->d_dqtiles + c->dq_begin[b],
-                                          c->dq_begin[b + 1] - c->dq_begin[b]))
+                                          c->edge_begin[b + 1] - c->edge_begin[b], c->d_ftiles + c->ft_begin[b],
+                                          c->ft_begin[b + 1] - c->ft_begin[b]))
       return r;
   }
   return 0;
 }
 
 template <typename T, int NS>
-int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge, const Tile *dq_tiles,
-                       int n_dq) {
+int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge, const Tile *face_tiles,
+                       int n_ft) {
   if ((variant == 1 || variant == 3 || variant == 4 || variant == 5) && !c->d_tmaps)
     return fail(CC_ERR_STATE, "TMA variant without tensor maps");
   if (variant == 5) {  // faces differenced in the tile (dq), then the update
     a.faces = (T *)c->faces;
     a.dq_direct = 1;
     const size_t nb = c->blocks.size();
-    CK((Launch<T, NS>::faces_dq(a, dq_tiles, c->d_tmaps + ((size_t)tma_shape(c->dq_ty) * 2 + pc) * nb, c->chem,
-                                n_dq, c->dq_ty, c->stream)));
+    CK((Launch<T, NS>::faces_dq(a, face_tiles, c->d_tmaps + ((size_t)tma_shape(c->face_ty) * 2 + pc) * nb, c->chem,
+                                n_ft, c->face_ty, c->stream)));
     if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
     CK((Launch<T, NS>::update(a, c->chem, nt, c->stream)));
     return 0;
@@ -755,11 +784,12 @@ int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, i
     if (variant == 2) {
       CK((Launch<T, NS>::faces(a, c->chem, nt, n_edge, c->stream)));
     } else {  // regular tiles from TMA-staged planes (persistent CTAs for 4), edge tiles through L1
+      const CUtensorMap *maps = c->d_tmaps + ((size_t)tma_shape(c->face_ty) * 2 + pc) * c->blocks.size();
       if (variant == 3)
-        CK((Launch<T, NS>::faces_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
+        CK((Launch<T, NS>::faces_tma(a, face_tiles, c->face_ty, maps, c->chem, n_ft, c->stream)));
       else
-        CK((Launch<T, NS>::faces_tma_persistent(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt,
-                                                c->d_ticket, c->stream)));
+        CK((Launch<T, NS>::faces_tma_persistent(a, face_tiles, c->face_ty, maps, c->chem, n_ft, c->d_ticket,
+                                                c->stream)));
       CK((Launch<T, NS>::faces(a, c->chem, 0, n_edge, c->stream)));
     }
     if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
@@ -777,8 +807,7 @@ int after_stage(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, 
   if (c->closure_on) CK((Launch<T, NS>::props_mlp(a.Pn, a.Prn, c->N, &c->cl, c->d_status, c->chem, c->stream)));
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
-  if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next)) return r;
-  if (a.vel) CK(launch_zero_points(c->d_vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream));
+  if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next, a.vel ? c->d_vel : nullptr)) return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
   return 0;
 }
@@ -802,8 +831,9 @@ int lusgs_and_halo(cc_ctx *c, StageArgs<T> a, int pn, int pc) {
   a.faces = (T *)c->faces;
   a.edge_tiles = c->d_edges;
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
-  if (c->tma_ok && c->d_tmaps) {
-    CK((Launch<T, NS>::faces_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
+  if (c->tma_ok && c->d_tmaps) {  // the regular 32 x 8 tiles
+    CK((Launch<T, NS>::faces_tma(a, c->d_tiles, 8, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt,
+                                 c->stream)));
     CK((Launch<T, NS>::faces(a, c->chem, 0, n_edge, c->stream)));
   } else {
     CK((Launch<T, NS>::faces(a, c->chem, nt, n_edge, c->stream)));
@@ -932,7 +962,7 @@ int autotune(cc_ctx *c) {
   double best = 1e300;
   int best_kz = c->kz;
   int best_variant = 0;
-  int best_ty = c->dq_ty;
+  int best_ty = c->face_ty;
   if (c->force_kz > 0) kzs.assign(1, c->force_kz);
   std::vector<int> variants;
   if (c->force_variant >= 0 && !variant_ok(c, c->force_variant))
@@ -943,17 +973,20 @@ int autotune(cc_ctx *c) {
   else
     for (int v : {0, 1, 2, 3, 4, 5})
       if (variant_ok(c, v)) variants.push_back(v);
-  // tile heights of the dq face kernel (variant 5; the other variants' tiles are 32 x 8)
-  std::vector<int> tys = {4, 8, 16};
-  if (c->force_ty > 0) tys.assign(1, c->force_ty);
+  // tile heights of the TMA face kernels (variants 3-5; the other variants'
+  // tiles are 32 x 8), those whose plane ring fits in shared memory
+  std::vector<int> tys;
+  for (int ty : {4, 8, 16})
+    if ((c->force_ty <= 0 || ty == c->force_ty) && Launch<T, NS>::faces_tma_smem(ty) != 0) tys.push_back(ty);
+  if (tys.empty()) return fail(CC_ERR_ARG, "the face tile height does not fit in shared memory in this precision");
   for (int variant : variants) {
-    for (int ty : (variant == 5 ? tys : std::vector<int>{8})) {
+    for (int ty : (variant >= 3 ? tys : std::vector<int>{8})) {
       for (int kz : kzs) {
         build_tiles_kz(c, kz);
         CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
                            c->stream));
-        build_dq_tiles(c, ty, kz);
-        CK(cudaMemcpyAsync(c->d_dqtiles, c->hdq.data(), sizeof(Tile) * c->hdq.size(), cudaMemcpyHostToDevice,
+        build_face_tiles(c, ty, kz);
+        CK(cudaMemcpyAsync(c->d_ftiles, c->hftiles.data(), sizeof(Tile) * c->hftiles.size(), cudaMemcpyHostToDevice,
                            c->stream));
         const int nt = (int)c->htiles.size();
         if (int r = launch_stage<T, NS>(c, a, pc, variant, nt)) return r;
@@ -966,7 +999,7 @@ int autotune(cc_ctx *c) {
         CK(cudaEventElapsedTime(&ms, e0, e1));
         if (verbose)
           std::fprintf(stderr, "cc autotune: %s tile 32x%dx%d tiles=%d %.4f ms\n", kVariantName[variant],
-                       variant == 5 ? ty : kTY, kz, variant == 5 ? (int)c->hdq.size() : nt, ms / 3);
+                       variant >= 3 ? ty : kTY, kz, variant >= 3 ? (int)c->hftiles.size() : nt, ms / 3);
         if (ms / 3 < best) best = ms / 3, best_kz = kz, best_variant = variant, best_ty = ty;
       }
     }
@@ -976,8 +1009,8 @@ int autotune(cc_ctx *c) {
   build_tiles_kz(c, best_kz);
   CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
                      c->stream));
-  build_dq_tiles(c, best_variant == 5 ? best_ty : 8, best_kz);
-  CK(cudaMemcpyAsync(c->d_dqtiles, c->hdq.data(), sizeof(Tile) * c->hdq.size(), cudaMemcpyHostToDevice,
+  build_face_tiles(c, best_variant >= 3 ? best_ty : 8, best_kz);
+  CK(cudaMemcpyAsync(c->d_ftiles, c->hftiles.data(), sizeof(Tile) * c->hftiles.size(), cudaMemcpyHostToDevice,
                      c->stream));
   c->variant = best_variant;
   c->tuned_ms = best;
@@ -1433,6 +1466,11 @@ int cc_status(cc_ctx *c, unsigned *flags) {
   CK(cudaMemcpyAsync(flags, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  // a grid barrier that gave up leaves its arrival count behind: reset it
+  if ((*flags & kStatusHaloTimeout) && c->d_gridbar) {
+    CK(cudaMemsetAsync(c->d_gridbar, 0, sizeof(GridBarrier), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
   return 0;
 }
 
@@ -1545,7 +1583,7 @@ int cc_tuning(cc_ctx *c, int *variant, int *kz, double *stage_ms, int tile[3]) {
   if (stage_ms) *stage_ms = c->tuned_ms;
   if (tile) {
     tile[0] = kTX;
-    tile[1] = c->variant == 5 ? c->dq_ty : kTY;
+    tile[1] = c->variant >= 3 ? c->face_ty : kTY;
     tile[2] = c->kz;
   }
   return 0;

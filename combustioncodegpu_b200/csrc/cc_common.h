@@ -126,6 +126,23 @@ enum StatusBits : unsigned {
   kStatusNewtonCap = 1u,     // temperature Newton hit its iteration cap
   kStatusNonFinite = 2u,     // NaN/Inf or non-positive rho/p/T after an update
   kStatusBadDt = 4u,         // global time step not positive and finite
+  kStatusHaloTimeout = 32u,  // a grid-wide barrier of the single-launch halo program gave up
+};
+
+// Arrival counter and generation of the bounded grid-wide barrier of the
+// single-launch halo program (zeroed at set-up; every completed barrier
+// leaves count at 0).
+struct GridBarrier {
+  unsigned count;
+  unsigned gen;
+};
+
+// Node levels the single-launch halo program takes (more fall back to one
+// launch per level), and their bounds in the node list.
+constexpr int kHaloMaxLevels = 8;
+struct HaloLevels {
+  int64_t begin[kHaloMaxLevels + 1];
+  int n;
 };
 
 // Arguments of one stage launch (see stage.cuh).

@@ -43,16 +43,36 @@ cudaError_t Launch<T, NS>::faces(const StageArgs<T> &a, const ChemParams &C, int
 }
 
 template <typename T, int NS>
-size_t Launch<T, NS>::faces_tma_smem() {
-  return FacesTmaLayout<T, NS>::kBytes;
+size_t Launch<T, NS>::faces_tma_smem(int ty) {
+  size_t b = ty == 4 ? FacesTmaLayout<T, NS, 4>::kBytes
+                     : (ty == 16 ? FacesTmaLayout<T, NS, 16>::kBytes : FacesTmaLayout<T, NS, 8>::kBytes);
+  return b <= 227 * 1024 ? b : 0;
 }
 
+// Whether the ring of the TMA face kernel of tile height TY fits in shared
+// memory (32 x 16 does not in FP64): only those kernels are instantiated.
+template <typename T, int NS, int TY>
+struct FacesTmaFits {
+  static constexpr bool value = FacesTmaLayout<T, NS, TY>::kOk;
+};
+
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::faces_tma(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
-                                     cudaStream_t s) {
+cudaError_t Launch<T, NS>::faces_tma(const StageArgs<T> &a, const Tile *tiles, int ty, const void *maps,
+                                     const ChemParams &C, int n_tiles, cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;
-  if (faces_tma_smem() > 227 * 1024) return cudaErrorInvalidConfiguration;
-  k_faces_tma<T, NS><<<n_tiles, dim3(kTX, kTY), faces_tma_smem(), s>>>(a, (const CUtensorMap *)maps, C);
+  const size_t smem = faces_tma_smem(ty);
+  if (smem == 0) return cudaErrorInvalidConfiguration;
+  const CUtensorMap *m = (const CUtensorMap *)maps;
+  if (ty == 4) {
+    k_faces_tma<T, NS, 4><<<n_tiles, dim3(kTX, 4), smem, s>>>(a, tiles, m, C);
+  } else if (ty == 8) {
+    k_faces_tma<T, NS, 8><<<n_tiles, dim3(kTX, 8), smem, s>>>(a, tiles, m, C);
+  } else if (ty == 16) {
+    if constexpr (FacesTmaFits<T, NS, 16>::value)
+      k_faces_tma<T, NS, 16><<<n_tiles, dim3(kTX, 16), smem, s>>>(a, tiles, m, C);
+  } else {
+    return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
@@ -91,24 +111,40 @@ cudaError_t Launch<T, NS>::faces_dq(const StageArgs<T> &a, const Tile *tiles, co
 }
 
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::faces_tma_persistent(const StageArgs<T> &a, const void *maps, const ChemParams &C,
-                                                int n_tiles, unsigned *ticket, cudaStream_t s) {
+cudaError_t Launch<T, NS>::faces_tma_persistent(const StageArgs<T> &a, const Tile *tiles, int ty, const void *maps,
+                                                const ChemParams &C, int n_tiles, unsigned *ticket, cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;
-  if (faces_tma_smem() > 227 * 1024) return cudaErrorInvalidConfiguration;
-  static int per_sm = 0, n_sm = 0;
-  if (per_sm == 0) {
+  const size_t smem = faces_tma_smem(ty);
+  if (smem == 0 || (ty != 4 && ty != 8 && ty != 16)) return cudaErrorInvalidConfiguration;
+  static int per_sm[3] = {0, 0, 0}, n_sm = 0;  // CTAs per SM for ty = 4, 8, 16
+  const int si = ty == 4 ? 0 : (ty == 8 ? 1 : 2);
+  if (per_sm[si] == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_faces_tma_persistent<T, NS>, kTX * kTY,
-                                                  faces_tma_smem());
-    per_sm = std::max(1, per_sm);
+    if (ty == 4) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[si], k_faces_tma_persistent<T, NS, 4>, kTX * 4, smem);
+    } else if (ty == 8) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[si], k_faces_tma_persistent<T, NS, 8>, kTX * 8, smem);
+    } else {
+      if constexpr (FacesTmaFits<T, NS, 16>::value)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[si], k_faces_tma_persistent<T, NS, 16>, kTX * 16,
+                                                      smem);
+    }
+    per_sm[si] = std::max(1, per_sm[si]);
   }
   cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  const int grid = std::min(n_tiles, n_sm * per_sm);
-  k_faces_tma_persistent<T, NS><<<grid, dim3(kTX, kTY), faces_tma_smem(), s>>>(a, (const CUtensorMap *)maps, C,
-                                                                              n_tiles, ticket);
+  const int grid = std::min(n_tiles, n_sm * per_sm[si]);
+  const CUtensorMap *m = (const CUtensorMap *)maps;
+  if (ty == 4) {
+    k_faces_tma_persistent<T, NS, 4><<<grid, dim3(kTX, 4), smem, s>>>(a, tiles, m, C, n_tiles, ticket);
+  } else if (ty == 8) {
+    k_faces_tma_persistent<T, NS, 8><<<grid, dim3(kTX, 8), smem, s>>>(a, tiles, m, C, n_tiles, ticket);
+  } else {
+    if constexpr (FacesTmaFits<T, NS, 16>::value)
+      k_faces_tma_persistent<T, NS, 16><<<grid, dim3(kTX, 16), smem, s>>>(a, tiles, m, C, n_tiles, ticket);
+  }
   return cudaGetLastError();
 }
 
@@ -152,11 +188,18 @@ cudaError_t Launch<T, NS>::configure() {
   if (e != cudaSuccess) return e;
   if (stage_tma_smem() <= 227 * 1024)
     e = cudaFuncSetAttribute(k_stage_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_tma_smem());
-  if (e == cudaSuccess && faces_tma_smem() <= 227 * 1024)
-    e = cudaFuncSetAttribute(k_faces_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)faces_tma_smem());
-  if (e == cudaSuccess && faces_tma_smem() <= 227 * 1024)
-    e = cudaFuncSetAttribute(k_faces_tma_persistent<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)faces_tma_smem());
+  auto faces_attr = [&](auto kernel, int ty) {
+    if (e == cudaSuccess && faces_tma_smem(ty) != 0)
+      e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)faces_tma_smem(ty));
+  };
+  faces_attr(k_faces_tma<T, NS, 4>, 4);
+  faces_attr(k_faces_tma<T, NS, 8>, 8);
+  faces_attr(k_faces_tma_persistent<T, NS, 4>, 4);
+  faces_attr(k_faces_tma_persistent<T, NS, 8>, 8);
+  if constexpr (FacesTmaFits<T, NS, 16>::value) {
+    faces_attr(k_faces_tma<T, NS, 16>, 16);
+    faces_attr(k_faces_tma_persistent<T, NS, 16>, 16);
+  }
   if constexpr (sizeof(T) == 4 && NS >= 0) {
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k_faces_dq<T, NS, 4, DqChunks<4>::value>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -243,6 +286,36 @@ cudaError_t Launch<T, NS>::halo_copies(const HaloArgs<T> &a, const ChemParams &C
   if (e != cudaSuccess || !a.dt_next || a.n_icopies <= 0) return e;
   k_halo_copy_dt<T, NS><<<(unsigned)((a.n_icopies + tpb - 1) / tpb), tpb, 0, s>>>(a, C);
   return cudaGetLastError();
+}
+
+template <typename T, int NS>
+cudaError_t Launch<T, NS>::halo_all(const HaloArgs<T> &a, const ChemParams &C, const HaloLevels &lv, double *vel,
+                                    const int64_t *vel_zero, int64_t n_vel_zero, GridBarrier *bar, unsigned *status,
+                                    cudaStream_t s) {
+  const int tpb = 256;
+  static int capacity = 0;  // CTAs that fit on the device at once
+  if (capacity == 0) {
+    int dev = 0, n_sm = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_halo_all<T, NS>, tpb, 0);
+    capacity = std::max(1, n_sm * per_sm);
+  }
+  int64_t work = std::max<int64_t>(3 * (a.end - a.begin), std::max<int64_t>(a.n_icopies, n_vel_zero));
+  for (int l = 0; l < lv.n; ++l) work = std::max(work, lv.begin[l + 1] - lv.begin[l]);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(capacity, (work + tpb - 1) / tpb));
+  const int ns = C.ns, np = 6 + ns, npr = 2 + ns, nq = 5 + ns;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(tpb);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: the grid barriers can complete
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_halo_all<T, NS>, a, C, lv, np, npr, nq, vel, vel_zero, n_vel_zero, bar, status);
 }
 
 template <typename T, int NS>

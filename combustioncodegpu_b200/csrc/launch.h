@@ -23,8 +23,11 @@ struct Launch {
   static cudaError_t faces(const StageArgs<T> &a, const ChemParams &C, int n_regular, int n_edge, cudaStream_t s);
   static cudaError_t update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s);
   // split variant with TMA-staged planes in the face kernel (regular tiles only)
-  static size_t faces_tma_smem();
-  static cudaError_t faces_tma(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
+  // TMA face kernel on tiles of 32 x ty points (ty = 4, 8, 16; 16 in FP32
+  // only): smem 0 when the ring does not fit
+  static size_t faces_tma_smem(int ty = 8);
+  static cudaError_t faces_tma(const StageArgs<T> &a, const Tile *tiles, int ty, const void *maps, const ChemParams &C,
+                               int n_tiles,
                                cudaStream_t s);
   // persistent form: resident CTAs take the n_tiles regular tiles from *ticket (zeroed here)
   // face kernel that differences the faces in the tile and writes dq
@@ -33,8 +36,8 @@ struct Launch {
   static size_t faces_dq_smem(int ty);
   static cudaError_t faces_dq(const StageArgs<T> &a, const Tile *tiles, const void *maps, const ChemParams &C,
                               int n_tiles, int ty, cudaStream_t s);
-  static cudaError_t faces_tma_persistent(const StageArgs<T> &a, const void *maps, const ChemParams &C, int n_tiles,
-                                          unsigned *ticket, cudaStream_t s);
+  static cudaError_t faces_tma_persistent(const StageArgs<T> &a, const Tile *tiles, int ty, const void *maps,
+                                          const ChemParams &C, int n_tiles, unsigned *ticket, cudaStream_t s);
   // learned transport closure (closure.cuh) over every arena point; cl is a ClosureDev
   static cudaError_t props_mlp(const T *P, T *Pr, int64_t N, const void *cl, unsigned *status, const ChemParams &C,
                                cudaStream_t s);
@@ -50,6 +53,11 @@ struct Launch {
                                   cudaStream_t s);
   static cudaError_t halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   static cudaError_t halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
+  // the whole halo program (node levels, copies, |V| zeroing at wall faces,
+  // post-exchange time step) in one cooperative launch (k_halo_all)
+  static cudaError_t halo_all(const HaloArgs<T> &a, const ChemParams &C, const HaloLevels &lv, double *vel,
+                              const int64_t *vel_zero, int64_t n_vel_zero, GridBarrier *bar, unsigned *status,
+                              cudaStream_t s);
   static cudaError_t cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, double *vel,
                                 cudaStream_t s);
   static cudaError_t props_all(const ChemParams &C, const T *P, T *Pr, int64_t N, cudaStream_t s);

@@ -573,14 +573,12 @@ __device__ __forceinline__ double total_energy(const ChemParams &C, double rho, 
   return e - p;
 }
 
-// Phase A: evaluate the halo nodes of one level into scratch slots.
+// Phase A: evaluate halo node e into its scratch slot.
 template <typename T, int NS>
-__global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemParams C) {
+__device__ __forceinline__ void halo_node(const HaloArgs<T> &a, const ChemParams &C, int64_t e) {
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   const int nv = 5 + ns;
-  const int64_t e = a.begin + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (e >= a.end) return;
   const HaloNode nd = a.nodes[e];
   const int64_t o = nd.slot;
   const int64_t S = a.NS_cap;
@@ -733,6 +731,14 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
   }
 }
 
+// Phase A, one launch per level: the nodes [a.begin, a.end).
+template <typename T, int NS>
+__global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemParams C) {
+  const int64_t e = a.begin + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= a.end) return;
+  halo_node<T, NS>(a, C, e);
+}
+
 // Phase B: write every changed point from its resolved source.  One thread
 // per (copy, array): grid y selects P, Pr or Q, and the thread moves all
 // fields of that array for its copy, loading them all before the first
@@ -741,13 +747,11 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
 // mostly sources) are consecutive, so every field access is coalesced; the
 // copy record is read once per array rather than once per field.
 template <typename T, int NS>
-__global__ void k_halo_copy_fields(const HaloArgs<T> a, int np, int npr, int nq) {
+__device__ __forceinline__ void halo_copy(const HaloArgs<T> &a, int64_t e, int which, int np, int npr, int nq) {
   constexpr int A = SpecCount<NS>::kArr;
-  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // copy (grid x)
-  if (e >= a.end - a.begin) return;
   const HaloCopy c = a.copies[a.begin + e];
   const RefPtrs<T> r = resolve(a, c.src);
-  if (blockIdx.y == 0) {
+  if (which == 0) {
     T v[6 + A];
 #pragma unroll
     for (int f = 0; f < 6 + A; ++f)
@@ -755,7 +759,7 @@ __global__ void k_halo_copy_fields(const HaloArgs<T> a, int np, int npr, int nq)
 #pragma unroll
     for (int f = 0; f < 6 + A; ++f)
       if (f < np) a.P[f * a.N + c.dst] = v[f];
-  } else if (blockIdx.y == 1) {
+  } else if (which == 1) {
     T v[2 + A];
 #pragma unroll
     for (int f = 0; f < 2 + A; ++f)
@@ -774,27 +778,110 @@ __global__ void k_halo_copy_fields(const HaloArgs<T> a, int np, int npr, int nq)
   }
 }
 
+template <typename T, int NS>
+__global__ void k_halo_copy_fields(const HaloArgs<T> a, int np, int npr, int nq) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // copy (grid x)
+  if (e >= a.end - a.begin) return;
+  halo_copy<T, NS>(a, e, blockIdx.y, np, npr, nq);  // grid y selects P, Pr or Q
+}
+
 // Interior points rewritten by phase B (coincident interface layers)
 // contribute their post-exchange local time step to the next global step,
 // as the reference evaluates the step after the exchange (Driver.cu:150-163).
 template <typename T, int NS>
-__global__ void k_halo_copy_dt(const HaloArgs<T> a, const __grid_constant__ ChemParams C) {
+__device__ __forceinline__ double halo_copy_dt_point(const HaloArgs<T> &a, const ChemParams &C, int64_t e) {
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
+  const HaloCopy c = a.copies[a.icopies[e]];
+  const int64_t p = c.dst, N = a.N;
+  T Y[A], gam, cs;
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) Y[l] = a.P[(6 + l) * N + p];
+  gamma_and_c<T, NS>(C, param_rec<T>(C), a.P[5 * N + p], Y, gam, cs);
+  return local_time_step<T>(C, a.G, N, p, (double)a.P[p], (double)a.P[N + p], (double)a.P[2 * N + p],
+                            (double)a.P[3 * N + p], (double)cs, (double)gam, (double)a.Pr[p], (c.src.pad & 2) != 0);
+}
+
+template <typename T, int NS>
+__global__ void k_halo_copy_dt(const HaloArgs<T> a, const __grid_constant__ ChemParams C) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double dt_min = 1e300;
-  if (e < a.n_icopies) {
-    const HaloCopy c = a.copies[a.icopies[e]];
-    const int64_t p = c.dst, N = a.N;
-    T Y[A], gam, cs;
+  if (e < a.n_icopies) dt_min = halo_copy_dt_point<T, NS>(a, C, e);
 #pragma unroll
-    for (int l = 0; l < A; ++l)
-      if (l < ns) Y[l] = a.P[(6 + l) * N + p];
-    gamma_and_c<T, NS>(C, param_rec<T>(C), a.P[5 * N + p], Y, gam, cs);
-    dt_min = local_time_step<T>(C, a.G, N, p, (double)a.P[p], (double)a.P[N + p], (double)a.P[2 * N + p],
-                                (double)a.P[3 * N + p], (double)cs, (double)gam, (double)a.Pr[p],
-                                (c.src.pad & 2) != 0);
+  for (int o = 16; o > 0; o >>= 1) dt_min = fmin(dt_min, __shfl_xor_sync(0xffffffffu, dt_min, o));
+  if ((threadIdx.x & 31) == 0) atomic_min_pos_double(a.dt_next, dt_min);
+}
+
+// Bounded grid-wide barrier of a cooperative launch (every CTA resident):
+// thread 0 of each CTA arrives on the counter after the CTA's writes (the
+// CTA barrier and its fence make them visible at GPU scope first); the last
+// arrival resets the counter and advances the generation, the others poll the
+// generation (at most max_polls times, 64 ns apart).  Returns false, in every
+// thread of the CTA, when the wait gave up.
+__device__ __forceinline__ bool grid_sync_bounded(GridBarrier *bar, long long max_polls) {
+  __shared__ int ok_sh;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned *vgen = &bar->gen;
+    const unsigned g = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&bar->count, 1u) + 1u;
+    if (arrived == gridDim.x) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      for (long long polls = 0; *vgen == g;) {
+        if (++polls > max_polls) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+    }
+    ok_sh = ok;
   }
+  __syncthreads();
+  return ok_sh != 0;
+}
+
+// The whole halo program in one cooperative launch: the node levels with a
+// grid-wide barrier after each, then the copies of every changed point (P,
+// Pr and Q, consecutive threads on consecutive copies), the zeroing of |V| at
+// wall-face points, and, when the next time step is reduced (a.dt_next), a
+// barrier and the post-exchange time step of the rewritten interior points.
+// The same device functions as the per-level launches, so the results are
+// identical.  A barrier that gives up sets kStatusHaloTimeout and the CTA
+// returns.
+
+template <typename T, int NS>
+__global__ void __launch_bounds__(256, 2)
+    k_halo_all(const HaloArgs<T> a, const __grid_constant__ ChemParams C, const HaloLevels lv, int np, int npr,
+               int nq, double *vel, const int64_t *vel_zero, int64_t n_vel_zero, GridBarrier *bar,
+               unsigned *status) {
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int l = 0; l < lv.n; ++l) {
+    for (int64_t e = lv.begin[l] + tid; e < lv.begin[l + 1]; e += stride) halo_node<T, NS>(a, C, e);
+    if (!grid_sync_bounded(bar, C.max_spins)) {
+      if (threadIdx.x == 0) atomicOr(status, kStatusHaloTimeout);
+      return;
+    }
+  }
+  const int64_t n = a.end - a.begin;
+  for (int64_t e = tid; e < 3 * n; e += stride) halo_copy<T, NS>(a, e % n, (int)(e / n), np, npr, nq);
+  if (vel)
+    for (int64_t e = tid; e < n_vel_zero; e += stride) vel[vel_zero[e]] = 0.0;
+  if (!a.dt_next || a.n_icopies <= 0) return;
+  if (!grid_sync_bounded(bar, C.max_spins)) {
+    if (threadIdx.x == 0) atomicOr(status, kStatusHaloTimeout);
+    return;
+  }
+  double dt_min = 1e300;
+  for (int64_t e = tid; e < a.n_icopies; e += stride) dt_min = fmin(dt_min, halo_copy_dt_point<T, NS>(a, C, e));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) dt_min = fmin(dt_min, __shfl_xor_sync(0xffffffffu, dt_min, o));
   if ((threadIdx.x & 31) == 0) atomic_min_pos_double(a.dt_next, dt_min);

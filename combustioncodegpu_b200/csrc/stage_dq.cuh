@@ -30,30 +30,6 @@
 
 namespace ccb {
 
-// Primitives around one face from a plane ring of HX-wide planes of PV values
-// per field (see SmemStencil).
-template <typename T, int HX, int PV>
-struct SmemStencilT {
-  const T *pm, *p0, *p1, *p2;
-  int q, d;
-  __device__ __forceinline__ const T *plane(int r) const {  // r = 0..3 -> k-1 .. k+2
-    return r == 0 ? pm : (r == 1 ? p0 : (r == 2 ? p1 : p2));
-  }
-  __device__ __forceinline__ T at(int f, int t) const {
-    if (d == 2) return plane(1 + t)[f * PV + q];
-    return p0[f * PV + q + t * (d == 0 ? 1 : HX)];
-  }
-  __device__ __forceinline__ T cross(int f, int c, int sg, int t) const {
-    if (c == 2) {
-      if (d == 2) return plane(1 + t + sg)[f * PV + q];
-      return plane(1 + sg)[f * PV + q + t * (d == 0 ? 1 : HX)];
-    }
-    const int cs = sg * (c == 0 ? 1 : HX);
-    if (d == 2) return plane(1 + t)[f * PV + q + cs];
-    return p0[f * PV + q + t * (d == 0 ? 1 : HX) + cs];
-  }
-};
-
 constexpr size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
 template <typename T, int NS, int TY, int NCH>

@@ -328,21 +328,52 @@ __global__ void __launch_bounds__(kTX *kTY, 1)
 
 namespace ccb {
 
+// Primitives around one face from a ring of planes HX points wide with PV
+// values per field (the same access pattern as SmemStencil, for any tile
+// height).
+template <typename T, int HX, int PV>
+struct SmemStencilT {
+  const T *pm, *p0, *p1, *p2;
+  int q, d;
+  __device__ __forceinline__ const T *plane(int r) const {  // r = 0..3 -> k-1 .. k+2
+    return r == 0 ? pm : (r == 1 ? p0 : (r == 2 ? p1 : p2));
+  }
+  __device__ __forceinline__ T at(int f, int t) const {
+    if (d == 2) return plane(1 + t)[f * PV + q];
+    return p0[f * PV + q + t * (d == 0 ? 1 : HX)];
+  }
+  __device__ __forceinline__ T cross(int f, int c, int sg, int t) const {
+    if (c == 2) {
+      if (d == 2) return plane(1 + t + sg)[f * PV + q];
+      return plane(1 + sg)[f * PV + q + t * (d == 0 ? 1 : HX)];
+    }
+    const int cs = sg * (c == 0 ? 1 : HX);
+    if (d == 2) return plane(1 + t)[f * PV + q + cs];
+    return p0[f * PV + q + t * (d == 0 ? 1 : HX) + cs];
+  }
+};
+
 // Face kernel of the split stage with TMA-staged primitive planes: the
 // regular tiles of k_faces, each computing the +x, +y, +z faces of its points
 // from a ring of 4 planes (k-1 .. k+2) in shared memory; plane k+3 is
 // requested into the slot of plane k-1 once the faces of plane k are done.
-// Without the fused kernel's flux planes the ring fits twice per SM in FP32
-// (once in FP64, 208 KB).
-// Transport and geometry are read through L1; the edge tiles stay with
-// k_faces.  Waits are bounded as in k_stage_tma.
-template <typename T, int NS>
+// The tile is 32 (i, one warp per row) x TY (j) points: TY = 8 fits the ring
+// twice per SM in FP32 (once in FP64, 208 KB), TY = 4 three times in FP32,
+// TY = 16 (16 warps, FP32 only) once.  Transport and geometry are read
+// through L1; the edge tiles stay with k_faces.  Waits are bounded as in
+// k_stage_tma.
+template <typename T, int NS, int TY = kTY>
 struct FacesTmaLayout {
+  static constexpr int HX = kTX + 4, HY = TY + 4, PV = HX * HY;
   static constexpr int kRing = 4;
-  static constexpr size_t kPlaneBytes = TmaLayout<T, NS>::kPlaneBytes;
+  static constexpr size_t kPlaneBytes = ((sizeof(T) * (6 + SpecCount<NS>::kArr) * PV + 127) / 128) * 128;
   static constexpr size_t kRec = ((sizeof(T) * SpecCount<NS>::kArr * 2 * kRecLen + 15) / 16) * 16;
   // alignment slack + barriers + ring + NASA records
   static constexpr size_t kBytes = 128 + 128 + kRing * kPlaneBytes + kRec;
+  // CTAs per SM that the shared memory allows (228 KB per SM, 1 KB reserved per CTA)
+  static constexpr int kFit = (int)((228 * 1024) / (kBytes + 1024));
+  static constexpr bool kOk = kBytes <= 227 * 1024;
+  static constexpr int kMinBlocks = kFit < 1 ? 1 : (kFit > 3 ? 3 : kFit);
 };
 
 // One regular tile of the face kernel: fill the ring with planes k0-1 ..
@@ -357,13 +388,13 @@ struct FacesTmaLayout {
 // of plane kp = k + 2 (1-point halo in j, the tile's i span plus one point
 // on each side), which the faces of plane k + 1 read for the first time
 // through L1.  Rows are spread over the CTA's threads; a hint nothing waits on.
-template <typename T>
+template <typename T, int TY>
 __device__ __forceinline__ void prefetch_props_geometry(const StageArgs<T> &a, const BlockInfo &B, const Tile &t,
                                                         int kp, int npr, int tid) {
   const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
-  const int j_lo = max(t.j0 - 1, -B.g), j_hi = min(t.j0 + kTY + 1, B.my + B.g), nr = j_hi - j_lo;
+  const int j_lo = max(t.j0 - 1, -B.g), j_hi = min(t.j0 + TY + 1, B.my + B.g), nr = j_hi - j_lo;
   const int n = (npr + 10) * nr;
-  for (int e = tid; e < n; e += kTX * kTY) {
+  for (int e = tid; e < n; e += kTX * TY) {
     const int f = e / nr, j = j_lo + e % nr;
     const T *base = f < npr ? a.Pr + (size_t)f * N : a.G + (size_t)(f - npr) * N;
     const int row = (int)B.base + sk * kp + sj * j;
@@ -371,11 +402,11 @@ __device__ __forceinline__ void prefetch_props_geometry(const StageArgs<T> &a, c
   }
 }
 
-template <typename T, int NS>
+template <typename T, int NS, int TY>
 __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUtensorMap *map, const ChemParams &C,
                                               uint64_t *bars, unsigned char *ring, const T *sRec, const Tile &t,
                                               unsigned pc0, bool &aborted) {
-  using L = FacesTmaLayout<T, NS>;
+  using L = FacesTmaLayout<T, NS, TY>;
   constexpr int NV = 5 + SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   const int nv = 5 + ns;
@@ -386,7 +417,7 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
   const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
   const int col = (int)B.base + i + sj * j;
   const bool three_d = B.mz > 1;
-  const unsigned plane_bytes = (unsigned)(sizeof(T) * (6 + ns) * kPlaneVals);
+  const unsigned plane_bytes = (unsigned)(sizeof(T) * (6 + ns) * L::PV);
   // tensor coordinates of plane kp: x = i0 - 2 + g, y = j0 - 2 + g, z = kp + g
   const int tx0 = t.i0 - 2 + B.g, ty0 = t.j0 - 2 + B.g;
   const int kfirst = t.k0 - 1, klast = t.k1 + 1;  // planes the sweep reads
@@ -406,7 +437,7 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
   }
   int k_issued = k_pro;
 
-  const int q = (ty + 2) * kHX + (tx + 2);  // in-plane index of this thread's point
+  const int q = (ty + 2) * L::HX + (tx + 2);  // in-plane index of this thread's point
   T F[NV];
   aborted = false;
   for (int k = t.k0; k < t.k1; ++k) {
@@ -425,13 +456,13 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
     const int p = col + sk * k;
     // (FP64 only: measured faster there, slower in FP32, whose smaller rows
     // stay in L2 without it)
-    if (sizeof(T) == 8 && k + 2 <= B.mz - 1 + B.g) prefetch_props_geometry<T>(a, B, t, k + 2, 2 + ns, tid);
+    if (sizeof(T) == 8 && k + 2 <= B.mz - 1 + B.g) prefetch_props_geometry<T, TY>(a, B, t, k + 2, 2 + ns, tid);
     if (act) {
 #pragma unroll 1
       for (int it = three_d ? 0 : 1; it < 3; ++it) {
         const int d = it == 0 ? 2 : it - 1;
         const int sd = d == 0 ? 1 : (d == 1 ? sj : sk);
-        SmemStencil<T> S{plm, pl0, pl1, pl2, q, d};
+        SmemStencilT<T, L::HX, L::PV> S{plm, pl0, pl1, pl2, q, d};
         face_flux_gen<T, NS>(C, sRec, S, a.Pr, a.G, N, p, sd, d, F);
 #pragma unroll
         for (int l = 0; l < NV; ++l)
@@ -453,7 +484,7 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
     // let this CTA's copies in flight land before it leaves (bounded)
     if (tid == 0)
       for (int kp = max(kfirst, k_issued - L::kRing + 1); kp <= k_issued; ++kp) {
-        long spins = 0;
+        long long spins = 0;
         while (!mbar_try_wait(&bars[slot_of(kp)], parity_of(kp)) && ++spins < kMaxSpins) {
         }
       }
@@ -462,10 +493,11 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
   return klast - kfirst + 1;
 }
 
-template <typename T, int NS>
-__global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
-    k_faces_tma(const StageArgs<T> a, const CUtensorMap *__restrict__ maps, const __grid_constant__ ChemParams C) {
-  using L = FacesTmaLayout<T, NS>;
+template <typename T, int NS, int TY>
+__global__ void __launch_bounds__(kTX *TY, (FacesTmaLayout<T, NS, TY>::kMinBlocks))
+    k_faces_tma(const StageArgs<T> a, const Tile *__restrict__ tiles, const CUtensorMap *__restrict__ maps,
+                const __grid_constant__ ChemParams C) {
+  using L = FacesTmaLayout<T, NS, TY>;
   const int ns = SpecCount<NS>::n(C);
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char *smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
@@ -473,26 +505,26 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   unsigned char *ring = smem_raw + 128;
   T *sRec = reinterpret_cast<T *>(ring + L::kRing * L::kPlaneBytes);
   const int tid = threadIdx.y * kTX + threadIdx.x;
-  const Tile t = a.tiles[blockIdx.x];
-  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * kTY) sRec[e] = param_rec<T>(C)[e];
+  const Tile t = tiles[blockIdx.x];
+  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * TY) sRec[e] = param_rec<T>(C)[e];
   if (tid == 0) {
     for (int b = 0; b < L::kRing; ++b) mbar_init(&bars[b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
   bool aborted;
-  faces_tma_tile<T, NS>(a, maps + t.blk, C, bars, ring, sRec, t, 0u, aborted);
+  faces_tma_tile<T, NS, TY>(a, maps + t.blk, C, bars, ring, sRec, t, 0u, aborted);
 }
 
 // Persistent form of k_faces_tma: as many CTAs as fit on the GPU take the
 // regular tiles in order from a device counter (zeroed before the launch),
 // initialising the NASA records and the mbarriers once; the plane count
 // carries the mbarrier phases from one tile to the next.
-template <typename T, int NS>
-__global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
-    k_faces_tma_persistent(const StageArgs<T> a, const CUtensorMap *__restrict__ maps,
+template <typename T, int NS, int TY>
+__global__ void __launch_bounds__(kTX *TY, (FacesTmaLayout<T, NS, TY>::kMinBlocks))
+    k_faces_tma_persistent(const StageArgs<T> a, const Tile *__restrict__ tiles, const CUtensorMap *__restrict__ maps,
                            const __grid_constant__ ChemParams C, int n_tiles, unsigned *ticket) {
-  using L = FacesTmaLayout<T, NS>;
+  using L = FacesTmaLayout<T, NS, TY>;
   const int ns = SpecCount<NS>::n(C);
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char *smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
@@ -501,7 +533,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   T *sRec = reinterpret_cast<T *>(ring + L::kRing * L::kPlaneBytes);
   __shared__ int sh_tile;
   const int tid = threadIdx.y * kTX + threadIdx.x;
-  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * kTY) sRec[e] = param_rec<T>(C)[e];
+  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * TY) sRec[e] = param_rec<T>(C)[e];
   if (tid == 0) {
     for (int b = 0; b < L::kRing; ++b) mbar_init(&bars[b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -514,7 +546,7 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
     __syncthreads();  // every thread has its tile index before the next ticket
     if (ti >= n_tiles) break;
     bool aborted;
-    pc += (unsigned)faces_tma_tile<T, NS>(a, maps + a.tiles[ti].blk, C, bars, ring, sRec, a.tiles[ti], pc, aborted);
+    pc += (unsigned)faces_tma_tile<T, NS, TY>(a, maps + tiles[ti].blk, C, bars, ring, sRec, tiles[ti], pc, aborted);
     if (aborted) break;
   }
 }

@@ -222,9 +222,10 @@ int cc_tuning(cc_ctx *ctx, int *variant, int *kz, double *stage_ms, int tile[3])
  * split with TMA-staged face planes, 4 = as 3 on persistent CTAs, 5 = faces
  * differenced in the tile (TMA variants: 0 or 9 species; 1 and 5: FP32 bulk
  * precision); kz = k-planes per tile, 0 = autotune; tile_j = points along j
- * of the variant-5 tile (4, 8 or 16; 0 = autotune; the other variants' tiles
- * are 32 x 8).  Before cc_init it applies to the first cc_init; after it,
- * the new configuration is timed and used from the next cc_step on. */
+ * of the TMA face kernel's tile in variants 3-5 (4, 8 or 16, 16 in the FP32
+ * bulk precision only; 0 = autotune; the other kernels' tiles are 32 x 8).
+ * Before cc_init it applies to the first cc_init; after it, the new
+ * configuration is timed and used from the next cc_step on. */
 int cc_set_tuning(cc_ctx *ctx, int variant, int kz, int tile_j);
 /* Launch granularity of the stage kernels: 0 (default) = one launch per
  * kernel over the tiles of every block; 1 = one launch per block per kernel,

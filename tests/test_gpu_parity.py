@@ -168,6 +168,49 @@ def test_dq_variant_tile_shape_and_chunking_are_bit_identical():
             np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("variant", ["split-tma", "split-tma-p"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["multiblock", "channel", "box_distorted"])
+def test_face_tile_heights_are_bit_identical(name, precision, variant):
+    """The TMA face kernel computes every face of a point once, whichever
+    tile (32 x 4, 32 x 8, 32 x 16 points; 32 x 16 in FP32 only) and k-chunk it
+    falls in: the state after two RK3 steps does not depend on the tile
+    shape, bit for bit."""
+    case = CASES[name]
+    shapes = [(8, 4), (4, 2), (4, 64)] + ([(16, 3), (16, 64)] if precision == "mixed" else [])
+    out = []
+    for tile_j, kz in shapes:
+        d = cc.Driver.from_case(case, precision)
+        d.set_tuning(variant, kz, tile_j)
+        d.initialize_computation()
+        assert d.tuning()["tile"] == (32, tile_j, kz)
+        d.simulate(2, "rk3")
+        assert d.status() == 0
+        out.append([d.field[b].get_state()[2] for b in range(len(case["blocks"]))])
+        d.close()
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("tile_j", [4, 16])
+def test_face_tile_heights_close_to_oracle(tile_j):
+    errs, status = compare(CASES["box"], "rk3", 2, "mixed", "split-tma", 3, tile_j)
+    assert status == 0
+    tol = {"res": 5e-3, "dt": 1e-5}
+    bad = {k: v for k, v in errs.items() if not v < tol.get(k, 1e-4)}
+    assert not bad, errs
+
+
+def test_face_tile_height_16_refused_in_fp64():
+    """The 32 x 16 tile's FP64 plane ring does not fit in shared memory."""
+    d = cc.Driver.from_case(CASES["box"], "fp64")
+    d.set_tuning("split-tma", 4, 16)
+    with pytest.raises(RuntimeError, match="does not fit"):
+        d.initialize_computation()
+    d.close()
+
+
 @pytest.mark.parametrize("variant", ["l1", "split", "split-tma", "split-tma-p"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_k_chunking_is_bit_identical(precision, variant):
