@@ -54,6 +54,8 @@ def parse():
                          "timings are distorted)")
     ap.add_argument("--kz", type=int, default=4, help="k-planes per tile when --variant pins the stage kernels")
     ap.add_argument("--tile-j", type=int, default=0, help="points along j of the dq-tma tile when --variant pins it")
+    ap.add_argument("--ref-n", type=int, default=128, help="box size of the reference-kernel timing (0 skips it)")
+    ap.add_argument("--ref-steps", type=int, default=5, help="timed steps of the reference-kernel timing")
     return ap.parse_args()
 
 
@@ -500,6 +502,42 @@ def run_closure(args):
     print(json.dumps(line), flush=True)
 
 
+def reference_kernels_b200(n, steps):
+    """The reference's own CUDA kernels, FP64, timed on this GPU: built from
+    the reference sources into oracle/_ref/ref_harness_ms by
+    oracle/ref_harness/build_ref.sh (with the three patches of its header) and
+    driven by its harness on the n^3 box of the workload's generator.  The
+    harness times `steps` explicit steps after one warm-up step with CUDA
+    events: the per-block kernels of a step alone (the reference's one
+    launch per block per kernel: set_dq_to_0, inviscid and viscous fluxes,
+    local time step, update_cv_and_bv, update_physical_properties), and with
+    the boundary launches and the harness's interface fill.  One explicit step
+    is one stage of work, so Mcell-updates/s per stage = points / step time."""
+    import tempfile
+    from combustioncodegpu_b200 import cases
+    from oracle.ref_harness.case_file import write_case
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness_ms")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_harness_ms is not built (it needs the reference sources)"}
+    case = cases.case_box(n, species=cases.synthetic_species(), seed=1234)
+    case["n_steps"] = 1
+    with tempfile.TemporaryDirectory() as d:
+        cf, of = os.path.join(d, "case.bin"), os.path.join(d, "out.bin")
+        write_case(cf, case)
+        r = subprocess.run([exe, cf, of, "--time", str(steps)], capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return {"unavailable": "harness exit %d: %s" % (r.returncode, (r.stderr or r.stdout).strip()[-200:])}
+    t = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    pts = t["points"]
+    return {"grid": "%d^3 points, same generator and seed as the workload" % n, "precision": "fp64",
+            "steps_timed": steps, "kernels_ms_per_step": t["kernels_ms_per_step"],
+            "step_ms_with_halo_fill": t["step_ms_with_halo_fill"],
+            "value": pts / (t["kernels_ms_per_step"] / 1e3) / 1e6, "unit": "Mcell-updates/s per stage",
+            "timing": "CUDA events around the reference's per-block kernel launches (one explicit step = one "
+                      "stage of work)"}
+
+
 def cpu_baseline(args, n_threads, steps=1, n=64):
     """The oracle on the host cores: bounded sample of the workload (an
     n^3-point box with the same per-point work, `steps` RK3 steps)."""
@@ -589,11 +627,18 @@ def main():
         traffic = ncu_traffic("stage_kernel_box128_mixed")
     achieved = kbpp * mixed["npts"] / (kms / 1e3) / 1e9
     cpu = cpu_baseline(args, os.cpu_count() or 1, steps=2, n=96)
+    refk = reference_kernels_b200(args.ref_n, args.ref_steps) if args.ref_n > 0 else None
+    if refk and "value" in refk:
+        refk["ours_mixed_over_reference"] = value / refk["value"]
+        refk["ours_fp64_over_reference"] = value_plain / refk["value"]
     levels = mixed["info"]["halo_levels"]
-    # per stage: stage kernels, halo node levels, halo copies; per step: the
-    # third stage's post-exchange dt of rewritten interior points, dt finalize
+    # per stage: the stage kernels and the halo program (the node levels in
+    # one cooperative launch, or one per level beyond 8 levels, then one launch
+    # of the copies with the post-exchange time step); per step: the
+    # time-step finalisation
     n_stage = {"l1": 1, "tma": 1, "split": 2, "split-tma": 3, "split-tma-p": 3, "dq-tma": 2}[variant]
-    launches_per_step = 3 * (n_stage + levels + 1) + 2
+    halo = (min(levels, 1) if levels <= 8 else levels) + 1
+    launches_per_step = 3 * (n_stage + halo) + 1
     line = {
         "metric": METRIC, "value": value, "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -615,6 +660,7 @@ def main():
         "cpu_baseline": {"value": cpu["value"], "unit": cpu["unit"], "cores": cpu["cores"], "kind": cpu["kind"],
                          "sample": cpu["sample"]},
         "e2e": e2e,
+        "reference_kernels_b200": refk,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": mixed["clocks"],
         "status": {"mixed": mixed["status"], "fp64": plain["status"]},

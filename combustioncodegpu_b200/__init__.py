@@ -127,7 +127,17 @@ EXPORTS = {
                     ctypes.c_int),
     "cc_residual_rms_noalloc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p],
                                 ctypes.c_int),
+    "cc_set_owned_blocks": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
+    "cc_set_exchange": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "cc_exchange_fields": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "cc_pack_points": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, _dp], ctypes.c_int),
+    "cc_unpack_points": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, _dp], ctypes.c_int),
+    "cc_residual_sums": ([ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
 }
+
+# cc_exchange_fn: int (*)(void *user, int event, int stage, double *value)
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp)
+CC_EXCHANGE_STAGE, CC_EXCHANGE_DT = 0, 1
 
 _lib = None
 

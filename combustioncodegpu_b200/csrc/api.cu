@@ -84,7 +84,7 @@ struct cc_ctx {
   HaloPlan plan;
   HaloNode *d_nodes = nullptr;
   HaloCopy *d_copies = nullptr;
-  int64_t *d_icopies = nullptr;   // copies that rewrite an interior point
+  uint32_t *d_dt_copy_mask = nullptr;  // bit per halo copy: its post-exchange time step enters the next step
   void *sP = nullptr, *sPr = nullptr;
   double *sQ = nullptr;
   int64_t ns_cap = 1;
@@ -126,6 +126,23 @@ struct cc_ctx {
                                   // primitive arenas P[0], P[1] per block
   unsigned *d_ticket = nullptr;   // tile counter of the persistent face kernel
   GridBarrier *d_gridbar = nullptr;  // grid-wide barrier of the single-launch halo program
+  // multi-process runs (cc_set_owned_blocks, cc_set_exchange): the blocks
+  // this process advances, the hook called between a stage's kernels and its
+  // halo program and on the local next time step, the owned blocks' BlockInfo
+  // (interior offsets renumbered over them) for the time step and residual
+  // reductions, and the state buffers the hook's pack / unpack address
+  std::vector<char> owned;        // per block (empty: every block)
+  cc_exchange_fn hook = nullptr;
+  void *hook_user = nullptr;
+  std::vector<BlockInfo> hblocks_owned;
+  BlockInfo *d_blocks_owned = nullptr;
+  int64_t n_int_owned = 0;
+  std::vector<uint32_t> dt_copy_mask;   // bit per copy rewriting an owned block's interior point
+  int x_pn = 1, x_pp = 0;               // P / Pr buffers of the current and previous state during the hook
+  double *x_qn = nullptr, *x_qp = nullptr;
+  double *d_xbuf = nullptr;             // pack / unpack staging [n_fields][cap]
+  int64_t *d_xidx = nullptr;
+  int64_t x_cap = 0;
   bool halo_coop = false;         // the device takes cooperative launches (single-launch halo program)
   LusgsArgs lu{};                 // LU-SGS work arrays (allocated by the first LU-SGS step)
   std::vector<int64_t> lu_hb;     // sweep positions where each hyperplane begins, + end
@@ -264,6 +281,9 @@ void transpose_fields(const double *src, int64_t ng, int nf, std::vector<double>
     }
 }
 
+// Whether this process advances block b (cc_set_owned_blocks).
+bool owns(const cc_ctx *c, int b) { return c->owned.empty() || c->owned[(size_t)b]; }
+
 // Tensor-map plane boxes: tile heights 8 (the kTY tiles of the split and
 // fused kernels, and the dq kernel), 4 and 16 (dq kernel), each plus the
 // 2-point halo on both sides.
@@ -277,6 +297,7 @@ void build_face_tiles(cc_ctx *c, int ty, int kz) {
   for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
     c->ft_begin.push_back((int)c->hftiles.size());
     const auto &b = c->blocks[bi];
+    if (!owns(c, bi)) continue;
     for (int k0 = 0; k0 < b.mz; k0 += kz)
       for (int j0 = 0; j0 < b.my; j0 += ty)
         for (int i0 = 0; i0 < b.mx; i0 += 32) {
@@ -302,6 +323,7 @@ void build_tiles_kz(cc_ctx *c, int kz) {
   for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
     c->tile_begin.push_back((int)c->htiles.size());
     const auto &b = c->blocks[bi];
+    if (!owns(c, bi)) continue;
     for (int k0 = 0; k0 < b.mz; k0 += kz)
       for (int j0 = 0; j0 < b.my; j0 += kTY)
         for (int i0 = 0; i0 < b.mx; i0 += kTX) {
@@ -323,6 +345,7 @@ void build_edge_tiles(cc_ctx *c) {
   for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
     c->edge_begin.push_back((int)c->hedges.size());
     const auto &b = c->blocks[bi];
+    if (!owns(c, bi)) continue;
     for (int k0 = 0; k0 < b.mz; k0 += kTY) {
       for (int j0 = 0; j0 < b.my; j0 += kTX) c->hedges.push_back(Tile{bi, -1, j0, k0, std::min(b.mz, k0 + kTY), 0, 0, 0});
       for (int i0 = 0; i0 < b.mx; i0 += kTX) c->hedges.push_back(Tile{bi, i0, -1, k0, std::min(b.mz, k0 + kTY), 1, 0, 0});
@@ -414,6 +437,54 @@ int build_tensor_maps(cc_ctx *c) {
   return 0;
 }
 
+// After set-up or a change of the owned blocks: the work lists over the
+// owned blocks (stage tiles at the current k-chunk, face tiles at the current
+// tile height, edge tiles), the owned blocks' BlockInfo with interior offsets
+// renumbered over them (time-step and residual reductions), and the halo
+// copies that rewrite an owned interior point (their post-exchange time step).
+int apply_ownership(cc_ctx *c) {
+  build_tiles_kz(c, c->kz);
+  build_face_tiles(c, c->face_ty, c->kz);
+  build_edge_tiles(c);
+  c->hblocks_owned.clear();
+  int64_t off = 0;
+  for (size_t b = 0; b < c->hblocks.size(); ++b)
+    if (owns(c, (int)b)) {
+      BlockInfo B = c->hblocks[b];
+      B.interior_off = off;
+      off += (int64_t)B.mx * B.my * B.mz;
+      c->hblocks_owned.push_back(B);
+    }
+  c->n_int_owned = off;
+  c->dt_copy_mask.assign(c->plan.copies.size() / 32 + 1, 0u);
+  for (int64_t ci : c->plan.interior_copies) {
+    const int64_t dst = c->plan.copies[(size_t)ci].dst;
+    for (size_t b = 0; b < c->hblocks.size(); ++b) {
+      const BlockInfo &B = c->hblocks[b];
+      if (dst >= B.off && dst < B.off + B.ng) {
+        if (owns(c, (int)b)) c->dt_copy_mask[(size_t)(ci >> 5)] |= 1u << (ci & 31);
+        break;
+      }
+    }
+  }
+  if (!c->htiles.empty())
+    CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+  if (!c->hftiles.empty())
+    CK(cudaMemcpyAsync(c->d_ftiles, c->hftiles.data(), sizeof(Tile) * c->hftiles.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+  if (!c->hedges.empty())
+    CK(cudaMemcpyAsync(c->d_edges, c->hedges.data(), sizeof(Tile) * c->hedges.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+  if (!c->hblocks_owned.empty())
+    CK(cudaMemcpyAsync(c->d_blocks_owned, c->hblocks_owned.data(), sizeof(BlockInfo) * c->hblocks_owned.size(),
+                       cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_dt_copy_mask, c->dt_copy_mask.data(), sizeof(uint32_t) * c->dt_copy_mask.size(),
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
 // Arena layout: rows padded to 32 points, every block starting on a
 // 32-point boundary.  Fills each block's extents and offsets and its
 // BlockInfo; returns the arena size (a multiple of 32 points).
@@ -462,6 +533,8 @@ int setup_device(cc_ctx *c) {
   void *p;
   if (dev_alloc(c, &p, sizeof(BlockInfo) * c->hblocks.size())) return CC_ERR_CUDA;
   c->d_blocks = (BlockInfo *)p;
+  if (dev_alloc(c, &p, sizeof(BlockInfo) * c->hblocks.size())) return CC_ERR_CUDA;
+  c->d_blocks_owned = (BlockInfo *)p;
   if (dev_alloc(c, &p, sizeof(Tile) * (size_t)std::max(1, max_tiles(c)))) return CC_ERR_CUDA;
   c->d_tiles = (Tile *)p;
   if (dev_alloc(c, &p, sizeof(Tile) * (size_t)std::max(1, max_face_tiles(c)))) return CC_ERR_CUDA;
@@ -516,11 +589,8 @@ int setup_device(cc_ctx *c) {
   c->d_nodes = (HaloNode *)p;
   if (dev_alloc(c, &p, sizeof(HaloCopy) * std::max<size_t>(1, c->plan.copies.size()))) return CC_ERR_CUDA;
   c->d_copies = (HaloCopy *)p;
-  if (dev_alloc(c, &p, sizeof(int64_t) * std::max<size_t>(1, c->plan.interior_copies.size()))) return CC_ERR_CUDA;
-  c->d_icopies = (int64_t *)p;
-  if (!c->plan.interior_copies.empty())
-    CK(cudaMemcpyAsync(c->d_icopies, c->plan.interior_copies.data(),
-                       sizeof(int64_t) * c->plan.interior_copies.size(), cudaMemcpyHostToDevice, c->stream));
+  if (dev_alloc(c, &p, sizeof(uint32_t) * (c->plan.copies.size() / 32 + 1))) return CC_ERR_CUDA;
+  c->d_dt_copy_mask = (uint32_t *)p;
   if (dev_alloc(c, &p, sizeof(BcDevice) * std::max<size_t>(1, c->bcs.size()))) return CC_ERR_CUDA;
   c->d_bcs = (BcDevice *)p;
   if (dev_alloc(c, &p, sizeof(double) * 4)) return CC_ERR_CUDA;
@@ -529,7 +599,7 @@ int setup_device(cc_ctx *c) {
   c->d_dt_next = (unsigned long long *)p;
   if (dev_alloc(c, &p, sizeof(unsigned) * 4)) return CC_ERR_CUDA;
   c->d_status = (unsigned *)p;
-  if (dev_alloc(c, &p, sizeof(double) * 4)) return CC_ERR_CUDA;
+  if (dev_alloc(c, &p, sizeof(double) * 8)) return CC_ERR_CUDA;  // norms, then their sums of squares
   c->d_res = (double *)p;
   if (dev_alloc(c, &p, sizeof(double) * 4 * c->n_partials)) return CC_ERR_CUDA;
   c->d_partials = (double *)p;
@@ -566,6 +636,7 @@ int setup_device(cc_ctx *c) {
   const unsigned long long inf_bits = 0x7ff0000000000000ull;
   CK(cudaMemcpyAsync(c->d_dt_next, &inf_bits, sizeof inf_bits, cudaMemcpyHostToDevice, c->stream));
   if (int r = upload_bcs(c)) return r;
+  if (int r = apply_ownership(c)) return r;
 
   // geometry: user layout -> FP64 staging -> bulk precision
   CK(cudaMemsetAsync(c->stage64, 0, sizeof(double) * N * 10, c->stream));
@@ -573,6 +644,34 @@ int setup_device(cc_ctx *c) {
     if (int r = copy_fields_h2d(c, c->blocks[b], c->h_geo[b].data(), c->stage64, 10)) return r;
   if (int r = from64(c, c->stage64, c->G, N * 10)) return r;
   CK(cudaMemsetAsync(c->stage64, 0, sizeof(double) * N * std::max(np_of(c), 10), c->stream));
+  return 0;
+}
+
+// Multi-process hooks (cc_set_exchange).  Stage: with the stage's kernels
+// done, the hook moves the halo sources between processes (cc_pack_points /
+// cc_unpack_points address the buffers recorded here).  Time step: the local
+// next time step (the bit pattern the atomicMin reduction keeps) is replaced
+// by the hook's minimum over processes.
+int exchange_stage(cc_ctx *c, int stage, int pn, int pp, double *qn, double *qp) {
+  if (!c->hook) return 0;
+  c->x_pn = pn, c->x_pp = pp, c->x_qn = qn, c->x_qp = qp;
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->hook(c->hook_user, CC_EXCHANGE_STAGE, stage, nullptr) != 0)
+    return fail(CC_ERR_STATE, "exchange hook failed at stage " + std::to_string(stage));
+  return 0;
+}
+
+int exchange_dt(cc_ctx *c) {
+  if (!c->hook) return 0;
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->d_dt_next, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double v;
+  std::memcpy(&v, &bits, sizeof v);
+  if (c->hook(c->hook_user, CC_EXCHANGE_DT, 0, &v) != 0) return fail(CC_ERR_STATE, "exchange hook failed on dt");
+  std::memcpy(&bits, &v, sizeof v);
+  CK(cudaMemcpyAsync(c->d_dt_next, &bits, sizeof bits, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));  // bits is a local
   return 0;
 }
 
@@ -593,17 +692,16 @@ HaloArgs<T> halo_args(cc_ctx *c, int pn, int pp, double *qn, const double *qp) {
   h.bcs = c->d_bcs;
   h.nodes = c->d_nodes;
   h.copies = c->d_copies;
-  h.icopies = c->d_icopies;
-  h.n_icopies = (int64_t)c->plan.interior_copies.size();
+  h.dt_copy_mask = c->d_dt_copy_mask;
   return h;
 }
 
-// The halo program after a stage: one cooperative launch of the whole
-// program (node levels, copies, the zeroing of |V| at wall faces when vel is
-// given, the post-exchange time step), or, in the per-block launch mode (the
-// reference's granularity) and for programs of more than kHaloMaxLevels node
-// levels, one launch per level, one for the copies (and time step) and one for
-// |V|.  Both run the same device functions: identical results.
+// The halo program after a stage: the node levels (one cooperative launch
+// with a grid barrier between levels, or, in the per-block launch mode of the
+// reference's granularity and for programs of more than kHaloMaxLevels
+// levels, one launch per level), then one launch for the copies, the
+// post-exchange time step and the zeroing of |V| at wall faces (vel).  Both
+// forms run the same device functions: identical results.
 template <typename T, int NS>
 int run_halo(cc_ctx *c, int pn, int pp, double *qn, const double *qp, unsigned long long *dt_next = nullptr,
              double *vel = nullptr) {
@@ -612,22 +710,19 @@ int run_halo(cc_ctx *c, int pn, int pp, double *qn, const double *qp, unsigned l
   h.dt_next = dt_next;
   const auto &lb = c->plan.level_begin;
   const int n_levels = lb.empty() ? 0 : (int)lb.size() - 1;
-  if (!c->per_block && c->halo_coop && n_levels <= kHaloMaxLevels) {
+  if (n_levels > 0 && !c->per_block && c->halo_coop && n_levels <= kHaloMaxLevels) {
     HaloLevels lv{};
     lv.n = n_levels;
     for (int l = 0; l <= n_levels; ++l) lv.begin[l] = lb[l];
-    h.begin = 0, h.end = (int64_t)c->plan.copies.size();
-    CK((Launch<T, NS>::halo_all(h, c->chem, lv, vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->d_gridbar,
-                                c->d_status, c->stream)));
-    return 0;
-  }
-  for (size_t l = 0; l + 1 < lb.size(); ++l) {
-    h.begin = lb[l], h.end = lb[l + 1];
-    CK((Launch<T, NS>::halo_nodes(h, c->chem, c->stream)));
+    CK((Launch<T, NS>::halo_levels(h, c->chem, lv, c->d_gridbar, c->d_status, c->stream)));
+  } else {
+    for (int l = 0; l < n_levels; ++l) {
+      h.begin = lb[l], h.end = lb[l + 1];
+      CK((Launch<T, NS>::halo_nodes(h, c->chem, c->stream)));
+    }
   }
   h.begin = 0, h.end = (int64_t)c->plan.copies.size();
-  CK((Launch<T, NS>::halo_copies(h, c->chem, c->stream)));
-  if (vel) CK(launch_zero_points(vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream));
+  CK((Launch<T, NS>::halo_copies(h, c->chem, vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream)));
   return 0;
 }
 
@@ -651,12 +746,12 @@ int derive_state(cc_ctx *c) {
   CK((Launch<T, NS>::props_all(c->chem, (const T *)c->P[0], (T *)c->Pr[0], N, c->stream)));
   CK(cudaMemcpyAsync(c->P[1], c->P[0], c->elem * N * np_of(c), cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->Pr[1], c->Pr[0], c->elem * N * npr_of(c), cudaMemcpyDeviceToDevice, c->stream));
-  if (int r = run_halo<T, NS>(c, 1, 0, c->Q[0], c->Q[1])) return r;
-  CK(launch_zero_points(c->d_vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream));
+  if (int r = run_halo<T, NS>(c, 1, 0, c->Q[0], c->Q[1], nullptr, c->d_vel)) return r;
   c->cur = 1;
   // inflow transport properties: evaluated once by the same point function
-  CK((Launch<T, NS>::dt_reduce(c->chem, c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[1],
-                               (const T *)c->Pr[1], (const T *)c->G, N, c->n_int, c->d_dt_next, c->stream)));
+  CK((Launch<T, NS>::dt_reduce(c->chem, c->d_blocks_owned, (int)c->hblocks_owned.size(), (const T *)c->P[1],
+                               (const T *)c->Pr[1], (const T *)c->G, N, c->n_int_owned, c->d_dt_next, c->stream)));
+  if (int r = exchange_dt(c)) return r;
   CK(launch_dt_finalize(c->d_dt, c->d_dt_next, c->d_status, nullptr, c->stream));
   c->state_dirty = false;
   return 0;
@@ -803,9 +898,10 @@ int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, i
 // The closure transport of the new state (when on), the end of the stage's
 // timing bracket and the halo program.
 template <typename T, int NS>
-int after_stage(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin) {
+int after_stage(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin, int stage = 0) {
   if (c->closure_on) CK((Launch<T, NS>::props_mlp(a.Pn, a.Prn, c->N, &c->cl, c->d_status, c->chem, c->stream)));
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
+  if (int r = exchange_stage(c, stage, pn, pc, qout, const_cast<double *>(qin))) return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
   if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next, a.vel ? c->d_vel : nullptr)) return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
@@ -813,11 +909,12 @@ int after_stage(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, 
 }
 
 template <typename T, int NS>
-int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin) {
+int stage_and_halo(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, const double *qin,
+                   int stage = 0) {
   const int nt = (int)c->htiles.size();
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
   if (int r = launch_stage<T, NS>(c, a, pc, c->variant, nt)) return r;
-  return after_stage<T, NS>(c, a, pn, pc, qout, qin);
+  return after_stage<T, NS>(c, a, pn, pc, qout, qin, stage);
 }
 
 // LU-SGS steady step (lusgs.cuh): the face fluxes of the current state (the
@@ -1064,13 +1161,15 @@ int enqueue_step(cc_ctx *c, int scheme) {
     a.a = A[st], a.b = Bc[st], a.local_dt = 0;
     a.dt_next = (st == 2 && !dt_after) ? c->d_dt_next : nullptr;
     a.vel = st == 2 ? c->d_vel : nullptr;
-    if (int r = stage_and_halo<T, NS>(c, a, pn, pc, qout, qin)) return r;
+    if (int r = stage_and_halo<T, NS>(c, a, pn, pc, qout, qin, st)) return r;
     c->cur = pn;
   }
   if (dt_after)
-    CK((Launch<T, NS>::dt_reduce(c->chem, c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur],
-                                 (const T *)c->Pr[c->cur], (const T *)c->G, c->N, c->n_int, c->d_dt_next,
+    CK((Launch<T, NS>::dt_reduce(c->chem, c->d_blocks_owned, (int)c->hblocks_owned.size(),
+                                 (const T *)c->P[c->cur], (const T *)c->Pr[c->cur], (const T *)c->G, c->N,
+                                 c->n_int_owned, c->d_dt_next,
                                  c->stream)));
+  if (int r = exchange_dt(c)) return r;  // minimum over processes (multi-process runs)
   CK(launch_dt_finalize(c->d_dt, c->d_dt_next, c->d_status, c->d_dt + 1, c->stream));
   return 0;
 }
@@ -1083,7 +1182,7 @@ void destroy_graphs(cc_ctx *c) {
 
 template <typename T, int NS>
 int step_once(cc_ctx *c, int scheme) {
-  if (!c->use_graph) return enqueue_step<T, NS>(c, scheme);
+  if (!c->use_graph || c->hook) return enqueue_step<T, NS>(c, scheme);  // the hook runs on the host between launches
   cudaGraphExec_t &ge = c->graph[scheme][c->cur];
   if (!ge) {
     const int cur0 = c->cur;
@@ -1121,6 +1220,58 @@ int validate_params(const cc_params *p) {
 }
 
 int check_ctx(cc_ctx *c) { return c ? 0 : fail(CC_ERR_ARG, "context is null"); }
+
+// The staging buffers of cc_pack_points / cc_unpack_points, grown to n points
+// (host-side exchange calls between launches, outside any capture).
+int exchange_staging(cc_ctx *c, int64_t n) {
+  if (n <= c->x_cap) return 0;
+  const int nf = np_of(c) + npr_of(c) + nv_of(c);
+  if (c->d_xbuf) cudaFree(c->d_xbuf), c->d_xbuf = nullptr;
+  if (c->d_xidx) cudaFree(c->d_xidx), c->d_xidx = nullptr;
+  c->x_cap = 0;
+  CK(cudaMalloc((void **)&c->d_xbuf, sizeof(double) * (size_t)(nf * n)));
+  CK(cudaMalloc((void **)&c->d_xidx, sizeof(int64_t) * (size_t)n));
+  c->x_cap = n;
+  return 0;
+}
+
+// cc_pack_points / cc_unpack_points: all fields of the listed points of the
+// state the halo program reads as current (which 0) or previous (which 1),
+// between the device arenas and [n_fields][n] FP64 host rows.
+int pack_unpack(cc_ctx *c, int which, const int64_t *idx, int64_t n, double *host, bool pack) {
+  if (int r = check_ctx(c)) return r;
+  if (!c->initialized) return fail(CC_ERR_STATE, "cc_pack_points / cc_unpack_points before cc_init");
+  if (which != 0 && which != 1) return fail(CC_ERR_ARG, "which must be 0 (current) or 1 (previous)");
+  if (n < 0 || (n > 0 && (!idx || !host))) return fail(CC_ERR_ARG, "null index or value array");
+  if (n == 0) return 0;
+  for (int64_t i = 0; i < n; ++i)
+    if (idx[i] < 0 || idx[i] >= c->N) return fail(CC_ERR_ARG, "point index outside the arena");
+  double *Q = which == 0 ? c->x_qn : c->x_qp;
+  if (!Q) return fail(CC_ERR_STATE, "cc_pack_points / cc_unpack_points outside an exchange hook call");
+  if (int r = exchange_staging(c, n)) return r;
+  const int np = np_of(c), npr = npr_of(c), nv = nv_of(c), nf = np + npr + nv;
+  void *P = c->P[which == 0 ? c->x_pn : c->x_pp], *Pr = c->Pr[which == 0 ? c->x_pn : c->x_pp];
+  CK(cudaMemcpyAsync(c->d_xidx, idx, sizeof(int64_t) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  double *bP = c->d_xbuf, *bPr = bP + (size_t)np * n, *bQ = bPr + (size_t)npr * n;
+  const bool f32 = c->elem == 4;
+  if (pack) {
+    CK(f32 ? launch_gather_points<float>((const float *)P, c->N, np, c->d_xidx, n, bP, c->stream)
+           : launch_gather_points<double>((const double *)P, c->N, np, c->d_xidx, n, bP, c->stream));
+    CK(f32 ? launch_gather_points<float>((const float *)Pr, c->N, npr, c->d_xidx, n, bPr, c->stream)
+           : launch_gather_points<double>((const double *)Pr, c->N, npr, c->d_xidx, n, bPr, c->stream));
+    CK(launch_gather_points<double>(Q, c->N, nv, c->d_xidx, n, bQ, c->stream));
+    CK(cudaMemcpyAsync(host, c->d_xbuf, sizeof(double) * (size_t)(nf * n), cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    CK(cudaMemcpyAsync(c->d_xbuf, host, sizeof(double) * (size_t)(nf * n), cudaMemcpyHostToDevice, c->stream));
+    CK(f32 ? launch_scatter_points<float>((float *)P, c->N, np, c->d_xidx, n, bP, c->stream)
+           : launch_scatter_points<double>((double *)P, c->N, np, c->d_xidx, n, bP, c->stream));
+    CK(f32 ? launch_scatter_points<float>((float *)Pr, c->N, npr, c->d_xidx, n, bPr, c->stream)
+           : launch_scatter_points<double>((double *)Pr, c->N, npr, c->d_xidx, n, bPr, c->stream));
+    CK(launch_scatter_points<double>(Q, c->N, nv, c->d_xidx, n, bQ, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
 
 }  // namespace
 
@@ -1169,6 +1320,8 @@ int cc_destroy(cc_ctx *c) {
   for (auto e : c->ev_halo) cudaEventDestroy(e);
   for (auto e : c->ev_mid) cudaEventDestroy(e);
   for (void *p : c->allocs) cudaFree(p);
+  if (c->d_xbuf) cudaFree(c->d_xbuf);
+  if (c->d_xidx) cudaFree(c->d_xidx);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -1346,6 +1499,8 @@ int cc_step(cc_ctx *c, int n_steps, int scheme, int want_residual) {
   if (scheme != CC_RK3 && scheme != CC_STEADY_EULER && scheme != CC_STEADY_LUSGS)
     return fail(CC_ERR_ARG, "unknown time scheme");
   if (n_steps < 0) return fail(CC_ERR_ARG, "n_steps must be >= 0");
+  if (scheme == CC_STEADY_LUSGS && (c->hook || !c->owned.empty()))
+    return fail(CC_ERR_STATE, "the LU-SGS step sweeps every block in one order: not available in multi-process runs");
   if (scheme == CC_STEADY_LUSGS)
     if (int r = lusgs_alloc(c)) return r;
   if (c->state_dirty) {
@@ -1358,13 +1513,13 @@ int cc_step(cc_ctx *c, int n_steps, int scheme, int want_residual) {
     constexpr int NS = decltype(nn)::value;
     for (int s = 0; s < n_steps; ++s) {
       if (want_residual && s == n_steps - 1)
-        CK(launch_store_last<T>(c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur], c->d_vel, c->N,
-                                c->n_int, c->d_last, c->stream));
+        CK(launch_store_last<T>(c->d_blocks_owned, (int)c->hblocks_owned.size(), (const T *)c->P[c->cur],
+                                c->d_vel, c->N, c->n_int_owned, c->d_last, c->stream));
       if (int r = step_once<T, NS>(c, scheme)) return r;
     }
     if (want_residual && n_steps > 0)
-      CK(launch_residual<T>(c->d_blocks, (int)c->hblocks.size(), (const T *)c->P[c->cur], c->d_vel, c->N,
-                            c->n_int, c->d_last, c->d_partials, c->n_partials, c->d_res, c->stream));
+      CK(launch_residual<T>(c->d_blocks_owned, (int)c->hblocks_owned.size(), (const T *)c->P[c->cur], c->d_vel,
+                            c->N, c->n_int_owned, c->d_last, c->d_partials, c->n_partials, c->d_res, c->stream));
     return 0;
   });
 }
@@ -1849,6 +2004,57 @@ int cc_set_launch_mode(cc_ctx *c, int per_block) {
   if (int r = check_ctx(c)) return r;
   c->per_block = per_block != 0;
   destroy_graphs(c);
+  return 0;
+}
+
+int cc_set_owned_blocks(cc_ctx *c, const int *blocks, int n) {
+  if (int r = check_ctx(c)) return r;
+  std::vector<char> owned;
+  if (n > 0) {
+    if (!blocks) return fail(CC_ERR_ARG, "cc_set_owned_blocks: blocks is null");
+    owned.assign(c->blocks.size(), 0);
+    for (int i = 0; i < n; ++i) {
+      if (blocks[i] < 0 || blocks[i] >= (int)c->blocks.size())
+        return fail(CC_ERR_ARG, "cc_set_owned_blocks: no block " + std::to_string(blocks[i]));
+      owned[(size_t)blocks[i]] = 1;
+    }
+  }
+  c->owned = owned;
+  if (!c->initialized) return 0;
+  destroy_graphs(c);
+  return apply_ownership(c);
+}
+
+int cc_set_exchange(cc_ctx *c, cc_exchange_fn fn, void *user) {
+  if (int r = check_ctx(c)) return r;
+  c->hook = fn;
+  c->hook_user = user;
+  destroy_graphs(c);
+  return 0;
+}
+
+int cc_exchange_fields(cc_ctx *c, int *n_fields) {
+  if (int r = check_ctx(c)) return r;
+  if (!n_fields) return fail(CC_ERR_ARG, "n_fields is null");
+  *n_fields = np_of(c) + npr_of(c) + nv_of(c);
+  return 0;
+}
+
+int cc_pack_points(cc_ctx *c, int which, const int64_t *idx, int64_t n, double *out) {
+  return pack_unpack(c, which, idx, n, out, true);
+}
+
+int cc_unpack_points(cc_ctx *c, int which, const int64_t *idx, int64_t n, const double *in) {
+  return pack_unpack(c, which, idx, n, const_cast<double *>(in), false);
+}
+
+int cc_residual_sums(cc_ctx *c, double sums[4], int64_t *count) {
+  if (int r = check_ctx(c)) return r;
+  if (!c->initialized) return fail(CC_ERR_STATE, "cc_residual_sums before cc_init");
+  if (!sums || !count) return fail(CC_ERR_ARG, "null output");
+  CK(cudaMemcpyAsync(sums, c->d_res + 4, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *count = c->n_int_owned;
   return 0;
 }
 

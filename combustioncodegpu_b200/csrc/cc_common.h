@@ -253,8 +253,8 @@ struct HaloArgs {
   const BcDevice *bcs;
   const HaloNode *nodes;
   const HaloCopy *copies;
-  const int64_t *icopies;         // copies that rewrite an interior point (their post-exchange time step)
-  int64_t n_icopies;
+  const uint32_t *dt_copy_mask;   // bit per copy: it rewrites an interior point of an owned block, whose
+                                  // post-exchange time step enters the next global step
   int64_t begin, end;
   const T *G;                     // geometry (time step of rewritten interior points)
   unsigned long long *dt_next;    // next global time step, or null

@@ -276,35 +276,32 @@ cudaError_t Launch<T, NS>::halo_nodes(const HaloArgs<T> &a, const ChemParams &C,
 }
 
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s) {
-  const int64_t n = a.end - a.begin;
+cudaError_t Launch<T, NS>::halo_copies(const HaloArgs<T> &a, const ChemParams &C, double *vel,
+                                       const int64_t *vel_zero, int64_t n_vel_zero, cudaStream_t s) {
+  const int64_t n = std::max<int64_t>(a.end - a.begin, vel ? n_vel_zero : 0);
   if (n <= 0) return cudaSuccess;
   const int ns = C.ns, np = 6 + ns, npr = 2 + ns, nq = 5 + ns;
   const int tpb = 256;
-  k_halo_copy_fields<T, NS><<<dim3((unsigned)((n + tpb - 1) / tpb), 3), tpb, 0, s>>>(a, np, npr, nq);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || !a.dt_next || a.n_icopies <= 0) return e;
-  k_halo_copy_dt<T, NS><<<(unsigned)((a.n_icopies + tpb - 1) / tpb), tpb, 0, s>>>(a, C);
+  k_halo_copy_fields<T, NS><<<dim3((unsigned)((n + tpb - 1) / tpb), 3), tpb, 0, s>>>(a, C, np, npr, nq, vel,
+                                                                                      vel_zero, n_vel_zero);
   return cudaGetLastError();
 }
 
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::halo_all(const HaloArgs<T> &a, const ChemParams &C, const HaloLevels &lv, double *vel,
-                                    const int64_t *vel_zero, int64_t n_vel_zero, GridBarrier *bar, unsigned *status,
-                                    cudaStream_t s) {
-  const int tpb = 256;
+cudaError_t Launch<T, NS>::halo_levels(const HaloArgs<T> &a, const ChemParams &C, const HaloLevels &lv,
+                                       GridBarrier *bar, unsigned *status, cudaStream_t s) {
+  const int tpb = 128;
   static int capacity = 0;  // CTAs that fit on the device at once
   if (capacity == 0) {
     int dev = 0, n_sm = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_halo_all<T, NS>, tpb, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_halo_levels<T, NS>, tpb, 0);
     capacity = std::max(1, n_sm * per_sm);
   }
-  int64_t work = std::max<int64_t>(3 * (a.end - a.begin), std::max<int64_t>(a.n_icopies, n_vel_zero));
+  int64_t work = 1;
   for (int l = 0; l < lv.n; ++l) work = std::max(work, lv.begin[l + 1] - lv.begin[l]);
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(capacity, (work + tpb - 1) / tpb));
-  const int ns = C.ns, np = 6 + ns, npr = 2 + ns, nq = 5 + ns;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)grid);
   cfg.blockDim = dim3(tpb);
@@ -315,7 +312,7 @@ cudaError_t Launch<T, NS>::halo_all(const HaloArgs<T> &a, const ChemParams &C, c
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_halo_all<T, NS>, a, C, lv, np, npr, nq, vel, vel_zero, n_vel_zero, bar, status);
+  return cudaLaunchKernelEx(&cfg, k_halo_levels<T, NS>, a, C, lv, bar, status);
 }
 
 template <typename T, int NS>

@@ -52,12 +52,13 @@ struct Launch {
   static cudaError_t lusgs_update(const StageArgs<T> &a, const LusgsArgs &L, const ChemParams &C, int n_tiles,
                                   cudaStream_t s);
   static cudaError_t halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
-  static cudaError_t halo_copies(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
-  // the whole halo program (node levels, copies, |V| zeroing at wall faces,
-  // post-exchange time step) in one cooperative launch (k_halo_all)
-  static cudaError_t halo_all(const HaloArgs<T> &a, const ChemParams &C, const HaloLevels &lv, double *vel,
-                              const int64_t *vel_zero, int64_t n_vel_zero, GridBarrier *bar, unsigned *status,
-                              cudaStream_t s);
+  // the copies of the halo program, with the post-exchange time step
+  // (a.dt_next) and the zeroing of |V| at wall faces (vel, when not null)
+  static cudaError_t halo_copies(const HaloArgs<T> &a, const ChemParams &C, double *vel, const int64_t *vel_zero,
+                                 int64_t n_vel_zero, cudaStream_t s);
+  // every node level of the halo program in one cooperative launch
+  static cudaError_t halo_levels(const HaloArgs<T> &a, const ChemParams &C, const HaloLevels &lv, GridBarrier *bar,
+                                 unsigned *status, cudaStream_t s);
   static cudaError_t cv_from_bv(const ChemParams &C, const double *P0, double *Q, int64_t N, double *vel,
                                 cudaStream_t s);
   static cudaError_t props_all(const ChemParams &C, const T *P, T *Pr, int64_t N, cudaStream_t s);
@@ -84,6 +85,12 @@ cudaError_t launch_convert_f2d(const float *src, double *dst, int64_t n, cudaStr
 cudaError_t launch_dt_finalize(double *dt, unsigned long long *dt_next, unsigned *status, double *dt_hist,
                                cudaStream_t s);
 cudaError_t launch_zero_points(double *field, const int64_t *points, int64_t n, cudaStream_t s);
+template <typename T>
+cudaError_t launch_gather_points(const T *src, int64_t N, int nf, const int64_t *idx, int64_t n, double *out,
+                                 cudaStream_t s);
+template <typename T>
+cudaError_t launch_scatter_points(T *dst, int64_t N, int nf, const int64_t *idx, int64_t n, const double *in,
+                                  cudaStream_t s);
 template <typename T>
 cudaError_t launch_store_last(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
                               int64_t n_interior, double *bv_last, cudaStream_t s);

@@ -163,7 +163,7 @@ __global__ void k_residual_final(const double *partials, int n_partials, int64_t
 #pragma unroll
   for (int l = 0; l < 4; ++l) {
     const double w = warp_sum(r[l]);
-    if (lane == 0) res[l] = sqrt(w / (double)n_int);
+    if (lane == 0) res[l] = sqrt(w / (double)n_int), res[4 + l] = w;  // the norm, and the sum it came from
   }
 }
 
@@ -183,6 +183,49 @@ cudaError_t launch_residual(const BlockInfo *blocks, int nblocks, const T *P, co
   k_residual_final<<<1, 32, 0, s>>>(partials, n_partials, n_interior, res);
   return cudaGetLastError();
 }
+
+// Multi-process exchange: nf fields (stride N) of the points idx[0..n) into
+// FP64 rows of out (stride n), and back; FP32 values round-trip exactly.
+template <typename T>
+__global__ void k_gather_points(const T *src, int64_t N, int nf, const int64_t *idx, int64_t n, double *out) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= n * nf) return;
+  const int64_t f = e / n, i = e % n;
+  out[e] = (double)src[f * N + idx[i]];
+}
+
+template <typename T>
+__global__ void k_scatter_points(T *dst, int64_t N, int nf, const int64_t *idx, int64_t n, const double *in) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= n * nf) return;
+  const int64_t f = e / n, i = e % n;
+  dst[f * N + idx[i]] = (T)in[e];
+}
+
+template <typename T>
+cudaError_t launch_gather_points(const T *src, int64_t N, int nf, const int64_t *idx, int64_t n, double *out,
+                                 cudaStream_t s) {
+  if (n <= 0 || nf <= 0) return cudaSuccess;
+  k_gather_points<T><<<(unsigned)((n * nf + 255) / 256), 256, 0, s>>>(src, N, nf, idx, n, out);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_scatter_points(T *dst, int64_t N, int nf, const int64_t *idx, int64_t n, const double *in,
+                                  cudaStream_t s) {
+  if (n <= 0 || nf <= 0) return cudaSuccess;
+  k_scatter_points<T><<<(unsigned)((n * nf + 255) / 256), 256, 0, s>>>(dst, N, nf, idx, n, in);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_gather_points<double>(const double *, int64_t, int, const int64_t *, int64_t, double *,
+                                                  cudaStream_t);
+template cudaError_t launch_gather_points<float>(const float *, int64_t, int, const int64_t *, int64_t, double *,
+                                                 cudaStream_t);
+template cudaError_t launch_scatter_points<double>(double *, int64_t, int, const int64_t *, int64_t, const double *,
+                                                   cudaStream_t);
+template cudaError_t launch_scatter_points<float>(float *, int64_t, int, const int64_t *, int64_t, const double *,
+                                                  cudaStream_t);
 
 template cudaError_t launch_store_last<double>(const BlockInfo *, int, const double *, const double *, int64_t,
                                                int64_t, double *, cudaStream_t);

@@ -746,11 +746,33 @@ __global__ void k_halo_nodes(const HaloArgs<T> a, const __grid_constant__ ChemPa
 // Consecutive threads take consecutive copies, whose destinations (and
 // mostly sources) are consecutive, so every field access is coalesced; the
 // copy record is read once per array rather than once per field.
+// Interior points rewritten by phase B (coincident interface layers)
+// contribute their post-exchange local time step to the next global step,
+// as the reference evaluates the step after the exchange (Driver.cu:150-163):
+// the thread that copies a flagged copy's primitives evaluates it from the
+// values it has just written (and the source's viscosity, which the
+// transport copy writes to the same point).
 template <typename T, int NS>
-__device__ __forceinline__ void halo_copy(const HaloArgs<T> &a, int64_t e, int which, int np, int npr, int nq) {
+__device__ __forceinline__ double halo_copy_dt(const HaloArgs<T> &a, const ChemParams &C, const HaloCopy &c,
+                                               const T *v, T mu) {
+  constexpr int A = SpecCount<NS>::kArr;
+  const int ns = SpecCount<NS>::n(C);
+  T Y[A], gam, cs;
+#pragma unroll
+  for (int l = 0; l < A; ++l)
+    if (l < ns) Y[l] = v[6 + l];
+  gamma_and_c<T, NS>(C, param_rec<T>(C), v[5], Y, gam, cs);
+  return local_time_step<T>(C, a.G, a.N, c.dst, (double)v[0], (double)v[1], (double)v[2], (double)v[3], (double)cs,
+                            (double)gam, (double)mu, (c.src.pad & 2) != 0);
+}
+
+template <typename T, int NS>
+__device__ __forceinline__ double halo_copy(const HaloArgs<T> &a, const ChemParams &C, int64_t e, int which,
+                                            int np, int npr, int nq) {
   constexpr int A = SpecCount<NS>::kArr;
   const HaloCopy c = a.copies[a.begin + e];
   const RefPtrs<T> r = resolve(a, c.src);
+  double dt = 1e300;
   if (which == 0) {
     T v[6 + A];
 #pragma unroll
@@ -759,6 +781,8 @@ __device__ __forceinline__ void halo_copy(const HaloArgs<T> &a, int64_t e, int w
 #pragma unroll
     for (int f = 0; f < 6 + A; ++f)
       if (f < np) a.P[f * a.N + c.dst] = v[f];
+    if (a.dt_next && ((a.dt_copy_mask[e >> 5] >> (e & 31)) & 1u))
+      dt = halo_copy_dt<T, NS>(a, C, c, v, r.Pr[r.idx]);
   } else if (which == 1) {
     T v[2 + A];
 #pragma unroll
@@ -776,41 +800,26 @@ __device__ __forceinline__ void halo_copy(const HaloArgs<T> &a, int64_t e, int w
     for (int f = 0; f < 5 + A; ++f)
       if (f < nq) a.Q[f * a.N + c.dst] = v[f];
   }
+  return dt;
 }
 
+// Phase B in one launch: every changed point from its resolved source (grid
+// y selects P, Pr or Q; consecutive threads take consecutive copies), the
+// post-exchange time step of the rewritten interior points (a.dt_next), and
+// the zeroing of |V| at wall-face points (vel).
 template <typename T, int NS>
-__global__ void k_halo_copy_fields(const HaloArgs<T> a, int np, int npr, int nq) {
+__global__ void k_halo_copy_fields(const HaloArgs<T> a, const __grid_constant__ ChemParams C, int np, int npr,
+                                   int nq, double *vel, const int64_t *vel_zero, int64_t n_vel_zero) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // copy (grid x)
-  if (e >= a.end - a.begin) return;
-  halo_copy<T, NS>(a, e, blockIdx.y, np, npr, nq);  // grid y selects P, Pr or Q
-}
-
-// Interior points rewritten by phase B (coincident interface layers)
-// contribute their post-exchange local time step to the next global step,
-// as the reference evaluates the step after the exchange (Driver.cu:150-163).
-template <typename T, int NS>
-__device__ __forceinline__ double halo_copy_dt_point(const HaloArgs<T> &a, const ChemParams &C, int64_t e) {
-  constexpr int A = SpecCount<NS>::kArr;
-  const int ns = SpecCount<NS>::n(C);
-  const HaloCopy c = a.copies[a.icopies[e]];
-  const int64_t p = c.dst, N = a.N;
-  T Y[A], gam, cs;
+  double dt = 1e300;
+  if (e < a.end - a.begin) dt = halo_copy<T, NS>(a, C, e, blockIdx.y, np, npr, nq);
+  if (a.dt_next && blockIdx.y == 0) {
 #pragma unroll
-  for (int l = 0; l < A; ++l)
-    if (l < ns) Y[l] = a.P[(6 + l) * N + p];
-  gamma_and_c<T, NS>(C, param_rec<T>(C), a.P[5 * N + p], Y, gam, cs);
-  return local_time_step<T>(C, a.G, N, p, (double)a.P[p], (double)a.P[N + p], (double)a.P[2 * N + p],
-                            (double)a.P[3 * N + p], (double)cs, (double)gam, (double)a.Pr[p], (c.src.pad & 2) != 0);
-}
-
-template <typename T, int NS>
-__global__ void k_halo_copy_dt(const HaloArgs<T> a, const __grid_constant__ ChemParams C) {
-  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  double dt_min = 1e300;
-  if (e < a.n_icopies) dt_min = halo_copy_dt_point<T, NS>(a, C, e);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) dt_min = fmin(dt_min, __shfl_xor_sync(0xffffffffu, dt_min, o));
-  if ((threadIdx.x & 31) == 0) atomic_min_pos_double(a.dt_next, dt_min);
+    for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
+    if ((threadIdx.x & 31) == 0) atomic_min_pos_double(a.dt_next, dt);
+  }
+  if (vel && blockIdx.y == 2)
+    for (int64_t z = e; z < n_vel_zero; z += (int64_t)gridDim.x * blockDim.x) vel[vel_zero[z]] = 0.0;
 }
 
 // Bounded grid-wide barrier of a cooperative launch (every CTA resident):
@@ -848,43 +857,23 @@ __device__ __forceinline__ bool grid_sync_bounded(GridBarrier *bar, long long ma
   return ok_sh != 0;
 }
 
-// The whole halo program in one cooperative launch: the node levels with a
-// grid-wide barrier after each, then the copies of every changed point (P,
-// Pr and Q, consecutive threads on consecutive copies), the zeroing of |V| at
-// wall-face points, and, when the next time step is reduced (a.dt_next), a
-// barrier and the post-exchange time step of the rewritten interior points.
-// The same device functions as the per-level launches, so the results are
-// identical.  A barrier that gives up sets kStatusHaloTimeout and the CTA
-// returns.
-
+// Phase A in one cooperative launch: the node levels with a grid-wide
+// barrier between levels (every node of a level reads only the state and
+// lower levels).  A barrier that gives up sets kStatusHaloTimeout and the
+// CTA returns.
 template <typename T, int NS>
-__global__ void __launch_bounds__(256, 2)
-    k_halo_all(const HaloArgs<T> a, const __grid_constant__ ChemParams C, const HaloLevels lv, int np, int npr,
-               int nq, double *vel, const int64_t *vel_zero, int64_t n_vel_zero, GridBarrier *bar,
-               unsigned *status) {
+__global__ void __launch_bounds__(128)
+    k_halo_levels(const HaloArgs<T> a, const __grid_constant__ ChemParams C, const HaloLevels lv, GridBarrier *bar,
+                  unsigned *status) {
   const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int l = 0; l < lv.n; ++l) {
-    for (int64_t e = lv.begin[l] + tid; e < lv.begin[l + 1]; e += stride) halo_node<T, NS>(a, C, e);
-    if (!grid_sync_bounded(bar, C.max_spins)) {
+    if (l > 0 && !grid_sync_bounded(bar, C.max_spins)) {
       if (threadIdx.x == 0) atomicOr(status, kStatusHaloTimeout);
       return;
     }
+    for (int64_t e = lv.begin[l] + tid; e < lv.begin[l + 1]; e += stride) halo_node<T, NS>(a, C, e);
   }
-  const int64_t n = a.end - a.begin;
-  for (int64_t e = tid; e < 3 * n; e += stride) halo_copy<T, NS>(a, e % n, (int)(e / n), np, npr, nq);
-  if (vel)
-    for (int64_t e = tid; e < n_vel_zero; e += stride) vel[vel_zero[e]] = 0.0;
-  if (!a.dt_next || a.n_icopies <= 0) return;
-  if (!grid_sync_bounded(bar, C.max_spins)) {
-    if (threadIdx.x == 0) atomicOr(status, kStatusHaloTimeout);
-    return;
-  }
-  double dt_min = 1e300;
-  for (int64_t e = tid; e < a.n_icopies; e += stride) dt_min = fmin(dt_min, halo_copy_dt_point<T, NS>(a, C, e));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) dt_min = fmin(dt_min, __shfl_xor_sync(0xffffffffu, dt_min, o));
-  if ((threadIdx.x & 31) == 0) atomic_min_pos_double(a.dt_next, dt_min);
 }
 
 // ------------------------------------------------------------ setup / misc

@@ -232,6 +232,37 @@ int cc_set_tuning(cc_ctx *ctx, int variant, int kz, int tile_j);
  * the reference's granularity (Driver.cu:144-177 launches per block), kept for
  * comparison.  Results are identical; takes effect at the next cc_step. */
 int cc_set_launch_mode(cc_ctx *ctx, int per_block);
+/* Multi-process runs: the reference's ParallelFace path (Mesh.h:62-102, with
+ * its MPI set-up at Driver.cu:80-82, 252-254), which it leaves unfinished.
+ * Every process holds the whole grid and advances the blocks it owns
+ * (cc_set_owned_blocks; n <= 0 = every block).  Inside cc_step the exchange
+ * hook (cc_set_exchange) is called on the host after each stage's kernels and
+ * before its halo program (event CC_EXCHANGE_STAGE, stage 0..2 of RK3, 0 of a
+ * steady step): the hook moves, between processes, the points its blocks'
+ * halo program reads from blocks that other processes own
+ * (cc_halo_dependencies), with cc_pack_points / cc_unpack_points.  After the
+ * time-step reduction of an RK3 step it is called with event CC_EXCHANGE_DT
+ * and *value = this process's next time step, which it replaces by the
+ * minimum over processes.  A nonzero return aborts cc_step with
+ * CC_ERR_STATE.  While a hook is set, steps are launched, not replayed from a
+ * CUDA graph; the LU-SGS step is not available. */
+#define CC_EXCHANGE_STAGE 0
+#define CC_EXCHANGE_DT 1
+typedef int (*cc_exchange_fn)(void *user, int event, int stage, double *value);
+int cc_set_owned_blocks(cc_ctx *ctx, const int *blocks, int n);
+int cc_set_exchange(cc_ctx *ctx, cc_exchange_fn fn, void *user);
+/* Inside a CC_EXCHANGE_STAGE call: all fields of the listed arena points of
+ * the state the halo program reads as current (which 0: the stage's new
+ * state) or previous (which 1), as [n_fields][n] FP64 host arrays;
+ * n_fields = (6+ns) primitives + (2+ns) transport properties (the bulk
+ * precision widened exactly) + (5+ns) conserved variables. */
+int cc_exchange_fields(cc_ctx *ctx, int *n_fields);
+int cc_pack_points(cc_ctx *ctx, int which, const int64_t *idx, int64_t n, double *out);
+int cc_unpack_points(cc_ctx *ctx, int which, const int64_t *idx, int64_t n, const double *in);
+/* The last residual's sums of squared changes of rho, |V|, p, T over this
+ * process's points and their number (cc_residual = sqrt(sums / count)); a
+ * multi-process run adds both over processes. */
+int cc_residual_sums(cc_ctx *ctx, double sums[4], int64_t *count);
 /* Learned transport closure (a22: absent in the reference, which always
  * evaluates Transport.cu:43-96).  An MLP maps (T, X_1..X_n) to
  * (log mu, log lambda, log rhoD_1..rhoD_n): inputs t = (T - t_center)/t_scale

@@ -26,6 +26,13 @@
 //   n_block x { int32 mx my mz n_bnd n_inner; int32 bnd[n_bnd][7];
 //               int32 inner[n_inner][13]; f64 jac[Ng] metric[9][Ng] bv[6][Ng]
 //               yk[n][Ng] }     (Ng = full ghosted box, i fastest)
+// With "--time N" after the two paths, the harness also times N further
+// explicit steps of the reference's kernels with CUDA events, after the case
+// file's steps as warm-up: the per-block kernels of a step (set_dq_to_0,
+// compute_inviscid_flux, compute_viscous_flux, local_time_step,
+// update_cv_and_bv, update_physical_properties; Driver.cu:144-177) alone, and
+// the whole step with the boundary launches and the harness's interface
+// fill, and prints one JSON line with the milliseconds per step.
 // Output: char[8] "CCOUT001", int32 n_block, then per block the processed
 // boundaries (9 ints each) and inner faces (26 ints each), the first step's
 // dq[n_var][N] and dt_local[N], the final bv[6][Ng] yk[n][Ng] cv[n_var][Ng]
@@ -113,11 +120,17 @@ static double *dev_copy(const std::vector<double> &h) {
 }
 
 int main(int argc, char **argv) {
-  if (argc < 3) {
-    std::fprintf(stderr, "usage: %s case.bin out.bin\n", argv[0]);
+  if (argc != 3 && argc != 5) {
+    std::fprintf(stderr, "usage: %s case.bin out.bin [--time N]\n", argv[0]);
     return 1;
   }
-  CK(cudaDeviceSetLimit(cudaLimitMallocHeapSize, 256u * 1024u * 1024u));
+  const int time_steps = argc == 5 && std::strcmp(argv[3], "--time") == 0 ? std::atoi(argv[4]) : 0;
+  // the reference's kernels allocate per-thread work arrays with device new
+  // (InviscidScheme.cu:33, Reconstruction.cu:63, Transport.cu:48-61,
+  // Field.cu:190, ViscousScheme.cu:84): at most ~1 KB per thread live at once
+  // for 9 species, and at most 2048 resident threads per SM, so 2 GiB of
+  // device heap covers every resident thread several times over
+  CK(cudaDeviceSetLimit(cudaLimitMallocHeapSize, (size_t)2 << 30));
   Reader rd{std::fopen(argv[1], "rb")};
   if (!rd.f) return 4;
   char magic[8];
@@ -404,6 +417,54 @@ int main(int argc, char **argv) {
         for (int l = 0; l < 4; ++l) res[l] += sq[q * 4 + l];
     }
     for (int l = 0; l < 4; ++l) res[l] = std::sqrt(res[l] / (double)n_total);
+  }
+
+  if (time_steps > 0) {
+    const int n_dev_threads = [] {
+      int dev = 0, n_sm = 0, per_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+      cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+      return n_sm * per_sm;
+    }();
+    auto step_kernels = [&]() {
+      for (int b = 0; b < n_block; ++b) {
+        const int mx = blocks[b].mx, my = blocks[b].my, mz = blocks[b].mz;
+        dim3 bpg((mx - 1) / tpb.x + 1, (my - 1) / tpb.y + 1, (mz - 1) / tpb.z + 1);
+        cfd::set_dq_to_0<<<bpg, tpb>>>(field[b].d_ptr);
+        cfd::compute_inviscid_flux(blocks[b], field[b].d_ptr, inv, param, n_var);
+        if (viscous_order == 2) cfd::compute_viscous_flux(blocks[b], field[b].d_ptr, vis, param, n_var);
+        cfd::local_time_step<<<bpg, tpb>>>(field[b].d_ptr, param, tmp);
+        cfd::update_cv_and_bv<<<bpg, tpb>>>(field[b].d_ptr, param);
+      }
+      props();
+      CK(cudaGetLastError());
+    };
+    cudaEvent_t e0, e1, e2, e3;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventCreate(&e2));
+    CK(cudaEventCreate(&e3));
+    step_kernels();
+    CK(cudaDeviceSynchronize());
+    CK(cudaEventRecord(e0));
+    for (int s = 0; s < time_steps; ++s) step_kernels();
+    CK(cudaEventRecord(e1));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventRecord(e2));
+    for (int s = 0; s < time_steps; ++s) {
+      step_kernels();
+      apply_bcs();
+      exchange();
+    }
+    CK(cudaEventRecord(e3));
+    CK(cudaEventSynchronize(e3));
+    float ms_k = 0, ms_s = 0;
+    CK(cudaEventElapsedTime(&ms_k, e0, e1));
+    CK(cudaEventElapsedTime(&ms_s, e2, e3));
+    std::printf("{\"points\": %ld, \"steps\": %d, \"kernels_ms_per_step\": %.6f, "
+                "\"step_ms_with_halo_fill\": %.6f, \"device_threads\": %d}\n",
+                n_total, time_steps, ms_k / time_steps, ms_s / time_steps, n_dev_threads);
   }
 
   Writer wr{std::fopen(argv[2], "wb")};

@@ -23,6 +23,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 from combustioncodegpu_b200 import cases  # noqa: E402
+from oracle.ref_harness.case_file import write_case  # noqa: E402,F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -61,38 +62,6 @@ def golden_cases():
                                       "bv": np.stack([rho, u, v, w, p, T]), "yk": np.zeros((0, ng)),
                                       "boundaries": [], "inner_faces": faces}]}
     return out
-
-
-def write_case(path, case):
-    prm = case["params"]
-    sp = prm.get("species")
-    ns = 0 if sp is None else int(sp["n_spec"])
-    with open(path, "wb") as f:
-        f.write(b"CCCASE01")
-        f.write(struct.pack("<8i", ns, len(case["blocks"]), prm["ngg"], prm["viscous_order"],
-                            prm["reconstruction"], prm["limiter"], case["n_steps"], len(case["bcs"])))
-        f.write(struct.pack("<3d", prm["prandtl_number"], prm["cfl"], prm["schmidt_number"]))
-        if ns:
-            for key in ("mw", "t_low", "t_mid", "t_high", "low_temp_coeff", "high_temp_coeff", "LJ_potent_inv",
-                        "vis_coeff", "WjDivWi_to_One4th", "sqrt_WiDivWjPl1Mul8"):
-                f.write(np.ascontiguousarray(sp[key], dtype="<f8").tobytes())
-        for bc in case["bcs"]:
-            f.write(struct.pack("<4i", bc["label"], bc["kind"], bc.get("thermal_type", 0), 0))
-            f.write(struct.pack("<7d", bc.get("t_wall", 300.0), bc.get("density", 0.0), bc.get("u", 0.0),
-                                bc.get("v", 0.0), bc.get("w", 0.0), bc.get("pressure", 0.0),
-                                bc.get("temperature", 0.0)))
-            yk = np.zeros(ns)
-            if "yk" in bc:
-                yk[:] = np.asarray(bc["yk"])[:ns]
-            f.write(yk.astype("<f8").tobytes())
-        for b in case["blocks"]:
-            f.write(struct.pack("<5i", *b["dims"], len(b["boundaries"]), len(b["inner_faces"])))
-            for r in b["boundaries"]:
-                f.write(struct.pack("<7i", *r))
-            for r in b["inner_faces"]:
-                f.write(struct.pack("<13i", *r))
-            for key in ("jac", "metric", "bv", "yk"):
-                f.write(np.ascontiguousarray(b[key], dtype="<f8").tobytes())
 
 
 def read_case(path):

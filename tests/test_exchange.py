@@ -102,3 +102,63 @@ def test_partition_and_single_process_plan():
     plan = exchange.ExchangePlan(d, [0] * len(case["blocks"]), 0, 1)
     assert plan.volume() == (0, 0) and plan.send == {} and plan.recv == {}
     d.close()
+
+
+def _step_worker(rank, world, port, out, precision):
+    import torch.distributed as dist
+
+    import combustioncodegpu_b200 as cc
+    from combustioncodegpu_b200 import exchange
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    case = _case()
+    d = cc.Driver.from_case(case, precision)
+    nb = len(case["blocks"])
+    owner = exchange.partition([int(c) for c in _spans(d, nb)[:, 1]], world)
+    step = exchange.DistributedStep(d, owner, rank, world)
+    d.initialize_computation()
+    d.simulate(3, "rk3", residual=True)
+    res = step.residual()
+    dt = d.last_dt()
+    status = d.status()
+    states = {b: d.field[b].get_state()[2] for b in range(nb) if owner[b] == rank}
+    step.close()
+    d.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    np.savez(os.path.join(out, "step%d.npz" % rank), res=res, dt=dt, status=status, owner=np.array(owner),
+             **{"b%d" % b: v for b, v in states.items()})
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_two_process_step_equals_single_process(tmp_path, precision):
+    """Two processes on one GPU (gloo between them, the exchange on the host
+    between launches, so no kernel waits on another process), each advancing
+    its own blocks of the 2 x 2 x 1 periodic multiblock case for three RK3
+    steps with the halo sources exchanged inside cc_step and the time step
+    reduced over processes: every block's state equals the single-process
+    run's bit for bit, the residual to rounding (its sums are added in
+    another order)."""
+    import combustioncodegpu_b200 as cc
+
+    world = 2
+    mp.spawn(_step_worker, args=(world, _free_port(), str(tmp_path), precision), nprocs=world, join=True)
+    case = _case()
+    d = cc.Driver.from_case(case, precision)
+    d.initialize_computation()
+    d.simulate(3, "rk3", residual=True)
+    want = [d.field[b].get_state()[2] for b in range(len(case["blocks"]))]
+    want_res, want_dt = d.residual(), d.last_dt()
+    assert d.status() == 0
+    d.close()
+    got = [np.load(tmp_path / ("step%d.npz" % r)) for r in range(world)]
+    owner = got[0]["owner"]
+    assert set(owner.tolist()) == {0, 1}
+    for b in range(len(case["blocks"])):
+        np.testing.assert_array_equal(got[owner[b]]["b%d" % b], want[b])
+    for g in got:
+        assert int(g["status"]) == 0
+        assert float(g["dt"]) == want_dt
+        np.testing.assert_allclose(g["res"], want_res, rtol=1e-12)
