@@ -112,6 +112,7 @@ EXPORTS = {
     "cc_set_closure": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "cc_use_closure": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_closure_stats": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+    "cc_set_closure_bound": ([ctypes.c_void_p, ctypes.c_double], ctypes.c_int),
     "cc_eval_transport": ([ctypes.c_void_p, ctypes.c_int64, _dp, _dp, ctypes.c_int, _dp], ctypes.c_int),
     "cc_save_checkpoint": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
     "cc_load_checkpoint": ([ctypes.c_void_p, ctypes.c_char_p], ctypes.c_int),
@@ -516,10 +517,15 @@ class Driver:
         _check(self.lib.cc_use_closure(self.ctx, 1 if on else 0))
 
     def closure_stats(self):
-        """(points evaluated by the closure kernel, exact fallbacks)."""
-        out = (ctypes.c_int64 * 2)()
+        """(points evaluated by the closure kernel, exact outside the
+        training hull, exact after the run-time error check)."""
+        out = (ctypes.c_int64 * 3)()
         _check(self.lib.cc_closure_stats(self.ctx, out))
-        return int(out[0]), int(out[1])
+        return int(out[0]), int(out[1]), int(out[2])
+
+    def set_closure_bound(self, rel_err=1e-3):
+        """Relative error bound of the closure's run-time check (0: off)."""
+        _check(self.lib.cc_set_closure_bound(self.ctx, float(rel_err)))
 
     def eval_transport(self, T, Y, mode="exact"):
         """(mu, lambda, rhoD_k) [2 + n_spec][n] of points (T [n], Y [n_spec][n])

@@ -8,16 +8,18 @@ outside the training hull in T take the exact transport.
 Training data: T ~ U[t_min, t_max], X ~ Dirichlet(alpha * 1_n), Y from X;
 targets are the library's own exact FP64 transport of those points
 (cc_eval_transport, mode 0).  The network is trained with the arithmetic of
-the kernel: inputs as BF16 (hi, lo) pairs, BF16 weights and BF16 hidden
-activations (rounding with a straight-through gradient), FP32 accumulation,
-FP32 biases; the loss is the mean squared error of the log properties, i.e.
-of the relative error.  Training runs on the GPU with the library's own
+the kernel: inputs as BF16 (hi, lo) pairs, BF16 weights (rounding with a
+straight-through gradient), FP32 hidden activations (the kernel keeps them
+as BF16 hi/lo pairs), FP32 accumulation and biases; the loss is the mean
+squared error of the log properties, i.e. of the relative error.  Training
+runs on the GPU with the library's own
 forward/backward and Adam kernels (cc_mlp_grad, cc_mlp_adam; an offline
 step, not the hot path), checked against the CPU restatement of the same
 math in oracle/closure_mlp.py; the result is a dict that Driver.set_closure
 takes.  ClosureNet is the plain PyTorch FP32 model of the same network with
-the same rounding points: the reference the inference kernel is tested
-against, and the evaluation of the trained weights.
+the same rounding points (BF16 weights and inputs, FP32 hidden activations,
+which the kernel carries as BF16 hi/lo pairs): the reference the inference
+kernel is tested against, and the evaluation of the trained weights.
 
   python -m combustioncodegpu_b200.closure --out closure_weights.npz
 """
@@ -88,10 +90,10 @@ class ClosureNet:
     def forward(self, x, quantized=True):
         import torch
         r = _round_ste if quantized else (lambda v: v)
-        h = x
+        h = x  # BF16 (hi, lo) features; the hidden activations stay FP32
         for i in range(4):
             w, b = self.params[2 * i], self.params[2 * i + 1]
-            h = r(h) @ r(w).T + b
+            h = h @ r(w).T + b
             if i < 3:
                 h = torch.nn.functional.silu(h)
         return h

@@ -119,6 +119,7 @@ struct cc_ctx {
   bool closure_set = false;       // cc_set_closure: learned transport closure uploaded
   bool closure_on = false;        // cc_use_closure: stages take transport from the closure kernel
   ClosureDev cl{};                // device weights, biases, normalisation, counters
+  double closure_bound = 1e-3;    // cc_set_closure_bound: relative error of the run-time check (0: none)
   double *d_gcl = nullptr;        // [3][N] geometric term of the gauge-pressure momentum fluxes
   int kz = 1;                     // k-chunk of the stage tiles
   double tuned_ms = 0;            // stage-kernel time of the chosen configuration
@@ -1854,7 +1855,7 @@ int cc_set_closure(cc_ctx *c, const cc_closure *m) {
   if (c->stream) CK(cudaStreamSynchronize(c->stream));
   if (!c->cl.w) {
     void *p = nullptr;
-    CK(cudaMalloc(&p, kMlpWBytes + sizeof(float) * kMlpBias + 2 * sizeof(unsigned long long)));
+    CK(cudaMalloc(&p, kMlpWBytes + sizeof(float) * kMlpBias + 3 * sizeof(unsigned long long)));
     c->allocs.push_back(p);
     c->cl.w = p;
     c->cl.b = reinterpret_cast<const float *>(static_cast<unsigned char *>(p) + kMlpWBytes);
@@ -1863,7 +1864,7 @@ int cc_set_closure(cc_ctx *c, const cc_closure *m) {
   }
   CK(cudaMemcpy(const_cast<void *>(c->cl.w), blob.data(), kMlpWBytes, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(const_cast<float *>(c->cl.b), bias.data(), sizeof(float) * kMlpBias, cudaMemcpyHostToDevice));
-  CK(cudaMemset(c->cl.counts, 0, 2 * sizeof(unsigned long long)));
+  CK(cudaMemset(c->cl.counts, 0, 3 * sizeof(unsigned long long)));
   for (int i = 0; i < kMlpOut; ++i) {
     c->cl.out_mean[i] = i < n_out ? m->out_mean[i] : 0.0f;
     c->cl.out_scale[i] = i < n_out ? m->out_scale[i] : 0.0f;
@@ -1872,6 +1873,7 @@ int cc_set_closure(cc_ctx *c, const cc_closure *m) {
   c->cl.t_inv_scale = (float)(1.0 / m->t_scale);
   c->cl.t_min = (float)m->t_min;
   c->cl.t_max = (float)m->t_max;
+  c->cl.err_bound = (float)c->closure_bound;
   c->closure_set = true;
   destroy_graphs(c);
   return 0;
@@ -1885,15 +1887,24 @@ int cc_use_closure(cc_ctx *c, int on) {
   return 0;
 }
 
-int cc_closure_stats(cc_ctx *c, int64_t out[2]) {
+int cc_closure_stats(cc_ctx *c, int64_t out[3]) {
   if (int r = check_ctx(c)) return r;
   if (!out) return fail(CC_ERR_ARG, "null pointer");
-  out[0] = out[1] = 0;
+  out[0] = out[1] = out[2] = 0;
   if (!c->cl.counts) return 0;
   if (c->stream) CK(cudaStreamSynchronize(c->stream));
-  unsigned long long h[2];
+  unsigned long long h[3];
   CK(cudaMemcpy(h, c->cl.counts, sizeof h, cudaMemcpyDeviceToHost));
-  out[0] = (int64_t)h[0], out[1] = (int64_t)h[1];
+  out[0] = (int64_t)h[0], out[1] = (int64_t)h[1], out[2] = (int64_t)h[2];
+  return 0;
+}
+
+int cc_set_closure_bound(cc_ctx *c, double rel_err) {
+  if (int r = check_ctx(c)) return r;
+  if (!(rel_err >= 0.0)) return fail(CC_ERR_ARG, "cc_set_closure_bound: the bound must be >= 0");
+  c->closure_bound = rel_err;
+  c->cl.err_bound = (float)rel_err;
+  destroy_graphs(c);  // the captured launches carry the closure parameters by value
   return 0;
 }
 

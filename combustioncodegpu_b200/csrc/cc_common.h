@@ -83,7 +83,10 @@ struct ClosureDev {
   const float *b;                       // kMlpBias
   float out_mean[kMlpOut], out_scale[kMlpOut];
   float t_center, t_inv_scale, t_min, t_max;
-  unsigned long long *counts;           // [0] points evaluated, [1] exact fallbacks
+  float err_bound;                      // run-time check: relative error above which a tile takes the exact
+                                        // transport (0: no check)
+  unsigned long long *counts;           // [0] points evaluated, [1] exact outside the hull, [2] exact after the
+                                        // run-time check (points of the tiles it sent back)
 };
 
 // One block of the multiblock grid in the concatenated field arena.

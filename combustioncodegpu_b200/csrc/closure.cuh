@@ -18,10 +18,20 @@
 //
 // Inputs: t = (T - t_center) / t_scale and the mole fractions, each as a BF16
 // pair (hi, lo = value - hi) so that BF16 input rounding does not limit the
-// fit: 2 + 2 ns features, padded to 32.  Outputs: 2 + ns values, padded to 16,
+// fit: 2 + 2 ns features, padded to 32.  The hidden activations are stored
+// the same way, as BF16 (hi, lo) pairs, and every layer after the first runs
+// two MMAs into the same accumulator (hi x W, then lo x W): the activations
+// keep ~16 significant bits instead of BF16's 8, which would otherwise floor
+// the closure's error near 1e-3.  Outputs: 2 + ns values, padded to 16,
 // mapped back by property = exp(o * out_scale + out_mean).  Points outside
 // the training hull in T, or with a mole fraction of at least 0.998, take the
 // exact transport in the same kernel.
+//
+// Run-time error check (err_bound > 0): after every round of up to 32 tiles a
+// CTA evaluates the exact transport at 4 fixed sample points of each tile
+// (1 in 32 points, one sample per thread, so the warps stay full) and
+// compares it with what the network wrote; a tile whose sample exceeds the
+// bound in any output is recomputed with the exact transport.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -29,7 +39,8 @@
 
 namespace ccb {
 
-constexpr int kMlpSmem = kMlpWBytes + kMlpXBytes + kMlpHBytes + kMlpBias * 4 + 64;
+constexpr int kMlpSmem = kMlpWBytes + kMlpXBytes + 2 * kMlpHBytes + kMlpBias * 4 + 64;
+constexpr int kMlpRound = 32;  // tiles per run-time check round (4 samples each: one per thread)
 constexpr int kMlpTmemCols = 64;
 constexpr unsigned kStatusMlpTimeout = 16u;  // an MMA completion wait gave up
 constexpr long long kMlpMaxSpins = kDefaultWaitSpins;  // bound of the drain after an abort
@@ -92,7 +103,7 @@ __device__ __forceinline__ bool mlp_test_wait(uint64_t *bar, uint32_t parity) {
 }
 
 // x * sigmoid(x) with the hardware exponential and division (relative error
-// ~1e-7, far below the BF16 rounding of the activations that follows)
+// ~1e-7, below the hi/lo BF16 representation of the activations that follows)
 __device__ __forceinline__ float mlp_silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
 
 __device__ __forceinline__ uint32_t mlp_pack(float a, float b) {
@@ -109,8 +120,9 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
   extern __shared__ __align__(128) unsigned char sm[];
   unsigned char *sW = sm;                                   // weights, operand layout
   unsigned char *sX = sW + kMlpWBytes;                      // A operand of layer 1 [128 x 32]
-  unsigned char *sH = sX + kMlpXBytes;                      // A operand of layers 2-4 [128 x 64]
-  float *sB = reinterpret_cast<float *>(sH + kMlpHBytes);   // biases
+  unsigned char *sH = sX + kMlpXBytes;                      // A operand of layers 2-4 [128 x 64], hi
+  unsigned char *sHl = sH + kMlpHBytes;                     // the same, lo = value - hi
+  float *sB = reinterpret_cast<float *>(sHl + kMlpHBytes);  // biases
   uint64_t *bar = reinterpret_cast<uint64_t *>(sB + kMlpBias);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -135,11 +147,27 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
   const uint32_t tmem = *tslot;
   const uint32_t t_row = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's 32 lanes
 
-  const uint32_t aX = mlp_smem_u32(sX), aH = mlp_smem_u32(sH), aW = mlp_smem_u32(sW);
+  const uint32_t aX = mlp_smem_u32(sX), aH = mlp_smem_u32(sH), aHl = mlp_smem_u32(sHl), aW = mlp_smem_u32(sW);
   const uint32_t aW1 = aW, aW2 = aW1 + kMlpW1, aW3 = aW2 + kMlpW2, aW4 = aW3 + kMlpW2;
   uint32_t phase = 0;
   bool late = false;
-  unsigned long long n_eval = 0, n_fb = 0;
+  unsigned long long n_eval = 0, n_fb = 0, n_chk = 0;
+  __shared__ int64_t s_round[kMlpRound];  // tile bases of the current check round
+  __shared__ unsigned s_fail;             // bit t: tile t of the round failed its samples
+  int n_round = 0;
+  // exact transport of point q into Pr (the fallback)
+  auto exact_at = [&](int64_t q) {
+    T Yt[A], mu, lam, rd[A], gam, c;
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) Yt[l] = P[(6 + l) * N + q];
+    point_props<T, NS>(C, param_rec<T>(C), P[5 * N + q], Yt, mu, lam, rd, gam, c);
+    Pr[q] = mu;
+    Pr[N + q] = lam;
+#pragma unroll
+    for (int l = 0; l < A; ++l)
+      if (l < ns) Pr[(2 + l) * N + q] = rd[l];
+  };
 
   for (int64_t base = (int64_t)blockIdx.x * kMlpRows; base < N; base += (int64_t)gridDim.x * kMlpRows) {
     const int64_t p = base + tid;
@@ -207,6 +235,10 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
         for (int s = 0; s < ksteps; ++s)
           mlp_mma(tmem, mlp_desc(aA + 2 * s * lboA, lboA, 128), mlp_desc(aB + 2 * s * lboB, lboB, 128),
                   mlp_idesc(n), s > 0);
+        if (layer > 0)  // the lo half of the hidden activations into the same accumulator
+          for (int s = 0; s < ksteps; ++s)
+            mlp_mma(tmem, mlp_desc(aHl + 2 * s * lboA, lboA, 128), mlp_desc(aB + 2 * s * lboB, lboB, 128),
+                    mlp_idesc(n), 1);
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                          mlp_smem_u32(bar))
                      : "memory");
@@ -227,6 +259,9 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
           mlp_ld16(t_row + 16 * q, v);
 #pragma unroll
           for (int i = 0; i < 16; ++i) v[i] = mlp_silu(v[i] + bias[16 * q + i]);
+          float lo[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) lo[i] = v[i] - __bfloat162float(__float2bfloat16_rn(v[i]));
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             uint4 w;
@@ -235,6 +270,11 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
             w.z = mlp_pack(v[8 * h + 4], v[8 * h + 5]);
             w.w = mlp_pack(v[8 * h + 6], v[8 * h + 7]);
             *reinterpret_cast<uint4 *>(sH + mlp_off(kMlpRows, tid, 16 * q + 8 * h)) = w;
+            w.x = mlp_pack(lo[8 * h], lo[8 * h + 1]);
+            w.y = mlp_pack(lo[8 * h + 2], lo[8 * h + 3]);
+            w.z = mlp_pack(lo[8 * h + 4], lo[8 * h + 5]);
+            w.w = mlp_pack(lo[8 * h + 6], lo[8 * h + 7]);
+            *reinterpret_cast<uint4 *>(sHl + mlp_off(kMlpRows, tid, 16 * q + 8 * h)) = w;
           }
         }
       } else {
@@ -254,16 +294,40 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
           if (l < ns) Pr[(2 + l) * N + p] = T(__expf(out[2 + l] * cl.out_scale[2 + l] + cl.out_mean[2 + l]));
       } else {
         ++n_fb;
-        T Yt[A], mu, lam, rd[A], gam, c;
+        exact_at(p);
+      }
+    }
+    if (cl.err_bound > 0.0f) {
+      // run-time check of the round: 4 fixed samples per tile, one per thread
+      if (tid == 0) s_round[n_round] = base;
+      ++n_round;
+      if (n_round == kMlpRound || base + (int64_t)gridDim.x * kMlpRows >= N) {
+        if (tid == 0) s_fail = 0u;
+        __syncthreads();  // the round's properties and tile list visible to the whole CTA
+        const int t = tid >> 2, smp = tid & 3;
+        if (t < n_round) {
+          const int64_t b = s_round[t];
+          const int64_t q = b + smp * 32 + (int)(((b / kMlpRows) * 7 + smp * 11) & 31);
+          if (q < N && P[q] > T(0)) {
+            T Yt[A], mu, lam, rd[A], gam, c;
 #pragma unroll
-        for (int l = 0; l < A; ++l)
-          if (l < ns) Yt[l] = P[(6 + l) * N + p];
-        point_props<T, NS>(C, param_rec<T>(C), P[5 * N + p], Yt, mu, lam, rd, gam, c);
-        Pr[p] = mu;
-        Pr[N + p] = lam;
+            for (int l = 0; l < A; ++l)
+              if (l < ns) Yt[l] = P[(6 + l) * N + q];
+            point_props<T, NS>(C, param_rec<T>(C), P[5 * N + q], Yt, mu, lam, rd, gam, c);
+            float e = fmaxf(fabsf((float)(Pr[q] / mu) - 1.0f), fabsf((float)(Pr[N + q] / lam) - 1.0f));
 #pragma unroll
-        for (int l = 0; l < A; ++l)
-          if (l < ns) Pr[(2 + l) * N + p] = rd[l];
+            for (int l = 0; l < A; ++l)
+              if (l < ns) e = fmaxf(e, fabsf((float)(Pr[(2 + l) * N + q] / rd[l]) - 1.0f));
+            if (!(e <= cl.err_bound)) atomicOr(&s_fail, 1u << t);
+          }
+        }
+        __syncthreads();
+        for (unsigned fail = s_fail; fail; fail &= fail - 1u) {  // tiles sent back to the exact transport
+          const int64_t q = s_round[__ffs(fail) - 1] + tid;
+          if (q < N && P[q] > T(0)) exact_at(q), ++n_chk;
+        }
+        __syncthreads();  // before the next round reuses the tile list
+        n_round = 0;
       }
     }
   }
@@ -280,10 +344,12 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
   for (int o = 16; o > 0; o >>= 1) {
     n_eval += __shfl_xor_sync(0xffffffffu, n_eval, o);
     n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
+    n_chk += __shfl_xor_sync(0xffffffffu, n_chk, o);
   }
   if ((tid & 31) == 0 && cl.counts) {
     atomicAdd(cl.counts, n_eval);
     atomicAdd(cl.counts + 1, n_fb);
+    atomicAdd(cl.counts + 2, n_chk);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

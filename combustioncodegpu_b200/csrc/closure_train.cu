@@ -1,10 +1,12 @@
 // Training kernels of the learned transport closure: forward, backward and
 // Adam for the 4-layer MLP (n_in -> H -> H -> H -> n_out, SiLU) with the
 // inference kernel's rounding points (quantisation-aware training): every
-// layer input and every weight is rounded to BF16 (round to nearest even) in
-// the forward pass and the rounding is passed through unchanged in the
-// backward pass (straight-through); accumulation, biases and the master
-// weights are FP32.  Loss: mean over the batch and the outputs of
+// weight is rounded to BF16 (round to nearest even) in the forward pass and
+// the rounding is passed through unchanged in the backward pass
+// (straight-through); the network inputs are BF16 (hi, lo) pairs as the
+// kernel forms them; the hidden activations stay FP32 (the inference kernel
+// carries them as BF16 hi/lo pairs, ~16 significant bits); accumulation,
+// biases and the master weights are FP32.  Loss: mean over the batch and the outputs of
 // ((o - y) scale_o)^2, i.e. the squared error of the log properties.
 //
 // Parameters are one FP32 buffer in the order W1 [H][n_in], b1 [H],
@@ -30,9 +32,8 @@ constexpr int kMaxWidth = 64; // widest layer (n_in, H, n_out <= 64)
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 __device__ __forceinline__ float sigm(float z) { return 1.0f / (1.0f + expf(-z)); }
 
-// Z = r(A) r(W)^T + b for kRows rows; H = r(silu(Z)) (hidden) or Z (output).
-// A holds already-rounded layer inputs (the first layer's inputs are BF16
-// values), so only the weights are rounded here.
+// Z = A r(W)^T + b for kRows rows; H = silu(Z) (hidden) or Z (output).
+// Only the weights are rounded (the first layer's inputs are BF16 values).
 __global__ void __launch_bounds__(kThreads) k_dense_fwd(const float *__restrict__ A, const float *__restrict__ W,
                                                         const float *__restrict__ b, float *__restrict__ Z,
                                                         float *__restrict__ H, int B, int n_in, int n_out, int act) {
@@ -51,7 +52,7 @@ __global__ void __launch_bounds__(kThreads) k_dense_fwd(const float *__restrict_
     float z = b[o];
     for (int i = 0; i < n_in; ++i) z = fmaf(sA[rl * n_in + i], sW[o * n_in + i], z);
     Z[(size_t)r * n_out + o] = z;
-    H[(size_t)r * n_out + o] = act ? bf16r(z * sigm(z)) : z;
+    H[(size_t)r * n_out + o] = act ? z * sigm(z) : z;
   }
 }
 
@@ -81,8 +82,8 @@ __global__ void __launch_bounds__(kThreads) k_loss(const float *__restrict__ O, 
   if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
-// dZ_prev = (G r(W)) silu'(Z_prev) for kRows rows (the rounding of W and of
-// the layer input are passed through).
+// dZ_prev = (G r(W)) silu'(Z_prev) for kRows rows (the rounding of W is
+// passed through).
 __global__ void __launch_bounds__(kThreads) k_dense_bwd_in(const float *__restrict__ G, const float *__restrict__ W,
                                                            const float *__restrict__ Zp, float *__restrict__ dZp,
                                                            int B, int n_in, int n_out) {

@@ -162,10 +162,16 @@ cudaError_t Launch<T, NS>::props_mlp(const T *P, T *Pr, int64_t N, const void *c
     return cudaErrorInvalidValue;  // the closure is for mixtures
   } else {
     if (N <= 0) return cudaSuccess;
+    static bool attr_set = false;  // the weights, operands and hi/lo activations take more than 48 KB
+    if (!attr_set) {
+      cudaError_t e = cudaFuncSetAttribute(k_props_mlp<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMlpSmem);
+      if (e != cudaSuccess) return e;
+      attr_set = true;
+    }
     int dev = 0, n_sm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     const int64_t tiles = (N + kMlpRows - 1) / kMlpRows;
-    const int grid = (int)std::min<int64_t>(tiles, (int64_t)n_sm * 4);
+    const int grid = (int)std::min<int64_t>(tiles, (int64_t)n_sm * 3);  // 3 CTAs per SM fit (64 KB each)
     k_props_mlp<T, NS><<<grid, kMlpRows, kMlpSmem, s>>>(P, Pr, N, *static_cast<const ClosureDev *>(cl), status, C);
     return cudaGetLastError();
   }
@@ -199,6 +205,10 @@ cudaError_t Launch<T, NS>::configure() {
   if constexpr (FacesTmaFits<T, NS, 16>::value) {
     faces_attr(k_faces_tma<T, NS, 16>, 16);
     faces_attr(k_faces_tma_persistent<T, NS, 16>, 16);
+  }
+  if constexpr (NS != 0) {  // the closure kernel (set here too, before any stream capture)
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_props_mlp<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMlpSmem);
   }
   if constexpr (sizeof(T) == 4 && NS >= 0) {
     if (e == cudaSuccess)

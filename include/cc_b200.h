@@ -289,9 +289,17 @@ int cc_set_closure(cc_ctx *ctx, const cc_closure *closure);
  * (1) or from the exact Wilke / constant-Schmidt evaluation (0, default).
  * With the closure on, the global time step is reduced after the halo. */
 int cc_use_closure(cc_ctx *ctx, int on);
-/* Points the closure kernel evaluated and, of those, how many took the
- * exact fallback, since cc_set_closure. */
-int cc_closure_stats(cc_ctx *ctx, int64_t out[2]);
+/* Since cc_set_closure: out[0] points the closure kernel evaluated, out[1]
+ * of those that took the exact transport outside the training hull, out[2]
+ * points of tiles the run-time error check sent back to the exact
+ * transport. */
+int cc_closure_stats(cc_ctx *ctx, int64_t out[3]);
+/* No counterpart in the reference.  Relative error bound of the closure's
+ * run-time check: every 128-point tile is sampled at 4 fixed points (1 in
+ * 32) against the exact transport (Transport.cu:43-96, the judge of the
+ * network), and a tile whose sample exceeds the bound in any property takes
+ * the exact transport.  Default 1e-3; 0 switches the check off. */
+int cc_set_closure_bound(cc_ctx *ctx, double rel_err);
 /* Transport properties of n points (host arrays): T [n], Y [n_spec][n] ->
  * out [2 + n_spec][n] = (mu, lambda, rhoD_k), by the exact FP64 evaluation
  * (mode 0) or by the closure kernel (mode 1).  Needs a device, not cc_init. */

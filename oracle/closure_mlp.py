@@ -3,9 +3,11 @@ math -- TEST INFRASTRUCTURE ONLY, what the training kernels are tested against
 (combustioncodegpu_b200/csrc/closure_train.cu); the product never calls it.
 
 Network: n_in -> H -> H -> H -> n_out, SiLU on the hidden layers.
-Quantisation-aware forward: every layer input and every weight is rounded
-to BF16 (round to nearest even); the backward pass treats the rounding as
-the identity (straight-through estimator).  Loss: mean over batch and
+Quantisation-aware forward: every weight is rounded to BF16 (round to
+nearest even) and the network inputs are BF16 values; the hidden activations
+are FP32 (the inference kernel carries them as BF16 hi/lo pairs); the
+backward pass treats the rounding as the identity (straight-through
+estimator).  Loss: mean over batch and
 outputs of ((o - y) * scale)^2.  Adam: Kingma & Ba (2015), bias-corrected.
 Parameters: one flat array W1 [H][n_in], b1, W2 [H][H], b2, W3, b3,
 W4 [n_out][H], b4.
@@ -54,7 +56,7 @@ def loss_and_grad(params, x, y, scale, n_in, H, n_out, quantized=True):
         zl = a[l] @ W[l].T + b[l]
         z.append(zl)
         if l < 3:
-            a.append(r(_silu(zl).astype(np.float32)) if quantized else _silu(zl))
+            a.append(_silu(zl).astype(np.float32).astype(np.float64) if quantized else _silu(zl))
     sc = np.asarray(scale, dtype=np.float64)
     err = (z[3] - np.asarray(y, dtype=np.float64)) * sc
     B = x.shape[0]
