@@ -241,7 +241,13 @@ def main():
     d = cc.Driver.from_case(cases.case_box(4, species=sp), "mixed")
     w, report = train(d, sp, n_samples=args.samples, epochs=args.epochs)
     d.set_closure(w)
+    d.set_closure_bound(0.0)  # the network alone
     report["kernel_rel_err"] = validate(d, sp)
+    d.set_closure_bound(1e-3)  # with the run-time check: the share of points it sends to the exact transport
+    d.set_closure(w)
+    report["kernel_rel_err_with_check"] = validate(d, sp)
+    n_eval, n_hull, n_chk = d.closure_stats()
+    report["check_fallback_rate"] = n_chk / max(1, n_eval)
     d.close()
     save(args.out, w, report)
     print(json.dumps(report))
