@@ -236,10 +236,12 @@ def main():
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--samples", type=int, default=2_000_000)
     ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--batch", type=int, default=4096)
     args = ap.parse_args()
     sp = cases.synthetic_species()
     d = cc.Driver.from_case(cases.case_box(4, species=sp), "mixed")
-    w, report = train(d, sp, n_samples=args.samples, epochs=args.epochs)
+    w, report = train(d, sp, n_samples=args.samples, epochs=args.epochs, lr=args.lr, batch=args.batch)
     d.set_closure(w)
     d.set_closure_bound(0.0)  # the network alone
     report["kernel_rel_err"] = validate(d, sp)

@@ -30,8 +30,9 @@
 // Run-time error check (err_bound > 0): after every round of up to 32 tiles a
 // CTA evaluates the exact transport at 4 fixed sample points of each tile
 // (1 in 32 points, one sample per thread, so the warps stay full) and
-// compares it with what the network wrote; a tile whose sample exceeds the
-// bound in any output is recomputed with the exact transport.
+// compares it with what the network wrote; a tile whose sampled outputs have
+// a root-mean-square relative error above the bound, or one of them above ten
+// times the bound, is recomputed with the exact transport.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -305,6 +306,7 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
         if (tid == 0) s_fail = 0u;
         __syncthreads();  // the round's properties and tile list visible to the whole CTA
         const int t = tid >> 2, smp = tid & 3;
+        float se = 0.0f, mx = 0.0f, cnt = 0.0f;  // squared and largest relative error of the sample's outputs
         if (t < n_round) {
           const int64_t b = s_round[t];
           const int64_t q = b + smp * 32 + (int)(((b / kMlpRows) * 7 + smp * 11) & 31);
@@ -314,13 +316,29 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
             for (int l = 0; l < A; ++l)
               if (l < ns) Yt[l] = P[(6 + l) * N + q];
             point_props<T, NS>(C, param_rec<T>(C), P[5 * N + q], Yt, mu, lam, rd, gam, c);
-            float e = fmaxf(fabsf((float)(Pr[q] / mu) - 1.0f), fabsf((float)(Pr[N + q] / lam) - 1.0f));
+            auto acc = [&](T got, T want) {
+              const float r = fabsf((float)(got / want) - 1.0f);
+              se += r * r, mx = fmaxf(mx, r), cnt += 1.0f;
+            };
+            acc(Pr[q], mu);
+            acc(Pr[N + q], lam);
 #pragma unroll
             for (int l = 0; l < A; ++l)
-              if (l < ns) e = fmaxf(e, fabsf((float)(Pr[(2 + l) * N + q] / rd[l]) - 1.0f));
-            if (!(e <= cl.err_bound)) atomicOr(&s_fail, 1u << t);
+              if (l < ns) acc(Pr[(2 + l) * N + q], rd[l]);
           }
         }
+        // the tile's 4 samples are 4 consecutive lanes
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+          se += __shfl_xor_sync(0xffffffffu, se, o);
+          mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+          cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        }
+        // fails: root-mean-square sampled error above the bound, or one sampled
+        // output above ten times the bound (NaN fails too)
+        if (smp == 0 && t < n_round && cnt > 0.0f &&
+            !(sqrtf(se / cnt) <= cl.err_bound && mx <= 10.0f * cl.err_bound))
+          atomicOr(&s_fail, 1u << t);
         __syncthreads();
         for (unsigned fail = s_fail; fail; fail &= fail - 1u) {  // tiles sent back to the exact transport
           const int64_t q = s_round[__ffs(fail) - 1] + tid;

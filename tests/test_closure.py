@@ -12,9 +12,11 @@ pointwise transport it replaces.
   (median);
 * the trained closure's accuracy against the exact transport (the judge of
   its error) with the run-time check off: median relative error at most
-  1e-3; and the run-time check itself: with the trained weights it sends
-  few tiles back, with a deliberately perturbed network it sends every tile
-  back and the output is the exact transport;
+  1e-3; and the run-time check itself (4 samples per 128-point tile: a tile
+  goes back to the exact transport when its sampled relative error exceeds
+  1e-3 in root mean square, or 1e-2 in one output): with the trained weights
+  it sends a minority of tiles back, with a deliberately perturbed network
+  every tile, and the output is then the exact transport;
 * the trained closure inside the stages, and its exact fallback outside the
   training hull;
 * the training kernels (cc_mlp_grad, cc_mlp_adam) against the CPU
@@ -66,6 +68,7 @@ def test_closure_kernel_matches_torch_reference():
         ref = net.forward(closure.features(T.astype(np.float32), X32, "cuda")).cpu().numpy().T
     d = _driver()
     d.set_closure(w)
+    d.set_closure_bound(0.0)  # the network itself, not the exact transport of failing tiles
     got = np.log(d.eval_transport(T, Y, "closure"))
     d.close()
     err = np.abs(got - ref)
@@ -99,7 +102,7 @@ def test_run_time_check_sends_bad_tiles_to_the_exact_transport():
     d.set_closure(w)  # the trained network, check at the default 1e-3
     got = d.eval_transport(T, Y, "closure")
     n_eval, n_hull, n_chk = d.closure_stats()
-    assert n_eval == T.size and n_chk < 0.25 * n_eval, (n_eval, n_hull, n_chk)
+    assert n_eval == T.size and n_chk < 0.5 * n_eval, (n_eval, n_hull, n_chk)
     rel = np.abs(got / exact - 1.0)
     assert np.median(rel) <= 1e-3
     # a network whose every output is off by 1 % (output bias shifted): every
@@ -129,7 +132,7 @@ def test_closure_in_stages_and_fallback():
         out[mode] = d.field[0].get_state()[0]
         if mode == "closure":
             n_eval, n_fb, n_chk = d.closure_stats()
-            assert n_eval >= 24 ** 3 * 15 and n_fb == 0 and n_chk < n_eval
+            assert n_eval >= 24 ** 3 * 15 and n_fb == 0 and n_chk < 0.5 * n_eval
         d.close()
     for f in (0, 4, 5):  # rho, p, T
         rel = np.abs(out["closure"][f] - out["exact"][f]).max() / np.abs(out["exact"][f]).max()
@@ -251,6 +254,7 @@ def test_short_training_run_learns_the_transport():
     d = _driver()
     w, rep = closure.train(d, SP, n_samples=100_000, n_val=20_000, epochs=10, batch=4096, lr=5e-3,
                            log=lambda *a: None)
+    d.set_closure_bound(0.0)  # the networks themselves
     d.set_closure(w)
     trained = closure.validate(d, SP, n=20_000, seed=8)
     d.set_closure(closure.ClosureNet(2 + 2 * ns, 2 + ns, "cuda", seed=7).export(w["out_mean"], w["out_scale"]))
