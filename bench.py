@@ -166,6 +166,33 @@ def ncu_traffic(kernel_tag):
     return None
 
 
+def ncu_instructions_per_point():
+    """Thread instructions per point of the TMA face kernel (FP32, 9 species)
+    from the committed ncu instruction-mix summary."""
+    path = os.path.join(ROOT, "profiles", "faces_update_instruction_mix_box96_mixed.txt")
+    try:
+        for ln in open(path):
+            if ln.startswith("thread_instructions_per_point:"):
+                return float(ln.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+def issue_roofline(instr_per_point, npts, kernel_ms, sm_mhz):
+    """The face kernel against its instruction-issue bound: every SM issues
+    at most 4 warp instructions (128 thread instructions) per cycle."""
+    if not instr_per_point or not sm_mhz:
+        return None
+    import torch
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    peak = n_sm * 4 * 32 * sm_mhz * 1e6  # thread instructions per second
+    bound_ms = instr_per_point * npts / peak * 1e3
+    return {"thread_instructions_per_point": instr_per_point, "source": "ncu instruction mix (96^3 capture)",
+            "issue_bound_ms": bound_ms, "kernel_ms": kernel_ms, "frac": bound_ms / kernel_ms,
+            "peak": "%d SMs x 4 schedulers x 32 lanes x %.0f MHz" % (n_sm, sm_mhz)}
+
+
 def max_over_ranks(ms, dist):
     """The slowest rank's time (replicas run independently; the job takes
     as long as its slowest GPU)."""
@@ -648,6 +675,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 fluxes/transport + f64 conserved/Newton/reductions", "data": "synthetic",
         "config": {"workload": WORKLOAD, "grid": "%d^3 points, 2 mm periodic cube" % args.n, "species": 9,
+                   "unique_points": "%d^3: the vertex-centred periodic box shares its end layer on each axis" %
+                                    (args.n - 1),
                    "scheme": "MUSCL-minmod + AUSM+ + 2nd-order viscous, SSP-RK3, CFL 0.5",
                    "precision": "mixed", "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (no flush)", "graph": "one CUDA graph per step"},
@@ -658,6 +687,9 @@ def main():
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "kernel": kname, "algorithmic_bytes_per_point": kbpp, "kernel_ms_per_launch": kms,
                      "peak_kind": peak_kind,
+                     "issue": (issue_roofline(ncu_instructions_per_point(), mixed["npts"], kms,
+                                              mixed["clocks"].get("sm_mhz")) if kname.startswith("k_faces_tma")
+                               else None),
                      "stage": {"ms": stage_ms, "faces_ms": kt["faces_ms"], "update_ms": kt["update_ms"],
                                "algorithmic_bytes_per_point": bpp, "achieved_gbs": stage_achieved,
                                "frac": stage_achieved / peaks["hbm_gbs"]}},
