@@ -55,7 +55,9 @@ def parse():
     ap.add_argument("--kz", type=int, default=4, help="k-planes per tile when --variant pins the stage kernels")
     ap.add_argument("--tile-j", type=int, default=0, help="points along j of the dq-tma tile when --variant pins it")
     ap.add_argument("--ref-n", type=int, default=128, help="box size of the reference-kernel timing (0 skips it)")
-    ap.add_argument("--ref-steps", type=int, default=5, help="timed steps of the reference-kernel timing")
+    ap.add_argument("--e2e-steps", type=int, default=E_STEPS, help="steps of the end-to-end job (profiling runs "
+                                                                     "shorten it)")
+    ap.add_argument("--ref-steps", type=int, default=2, help="timed steps of the reference-kernel timing")
     return ap.parse_args()
 
 
@@ -292,7 +294,7 @@ def run_ours(args, rank, world, dist):
         bv_o = pin(np.empty_like(bv_h))
         yk_o = pin(np.empty_like(yk_h))
         cv_o = pin(np.empty((14, ng)))
-        K = E_STEPS
+        K = args.e2e_steps
         res_h = pin(np.zeros((K, 4)))
         t0 = time.perf_counter()
         d.field[0].set_state(bv_h, yk_h)
