@@ -104,6 +104,7 @@ struct cc_ctx {
                                   // 3 split with TMA-staged face planes, 4 the same on persistent CTAs,
                                   // 5 face kernel differencing in the tile (dq) + update
   int face_ty = 8;                // variants 3-5: tile height of the TMA face kernel (32 x face_ty x kz points)
+  int update_occ = 0;             // 1: the FP32 update kernel sized for 4 CTAs per SM (autotuned)
   int force_ty = 0;               // cc_set_tuning: face tile height, 0 = autotune
   std::vector<Tile> hftiles;      // variants 3-5: tiles of the TMA face kernel
   std::vector<int> ft_begin;      // per block: first face tile (block-ordered list), + end
@@ -869,7 +870,7 @@ int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, i
     CK((Launch<T, NS>::faces_dq(a, face_tiles, c->d_tmaps + ((size_t)tma_shape(c->face_ty) * 2 + pc) * nb, c->chem,
                                 n_ft, c->face_ty, c->stream)));
     if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
-    CK((Launch<T, NS>::update(a, c->chem, nt, c->stream)));
+    CK((Launch<T, NS>::update(a, c->chem, nt, c->stream, c->update_occ)));
     return 0;
   }
   if (variant == 1) {
@@ -889,7 +890,7 @@ int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, i
       CK((Launch<T, NS>::faces(a, c->chem, 0, n_edge, c->stream)));
     }
     if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
-    CK((Launch<T, NS>::update(a, c->chem, nt, c->stream)));
+    CK((Launch<T, NS>::update(a, c->chem, nt, c->stream, c->update_occ)));
   } else {
     CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
   }
@@ -1077,8 +1078,12 @@ int autotune(cc_ctx *c) {
   for (int ty : {4, 8, 16})
     if ((c->force_ty <= 0 || ty == c->force_ty) && Launch<T, NS>::faces_tma_smem(ty) != 0) tys.push_back(ty);
   if (tys.empty()) return fail(CC_ERR_ARG, "the face tile height does not fit in shared memory in this precision");
+  const std::vector<int> occs = c->precision == CC_FP64 ? std::vector<int>{0} : std::vector<int>{0, 1};
+  int best_occ = 0;
   for (int variant : variants) {
     for (int ty : (variant >= 3 ? tys : std::vector<int>{8})) {
+      for (int occ : (variant >= 2 ? occs : std::vector<int>{0})) {
+      c->update_occ = occ;
       for (int kz : kzs) {
         build_tiles_kz(c, kz);
         CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
@@ -1096,12 +1101,15 @@ int autotune(cc_ctx *c) {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, e0, e1));
         if (verbose)
-          std::fprintf(stderr, "cc autotune: %s tile 32x%dx%d tiles=%d %.4f ms\n", kVariantName[variant],
-                       variant >= 3 ? ty : kTY, kz, variant >= 3 ? (int)c->hftiles.size() : nt, ms / 3);
-        if (ms / 3 < best) best = ms / 3, best_kz = kz, best_variant = variant, best_ty = ty;
+          std::fprintf(stderr, "cc autotune: %s tile 32x%dx%d update-occ %d tiles=%d %.4f ms\n",
+                       kVariantName[variant], variant >= 3 ? ty : kTY, kz, occ,
+                       variant >= 3 ? (int)c->hftiles.size() : nt, ms / 3);
+        if (ms / 3 < best) best = ms / 3, best_kz = kz, best_variant = variant, best_ty = ty, best_occ = occ;
+      }
       }
     }
   }
+  c->update_occ = best_occ;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   build_tiles_kz(c, best_kz);

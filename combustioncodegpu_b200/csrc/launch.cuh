@@ -149,8 +149,15 @@ cudaError_t Launch<T, NS>::faces_tma_persistent(const StageArgs<T> &a, const Til
 }
 
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s) {
+cudaError_t Launch<T, NS>::update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s,
+                                  int high_occ) {
   if (n_tiles <= 0) return cudaSuccess;
+  if constexpr (sizeof(T) == 4) {
+    if (high_occ) {
+      k_update<T, NS, 4><<<n_tiles, dim3(kTX, kTY), update_smem(), s>>>(a, C);
+      return cudaGetLastError();
+    }
+  }
   k_update<T, NS><<<n_tiles, dim3(kTX, kTY), update_smem(), s>>>(a, C);
   return cudaGetLastError();
 }

@@ -21,7 +21,9 @@ struct Launch {
   static size_t faces_smem();
   static size_t update_smem();
   static cudaError_t faces(const StageArgs<T> &a, const ChemParams &C, int n_regular, int n_edge, cudaStream_t s);
-  static cudaError_t update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s);
+  // update kernel; high_occ = 1 runs the FP32 form sized for 4 CTAs per SM
+  static cudaError_t update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s,
+                            int high_occ = 0);
   // split variant with TMA-staged planes in the face kernel (regular tiles only)
   // TMA face kernel on tiles of 32 x ty points (ty = 4, 8, 16; 16 in FP32
   // only): smem 0 when the ring does not fit

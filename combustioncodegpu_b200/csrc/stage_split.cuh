@@ -82,8 +82,10 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
   put(d, p);
 }
 
-template <typename T, int NS>
-__global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 2 : 3)
+// MINB: CTAs per SM the registers are sized for (the autotuner tries 4 in
+// FP32: 64 registers with some spills against 80 at 3).
+template <typename T, int NS, int MINB = (sizeof(T) == 8 ? 2 : 3)>
+__global__ void __launch_bounds__(kTX *kTY, MINB)
     k_update(const StageArgs<T> a, const __grid_constant__ ChemParams C) {
   constexpr int A = SpecCount<NS>::kArr;
   constexpr int NV = 5 + A;
