@@ -102,3 +102,25 @@ def test_struct_layouts_match_reference_pods():
     # cfd::Boundary is 9 ints, cfd::InnerFace 26 ints (Mesh.h:9-60)
     assert ctypes.sizeof(cc.CCBoundary) == 9 * 4
     assert ctypes.sizeof(cc.CCInnerFace) == 26 * 4
+
+
+def test_multi_process_entry_points_validate_arguments(cclib):
+    """cc_set_owned_blocks refuses blocks that do not exist, and the
+    exchange's pack / unpack refuse to run outside cc_init and an exchange
+    hook call (no device needed for either check)."""
+    case = cases.case_multiblock(([6, 7], [6, 5], [5]), species=cases.synthetic_species())
+    d = cc.Driver.from_case(case)
+    bad = (ctypes.c_int * 1)(7)
+    assert cclib.cc_set_owned_blocks(d.ctx, bad, 1) == -1
+    assert b"no block 7" in cclib.cc_last_error()
+    good = (ctypes.c_int * 2)(0, 3)
+    assert cclib.cc_set_owned_blocks(d.ctx, good, 2) == 0
+    assert cclib.cc_set_owned_blocks(d.ctx, None, 0) == 0  # every block again
+    nf = ctypes.c_int()
+    assert cclib.cc_exchange_fields(d.ctx, ctypes.byref(nf)) == 0
+    assert nf.value == (6 + 9) + (2 + 9) + (5 + 9)
+    idx = np.zeros(1, dtype=np.int64)
+    out = np.zeros(nf.value)
+    assert cclib.cc_pack_points(d.ctx, 0, idx.ctypes.data_as(ctypes.c_void_p), 1,
+                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == -2  # before cc_init
+    d.close()
