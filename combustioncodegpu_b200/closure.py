@@ -123,7 +123,7 @@ def one_cycle(step, total, max_lr, pct_start=0.05, div_factor=25.0, final_div_fa
     return cos(max_lr, lo_lr / final_div_factor, t), cos(beta_lo, beta_hi, t)
 
 
-def train(driver, species, n_samples=2_000_000, n_val=200_000, epochs=60, batch=4096, lr=2e-3, seed=7,
+def train(driver, species, n_samples=2_000_000, n_val=200_000, epochs=600, batch=4096, lr=4e-3, seed=7,
           device="cuda", log=print):
     """Fit the closure to the exact transport of `driver`'s species tables
     with the library's training kernels (cc_mlp_grad: quantisation-aware
@@ -235,8 +235,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--samples", type=int, default=2_000_000)
-    ap.add_argument("--epochs", type=int, default=60)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--epochs", type=int, default=600)
+    ap.add_argument("--lr", type=float, default=4e-3)
     ap.add_argument("--batch", type=int, default=4096)
     args = ap.parse_args()
     sp = cases.synthetic_species()
