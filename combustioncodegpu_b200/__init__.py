@@ -23,7 +23,9 @@ import numpy as np
 from . import cases  # noqa: F401
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libcc_b200.so")
+# CC_LIBRARY selects another build of the library (the bounds-checked
+# libcc_b200_bounds.so in its tests)
+LIB_PATH = os.environ.get("CC_LIBRARY") or os.path.join(_HERE, "libcc_b200.so")
 MAX_SPECIES = 16
 
 CC_FP64, CC_MIXED, CC_FP32 = 0, 1, 2

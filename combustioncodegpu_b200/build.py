@@ -3,6 +3,11 @@
 Every translation unit is compiled in parallel with nvcc
 (-gencode arch=compute_100a,code=sm_100a -lineinfo) and linked with the
 static CUDA runtime into combustioncodegpu_b200/libcc_b200.so.
+
+build(bounds=True) builds libcc_b200_bounds.so from the same sources with
+-DCC_BOUNDS_CHECK: the kernels check the arena, scratch and plane indices
+they compute and report an index out of range in the status word instead of
+accessing it (a stand-in for compute-sanitizer's memory check).
 """
 import concurrent.futures
 import os
@@ -14,6 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcc_b200.so")
+BUILD_BOUNDS = os.path.join(HERE, "_build_bounds")
+LIB_BOUNDS = os.path.join(HERE, "libcc_b200_bounds.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = [
     "api.cu", "misc.cu", "halo_plan.cpp", "noalloc.cu", "closure_train.cu",
@@ -40,18 +47,20 @@ def _stale(src, obj):
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(verbose=False, jobs=None):
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose=False, jobs=None, bounds=False):
+    build_dir, lib = (BUILD_BOUNDS, LIB_BOUNDS) if bounds else (BUILD, LIB)
+    extra = ["-DCC_BOUNDS_CHECK"] if bounds else []
+    os.makedirs(build_dir, exist_ok=True)
     nvcc = _nvcc()
     cmds = []
     objs = []
     for s in SOURCES:
         src = os.path.join(CSRC, s)
-        obj = os.path.join(BUILD, s + ".o")
+        obj = os.path.join(build_dir, s + ".o")
         objs.append(obj)
         if _stale(src, obj):
             lang = ["-x", "cu"] if s.endswith(".cu") else []
-            cmds.append([nvcc, *_flags(), *lang, "-c", src, "-o", obj])
+            cmds.append([nvcc, *_flags(), *extra, *lang, "-c", src, "-o", obj])
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -63,13 +72,13 @@ def build(verbose=False, jobs=None):
         for cmd in ex.map(run, cmds):
             if verbose:
                 print("compiled", cmd[-1], flush=True)
-    if cmds or not os.path.exists(LIB):
-        link = [nvcc, *ARCH, "-shared", "-o", LIB, *objs]
+    if cmds or not os.path.exists(lib):
+        link = [nvcc, *ARCH, "-shared", "-o", lib, *objs]
         r = subprocess.run(link, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv))
+    print(build(verbose="-v" in sys.argv, bounds="--bounds" in sys.argv))

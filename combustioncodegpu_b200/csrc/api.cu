@@ -601,6 +601,7 @@ int setup_device(cc_ctx *c) {
   c->d_dt_next = (unsigned long long *)p;
   if (dev_alloc(c, &p, sizeof(unsigned) * 4)) return CC_ERR_CUDA;
   c->d_status = (unsigned *)p;
+  c->chem.status = c->d_status;  // bounds-checked builds report there
   if (dev_alloc(c, &p, sizeof(double) * 8)) return CC_ERR_CUDA;  // norms, then their sums of squares
   c->d_res = (double *)p;
   if (dev_alloc(c, &p, sizeof(double) * 4 * c->n_partials)) return CC_ERR_CUDA;

@@ -53,6 +53,8 @@ struct ChemParams {
   // 1000; cc_set_newton_max_iter)
   int newton_max_iter;
   int pad_;
+  // status word of the context (bounds-checked builds report there)
+  unsigned *status;
   SpecTables<double> d;
   SpecTables<float> f;
 };
@@ -130,7 +132,32 @@ enum StatusBits : unsigned {
   kStatusNonFinite = 2u,     // NaN/Inf or non-positive rho/p/T after an update
   kStatusBadDt = 4u,         // global time step not positive and finite
   kStatusHaloTimeout = 32u,  // a grid-wide barrier of the single-launch halo program gave up
+  kStatusBounds = 64u,       // bounds-checked build: an index outside its array was caught
 };
+
+// Bounds-checked build (nvcc -DCC_BOUNDS_CHECK, libcc_b200_bounds.so): the
+// arena, scratch and plane indices the kernels compute are checked before
+// use; an index outside [0, n) sets kStatusBounds in the context's status
+// word and is replaced by 0, so the access stays inside the allocation.  It
+// stands in for compute-sanitizer's memory check.  In the normal build the
+// macros are the index itself.
+#if defined(CC_BOUNDS_CHECK) && defined(__CUDACC__)
+__device__ __forceinline__ int64_t ccb_checked_index(unsigned *status, int64_t idx, int64_t n) {
+  if (idx >= 0 && idx < n) return idx;
+  if (status) atomicOr(status, (unsigned)kStatusBounds);
+  return 0;
+}
+#define CCB_IDX(C, idx, n) ((decltype(idx))ccb_checked_index((C).status, (int64_t)(idx), (int64_t)(n)))
+#define CCB_CHECK(C, cond)                                                   \
+  do {                                                                       \
+    if (!(cond) && (C).status) atomicOr((C).status, (unsigned)kStatusBounds); \
+  } while (0)
+#else
+#define CCB_IDX(C, idx, n) (idx)
+#define CCB_CHECK(C, cond) \
+  do {                     \
+  } while (0)
+#endif
 
 // Arrival counter and generation of the bounded grid-wide barrier of the
 // single-launch halo program (zeroed at set-up; every completed barrier

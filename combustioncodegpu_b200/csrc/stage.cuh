@@ -88,7 +88,7 @@ __device__ __forceinline__ void face_flux_gen(const ChemParams &C, const T *rec,
   const int d = DIR >= 0 ? DIR : d_rt;
   constexpr int A = SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
-  const int p = gp, p1 = gp + gsd;
+  const int p = CCB_IDX(C, gp, N), p1 = CCB_IDX(C, gp + gsd, N);
   T v[4][5 + A];
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
@@ -234,6 +234,7 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
   constexpr int NV = 5 + A;
   const int ns = SpecCount<NS>::n(C);
   const int nv = 5 + ns;
+  p = CCB_IDX(C, p, N);
   const T *__restrict__ G = a.G;
   const double dtj = dt / (double)G[p];
   // whether this point's step enters the next global time step, read with
@@ -580,13 +581,14 @@ __device__ __forceinline__ void halo_node(const HaloArgs<T> &a, const ChemParams
   const int ns = SpecCount<NS>::n(C);
   const int nv = 5 + ns;
   const HaloNode nd = a.nodes[e];
-  const int64_t o = nd.slot;
+  const int64_t o = CCB_IDX(C, nd.slot, a.NS_cap);
   const int64_t S = a.NS_cap;
   double pr[6];
   double Y[A];
   double q[5 + A];
   bool props_copy = false;
   RefPtrs<T> ra = resolve(a, nd.a);
+  ra.idx = CCB_IDX(C, ra.idx, ra.stride);
   // every field is loaded into registers before the first store: the stores
   // may alias the sources as far as the compiler knows, and interleaving them
   // would serialise one memory round trip per field
@@ -615,6 +617,7 @@ __device__ __forceinline__ void halo_node(const HaloArgs<T> &a, const ChemParams
   }
   if (nd.op == kHaloAvg) {
     RefPtrs<T> rb = resolve(a, nd.b);
+    rb.idx = CCB_IDX(C, rb.idx, rb.stride);
     T xa[6 + A], xb[6 + A], vPr[2 + A];
     double qa[5 + A], qb[5 + A];
 #pragma unroll
@@ -689,6 +692,7 @@ __device__ __forceinline__ void halo_node(const HaloArgs<T> &a, const ChemParams
         pr[5] = tw;
       } else {
         RefPtrs<T> rb = resolve(a, nd.b);
+        rb.idx = CCB_IDX(C, rb.idx, rb.stride);
         const double tw = bc.thermal_type == 1 ? (double)rb.P[5 * rb.stride + rb.idx] : bc.t_wall;
         double tg = t_in;
         if (bc.thermal_type == 0) {
@@ -770,8 +774,10 @@ template <typename T, int NS>
 __device__ __forceinline__ double halo_copy(const HaloArgs<T> &a, const ChemParams &C, int64_t e, int which,
                                             int np, int npr, int nq) {
   constexpr int A = SpecCount<NS>::kArr;
-  const HaloCopy c = a.copies[a.begin + e];
-  const RefPtrs<T> r = resolve(a, c.src);
+  HaloCopy c = a.copies[a.begin + e];
+  c.dst = CCB_IDX(C, c.dst, a.N);
+  RefPtrs<T> r = resolve(a, c.src);
+  r.idx = CCB_IDX(C, r.idx, r.stride);
   double dt = 1e300;
   if (which == 0) {
     T v[6 + A];

@@ -127,13 +127,15 @@ __global__ void __launch_bounds__(kTX *kTY, MINB)
         for (int l = 0; l < NV; ++l)
           if (l < nv) dq[l] = (double)Fx[l * N + p];
       } else {
+        // the minus-side faces (checked in bounds-checked builds)
+        const int px = CCB_IDX(C, p - 1, N), py = CCB_IDX(C, p - sj, N), pz = CCB_IDX(C, p - sk, N);
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           if (l < nv) {
             const int o = l * N + p;
-            T acc = Fx[o] - Fx[o - 1];
-            acc += Fy[o] - Fy[o - sj];
-            if (three_d) acc += Fz[o] - Fz[o - sk];
+            T acc = Fx[o] - Fx[l * N + px];
+            acc += Fy[o] - Fy[l * N + py];
+            if (three_d) acc += Fz[o] - Fz[l * N + pz];
             dq[l] = -(double)acc;
           }
         }

@@ -424,16 +424,25 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
   auto slot_of = [&](int kp) { return (int)((pc0 + (unsigned)(kp - kfirst)) & (L::kRing - 1)); };
   auto parity_of = [&](int kp) { return ((pc0 + (unsigned)(kp - kfirst)) / L::kRing) & 1u; };
   const int k_pro = min(klast, kfirst + L::kRing - 1);
+  // request plane kp into its slot (thread 0).  Bounds-checked builds verify
+  // the tensor coordinates first (x on a 16-byte boundary, z inside the
+  // block's ghosted extent) and skip a bad request, whose wait then gives up.
+  auto issue = [&](int kp) {
+#ifdef CC_BOUNDS_CHECK
+    const bool ok = (tx0 * (int)sizeof(T)) % 16 == 0 && tx0 >= 0 && kp + B.g >= 0 && kp + B.g < B.nz;
+    CCB_CHECK(C, ok);
+    if (!ok) return;
+#endif
+    const int sl = slot_of(kp);
+    mbar_arrive_expect_tx(&bars[sl], plane_bytes);
+    tma_load_plane(ring + sl * L::kPlaneBytes, map, tx0, ty0, kp + B.g, &bars[sl]);
+  };
   if (tid == 0) {
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
                  : "memory");
     // a previous tile's threads read these slots through the generic proxy
     if (pc0 != 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    for (int kp = kfirst; kp <= k_pro; ++kp) {
-      const int sl = slot_of(kp);
-      mbar_arrive_expect_tx(&bars[sl], plane_bytes);
-      tma_load_plane(ring + sl * L::kPlaneBytes, map, tx0, ty0, kp + B.g, &bars[sl]);
-    }
+    for (int kp = kfirst; kp <= k_pro; ++kp) issue(kp);
   }
   int k_issued = k_pro;
 
@@ -472,10 +481,8 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
     __syncthreads();  // plane k-1 is no longer read
     if (k + 3 <= klast) {
       if (tid == 0) {
-        const int sl = slot_of(k + 3);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive_expect_tx(&bars[sl], plane_bytes);
-        tma_load_plane(ring + sl * L::kPlaneBytes, map, tx0, ty0, k + 3 + B.g, &bars[sl]);
+        issue(k + 3);
       }
       k_issued = k + 3;
     }
