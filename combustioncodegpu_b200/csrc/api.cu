@@ -1079,7 +1079,9 @@ int autotune(cc_ctx *c) {
   for (int ty : {4, 8, 16})
     if ((c->force_ty <= 0 || ty == c->force_ty) && Launch<T, NS>::faces_tma_smem(ty) != 0) tys.push_back(ty);
   if (tys.empty()) return fail(CC_ERR_ARG, "the face tile height does not fit in shared memory in this precision");
-  const std::vector<int> occs = c->precision == CC_FP64 ? std::vector<int>{0} : std::vector<int>{0, 1};
+  std::vector<int> occs = c->precision == CC_FP64 ? std::vector<int>{0} : std::vector<int>{0, 1};
+  if (const char *oe = std::getenv("CC_UPDATE_OCC"))  // pins it (profiling runs, whose timings are distorted)
+    occs.assign(1, c->precision == CC_FP64 ? 0 : (oe[0] == '1' ? 1 : 0));
   int best_occ = 0;
   for (int variant : variants) {
     for (int ty : (variant >= 3 ? tys : std::vector<int>{8})) {
