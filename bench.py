@@ -515,6 +515,7 @@ def run_closure(args):
             res[mode]["run_time_check"] = "4 samples per 128-point tile against the exact transport, bound 1e-3"
             d.set_closure_bound(0.0)  # the network alone
             res[mode]["closure_accuracy_fresh_states"] = closure.validate(d, sp, n=200_000, seed=31)
+            res[mode]["closure_accuracy_box_states"] = closure.validate(d, sp, n=200_000, seed=31, states="box")
         states[mode] = d.field[0].get_state()[0]
         d.close()
     sl = lambda a: a.reshape(6, n + 4, n + 4, n + 4)[:, 2:-2, 2:-2, 2:-2].reshape(6, -1)

@@ -5,8 +5,11 @@ The closure replaces the Wilke / constant-Schmidt transport evaluation
 log rhoD_1..rhoD_n) evaluated on the tensor cores (csrc/closure.cuh); points
 outside the training hull in T take the exact transport.
 
-Training data: T ~ U[t_min, t_max], X ~ Dirichlet(alpha * 1_n), Y from X;
-targets are the library's own exact FP64 transport of those points
+Training data: T ~ U[t_min, t_max] and compositions from three equal parts:
+X ~ Dirichlet(0.5 * 1_n) (near the edges of the simplex, a few species
+dominant), X ~ Dirichlet(4 * 1_n) (mixtures of all species) and
+Y ~ Dirichlet(2 * 1_n) (mixtures of all species by mass, whose mole
+fractions the light species dominate, as in the synthetic box); targets are the library's own exact FP64 transport of those points
 (cc_eval_transport, mode 0).  The network is trained with the arithmetic of
 the kernel: inputs as BF16 (hi, lo) pairs, BF16 weights (rounding with a
 straight-through gradient), FP32 hidden activations (the kernel keeps them
@@ -37,13 +40,29 @@ T_CENTER, T_SCALE = 0.5 * (T_MIN + T_MAX), 0.5 * (T_MAX - T_MIN)
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "closure_weights.npz")
 
 
-def sample_states(n, species, seed, alpha=0.5, t_range=(T_MIN, T_MAX)):
-    """n random states: T [n], Y [ns][n], X [ns][n]."""
+TRAIN_MIX = (("X", 0.5), ("X", 4.0), ("Y", 2.0))
+
+
+def sample_states(n, species, seed, mix=TRAIN_MIX, t_range=(T_MIN, T_MAX)):
+    """n random states: T [n], Y [ns][n], X [ns][n].  Each state's
+    composition comes from one part of `mix` (equal shares), a sequence of
+    (space, alpha): X ~ Dirichlet(alpha * 1_n) for space "X", Y ~
+    Dirichlet(alpha * 1_n) for "Y"; a single pair is accepted too."""
     rng = np.random.Generator(np.random.PCG64(seed))
     ns = species["n_spec"]
-    T = rng.uniform(t_range[0], t_range[1], n)
-    X = rng.dirichlet(np.full(ns, alpha), n).T
     mw = np.asarray(species["mw"])[:, None]
+    if isinstance(mix[0], str):
+        mix = (mix,)
+    T = rng.uniform(t_range[0], t_range[1], n)
+    which = rng.integers(0, len(mix), n)
+    X = np.empty((ns, n))
+    for i, (space, a) in enumerate(mix):
+        m = which == i
+        v = rng.dirichlet(np.full(ns, a), int(m.sum())).T
+        if space == "Y":
+            v = v / mw
+            v /= v.sum(axis=0, keepdims=True)
+        X[:, m] = v
     Y = X * mw / (X * mw).sum(axis=0, keepdims=True)
     return T, Y, X
 
@@ -207,10 +226,25 @@ def _err_summary(rel):
             "per_output_p99": [float(v) for v in np.percentile(rel, 99, axis=1)]}
 
 
-def validate(driver, species, n=200_000, seed=99):
+def box_states(n, species, seed):
+    """About n states of the synthetic multispecies box generator
+    (cases.multispecies_fields: T in [300, 1500] K, smooth positive Y_k) on a
+    cube of its own seed: T [m], Y [ns][m]."""
+    from . import cases
+    side = max(4, int(round(n ** (1.0 / 3.0))) - 4)
+    bv, yk = cases.multispecies_fields((side, side, side), species, seed=seed)
+    return bv[5], yk
+
+
+def validate(driver, species, n=200_000, seed=99, states="train"):
     """Relative error of the closure kernel (as uploaded to driver) against
-    the exact transport on fresh states inside the hull."""
-    T, Y, _ = sample_states(n, species, seed)
+    the exact transport on fresh states inside the hull: states "train"
+    (the training distribution), "edge" (its X ~ Dirichlet(0.5) part only)
+    or "box" (the synthetic box generator's states, box_states)."""
+    if states == "box":
+        T, Y = box_states(n, species, seed)
+    else:
+        T, Y, _ = sample_states(n, species, seed, mix=("X", 0.5) if states == "edge" else TRAIN_MIX)
     exact = driver.eval_transport(T, Y, "exact")
     got = driver.eval_transport(T, Y, "closure")
     return _err_summary(np.abs(got / exact - 1.0))
@@ -242,14 +276,16 @@ def main():
     sp = cases.synthetic_species()
     d = cc.Driver.from_case(cases.case_box(4, species=sp), "mixed")
     w, report = train(d, sp, n_samples=args.samples, epochs=args.epochs, lr=args.lr, batch=args.batch)
-    d.set_closure(w)
-    d.set_closure_bound(0.0)  # the network alone
-    report["kernel_rel_err"] = validate(d, sp)
-    d.set_closure_bound(1e-3)  # with the run-time check: the share of points it sends to the exact transport
-    d.set_closure(w)
-    report["kernel_rel_err_with_check"] = validate(d, sp)
-    n_eval, n_hull, n_chk = d.closure_stats()
-    report["check_fallback_rate"] = n_chk / max(1, n_eval)
+    for states in ("train", "edge", "box"):
+        sfx = "" if states == "train" else "_" + states
+        d.set_closure(w)
+        d.set_closure_bound(0.0)  # the network alone
+        report["kernel_rel_err" + sfx] = validate(d, sp, states=states)
+        d.set_closure_bound(1e-3)  # with the run-time check: the share of points it sends to the exact transport
+        d.set_closure(w)
+        report["kernel_rel_err_with_check" + sfx] = validate(d, sp, states=states)
+        n_eval, n_hull, n_chk = d.closure_stats()
+        report["check_fallback_rate" + sfx] = n_chk / max(1, n_eval)
     d.close()
     save(args.out, w, report)
     print(json.dumps(report))

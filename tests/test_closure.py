@@ -82,14 +82,17 @@ def _trained():
     return closure.load()[0]
 
 
-def test_trained_closure_accuracy():
+@pytest.mark.parametrize("states", ["train", "edge", "box"])
+def test_trained_closure_accuracy(states):
     """The network alone (run-time check off) on fresh states inside the
-    hull: median relative error over the 11 outputs at most 1e-3."""
+    hull, from the training distribution, from its Dirichlet(0.5) half, and
+    from the synthetic box generator: median relative error over the 11
+    outputs at most 1e-3."""
     w = _trained()
     d = _driver()
     d.set_closure(w)
     d.set_closure_bound(0.0)
-    rep = closure.validate(d, SP, n=50_000, seed=5)
+    rep = closure.validate(d, SP, n=50_000, seed=5, states=states)
     d.close()
     assert rep["median"] <= 1e-3 and rep["p99"] < 1e-2, rep
 
