@@ -70,7 +70,12 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region.
+    The GPU is named by its UUID (the CUDA index and nvidia-smi's differ
+    under CUDA_VISIBLE_DEVICES).  Entering waits for nvidia-smi's first
+    sample, so the timed region starts with the sampler running; only the
+    samples after that count.  A region shorter than the 50 ms interval
+    takes the first sample after it."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -80,16 +85,33 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.start = 0
+
+    @staticmethod
+    def _smi_id(index):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            return uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [v.strip() for v in vis.split(",") if v.strip()]
+            return ids[index] if index < len(ids) else str(index)
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                ["nvidia-smi", "-i", self._smi_id(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and self.proc.poll() is None and time.time() - t0 < 10:
+                time.sleep(0.005)
         except Exception:
             self.proc = None
+        self.start = len(self.lines)
         return self
 
     def _read(self):
@@ -98,6 +120,9 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc:
+            t0 = time.time()
+            while len(self.lines) <= self.start and self.proc.poll() is None and time.time() - t0 < 1:
+                time.sleep(0.002)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -107,7 +132,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.start:]:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
