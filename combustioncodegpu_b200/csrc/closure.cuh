@@ -112,6 +112,26 @@ __device__ __forceinline__ uint32_t mlp_pack(float a, float b) {
   return *reinterpret_cast<uint32_t *>(&h);
 }
 
+// BF16 (hi, lo) split of a hidden activation with integer operations only
+// (the conversion instructions share the transcendental unit with the
+// SiLU's exponential and reciprocal, which bound the kernel): adding 0x8000
+// to the bits of x rounds its magnitude to the nearest BF16 in the upper 16
+// bits (ties away from zero; a carry moves into the exponent correctly), so
+// hi = those upper bits; lo = x - hi is exact in FP32 and is rounded the same
+// way.  |x - hi - lo| <= 2^-16 |x| for normal x.  The returned words carry
+// the BF16 value in their upper halves.
+__device__ __forceinline__ void mlp_split(float x, uint32_t &hi_bits, uint32_t &lo_bits) {
+  hi_bits = __float_as_uint(x) + 0x8000u;
+  const float hi = __uint_as_float(hi_bits & 0xFFFF0000u);
+  lo_bits = __float_as_uint(x - hi) + 0x8000u;
+}
+
+// BF16x2 word of two split values: a in the low half, b in the high half
+// (the layout of __floats2bfloat162_rn(a, b)).
+__device__ __forceinline__ uint32_t mlp_pack_hi(uint32_t a_bits, uint32_t b_bits) {
+  return __byte_perm(a_bits, b_bits, 0x7632);
+}
+
 template <typename T, int NS>
 __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P, T *__restrict__ Pr, int64_t N,
                                                         const ClosureDev cl, unsigned *status,
@@ -260,21 +280,21 @@ __global__ void __launch_bounds__(kMlpRows) k_props_mlp(const T *__restrict__ P,
           mlp_ld16(t_row + 16 * q, v);
 #pragma unroll
           for (int i = 0; i < 16; ++i) v[i] = mlp_silu(v[i] + bias[16 * q + i]);
-          float lo[16];
+          uint32_t hb[16], lb[16];
 #pragma unroll
-          for (int i = 0; i < 16; ++i) lo[i] = v[i] - __bfloat162float(__float2bfloat16_rn(v[i]));
+          for (int i = 0; i < 16; ++i) mlp_split(v[i], hb[i], lb[i]);
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             uint4 w;
-            w.x = mlp_pack(v[8 * h], v[8 * h + 1]);
-            w.y = mlp_pack(v[8 * h + 2], v[8 * h + 3]);
-            w.z = mlp_pack(v[8 * h + 4], v[8 * h + 5]);
-            w.w = mlp_pack(v[8 * h + 6], v[8 * h + 7]);
+            w.x = mlp_pack_hi(hb[8 * h], hb[8 * h + 1]);
+            w.y = mlp_pack_hi(hb[8 * h + 2], hb[8 * h + 3]);
+            w.z = mlp_pack_hi(hb[8 * h + 4], hb[8 * h + 5]);
+            w.w = mlp_pack_hi(hb[8 * h + 6], hb[8 * h + 7]);
             *reinterpret_cast<uint4 *>(sH + mlp_off(kMlpRows, tid, 16 * q + 8 * h)) = w;
-            w.x = mlp_pack(lo[8 * h], lo[8 * h + 1]);
-            w.y = mlp_pack(lo[8 * h + 2], lo[8 * h + 3]);
-            w.z = mlp_pack(lo[8 * h + 4], lo[8 * h + 5]);
-            w.w = mlp_pack(lo[8 * h + 6], lo[8 * h + 7]);
+            w.x = mlp_pack_hi(lb[8 * h], lb[8 * h + 1]);
+            w.y = mlp_pack_hi(lb[8 * h + 2], lb[8 * h + 3]);
+            w.z = mlp_pack_hi(lb[8 * h + 4], lb[8 * h + 5]);
+            w.w = mlp_pack_hi(lb[8 * h + 6], lb[8 * h + 7]);
             *reinterpret_cast<uint4 *>(sHl + mlp_off(kMlpRows, tid, 16 * q + 8 * h)) = w;
           }
         }
