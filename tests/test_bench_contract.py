@@ -42,3 +42,30 @@ def test_reference_arm_line_has_every_key():
     assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_clock_sampler_counts_only_the_timed_region(tmp_path, monkeypatch):
+    """The sampler waits for nvidia-smi's first sample before the timed
+    region starts and summarises only the samples taken after that; a region
+    shorter than the sampling interval still gets the next sample.  A fake
+    nvidia-smi on PATH prints one line per interval: 1200 MHz before the
+    region (its first line), 1965 MHz after, sw_power_cap active."""
+    import time
+
+    import bench
+
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text(
+        "#!" + sys.executable + "\n"
+        "import sys, time\n"
+        "print('0, 1200, 1965, 300.0, 0x0, Not Active, Not Active, Not Active, Not Active', flush=True)\n"
+        "while True:\n"
+        "    time.sleep(0.05)\n"
+        "    print('0, 1965, 1965, 900.0, 0x4, Not Active, Not Active, Not Active, Active', flush=True)\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", str(tmp_path) + os.pathsep + os.environ.get("PATH", ""))
+    with bench.ClockSampler(0) as clk:
+        time.sleep(0.01)  # shorter than the 50 ms interval
+    s = clk.summary()
+    assert s["samples"] >= 1 and s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0, s
+    assert s["reasons"] == ["sw_power_cap"], s
