@@ -467,7 +467,11 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
     // stay in L2 without it)
     if (sizeof(T) == 8 && k + 2 <= B.mz - 1 + B.g) prefetch_props_geometry<T, TY>(a, B, t, k + 2, 2 + ns, tid);
     if (act) {
-#pragma unroll 1
+      // two faces interleaved in FP32 (their loads overlap: 0.74 -> 0.71 ms
+      // per launch at 128^3 despite the spills); one at a time in FP64, and
+      // all three interleaved spill too much (1.04 ms)
+      constexpr int kUnroll = sizeof(T) == 4 ? 2 : 1;
+#pragma unroll kUnroll
       for (int it = three_d ? 0 : 1; it < 3; ++it) {
         const int d = it == 0 ? 2 : it - 1;
         const int sd = d == 0 ? 1 : (d == 1 ? sj : sk);
