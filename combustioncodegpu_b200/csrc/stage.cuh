@@ -233,38 +233,32 @@ __device__ __forceinline__ void gamma_and_c(const ChemParams &C, const T *rec, T
 // Shu-Osher combination), FP64 primitives and Newton, transport properties of
 // the new state (Field.cu:178-210), |V| for the residual and the point's
 // contribution to the next global time step.
+// The conserved variable l of point p after the RK stage, from its residual
+// dq (TimeAdvanceFunc.cu:255-265; SSP-RK3 combination).
+template <typename T>
+__device__ __forceinline__ double conserved_update(const ChemParams &C, const StageArgs<T> &a, int p, int N, int l,
+                                                   double dql, double dtj, bool three_d) {
+  // momentum fluxes carry p - p_ref: add back -p_ref sum(k+ - k-) (zero on uniform grids)
+  if (a.gcl && l >= 1 && l <= 3) dql -= C.p_ref * a.gcl[(l - 1) * N + p];
+  double qs = a.Qin[l * N + p] + dql * dtj;
+  if (l == 3 && !three_d) qs = 0;
+  double q = (a.a != 0.0) ? a.a * a.Qn[l * N + p] + a.b * qs : qs;
+  if (a.q32) q = (double)(float)q;  // full-FP32 study: FP32 conserved state
+  return q;
+}
+
+// Stores the new conserved state q of point p, recovers its primitives (FP64
+// Newton), evaluates its transport and, when want_dt, its local time step.
 template <typename T, int NS>
-__device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, const double *rec_d,
-                                             const StageArgs<T> &a, int p, int N,
-                                             const double *dq, double dt, double t_warm, bool three_d,
-                                             unsigned &flags, double &dt_min) {
+__device__ __forceinline__ void point_finish(const ChemParams &C, const T *rec, const double *rec_d,
+                                             const StageArgs<T> &a, int p, int N, const double *q, double t_warm,
+                                             bool three_d, bool want_dt, unsigned &flags, double &dt_min) {
   constexpr int A = SpecCount<NS>::kArr;
-  constexpr int NV = 5 + A;
   const int ns = SpecCount<NS>::n(C);
   const int nv = 5 + ns;
-  p = CCB_IDX(C, p, N);
   const T *__restrict__ G = a.G;
-  const double dtj = dt / (double)G[p];
-  // whether this point's step enters the next global time step, read with
-  // the state rather than behind the stores below
-  const bool want_dt = a.dt_next && !((a.skip_dt[p >> 5] >> (p & 31)) & 1u);
-  double q[NV];
-  // all loads first, then the stores: Qout may alias Qin, so a store between
-  // two loads would keep the compiler from issuing the loads together
 #pragma unroll
-  for (int l = 0; l < NV; ++l) {
-    if (l < nv) {
-      double dql = dq[l];
-      // momentum fluxes carry p - p_ref: add back -p_ref sum(k+ - k-) (zero on uniform grids)
-      if (a.gcl && l >= 1 && l <= 3) dql -= C.p_ref * a.gcl[(l - 1) * N + p];
-      double qs = a.Qin[l * N + p] + dql * dtj;
-      if (l == 3 && !three_d) qs = 0;
-      q[l] = (a.a != 0.0) ? a.a * a.Qn[l * N + p] + a.b * qs : qs;
-      if (a.q32) q[l] = (double)(float)q[l];  // full-FP32 study: FP32 conserved state
-    }
-  }
-#pragma unroll
-  for (int l = 0; l < NV; ++l)
+  for (int l = 0; l < 5 + A; ++l)
     if (l < nv) a.Qout[l * N + p] = q[l];
   // primitives (TimeAdvanceFunc.cu:266-289), FP64
   const double rho = q[0];
@@ -352,6 +346,30 @@ __device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, 
     dt_min = fmin(dt_min, dtl);
   }
     }
+
+template <typename T, int NS>
+__device__ __forceinline__ void point_update(const ChemParams &C, const T *rec, const double *rec_d,
+                                             const StageArgs<T> &a, int p, int N,
+                                             const double *dq, double dt, double t_warm, bool three_d,
+                                             unsigned &flags, double &dt_min) {
+  constexpr int A = SpecCount<NS>::kArr;
+  constexpr int NV = 5 + A;
+  const int ns = SpecCount<NS>::n(C);
+  const int nv = 5 + ns;
+  p = CCB_IDX(C, p, N);
+  const T *__restrict__ G = a.G;
+  const double dtj = dt / (double)G[p];
+  // whether this point's step enters the next global time step, read with
+  // the state rather than behind the stores below
+  const bool want_dt = a.dt_next && !((a.skip_dt[p >> 5] >> (p & 31)) & 1u);
+  double q[NV];
+  // all loads first, then the stores: Qout may alias Qin, so a store between
+  // two loads would keep the compiler from issuing the loads together
+#pragma unroll
+  for (int l = 0; l < NV; ++l)
+    if (l < nv) q[l] = conserved_update<T>(C, a, p, N, l, dq[l], dtj, three_d);
+  point_finish<T, NS>(C, rec, rec_d, a, p, N, q, t_warm, three_d, want_dt, flags, dt_min);
+}
 
 // L2 prefetch of elements [s, e) of one field row through the bulk copy
 // engine: a hint that nothing waits on.  The range is clamped to the field's

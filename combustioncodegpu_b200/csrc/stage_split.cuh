@@ -119,27 +119,7 @@ __global__ void __launch_bounds__(kTX *kTY, MINB)
     // previous point's stores)
     const double dt_global = a.local_dt ? 0.0 : *a.dt;
     for (int k = t.k0; k < t.k1; ++k) {
-      const int p = col + sk * k;
-      // dq = -(sum over directions of F(+1/2) - F(-1/2)), the fused kernel's order
-      double dq[NV];
-      if (a.dq_direct) {  // dq differenced by the face kernel (k_faces_dq)
-#pragma unroll
-        for (int l = 0; l < NV; ++l)
-          if (l < nv) dq[l] = (double)Fx[l * N + p];
-      } else {
-        // the minus-side faces (checked in bounds-checked builds)
-        const int px = CCB_IDX(C, p - 1, N), py = CCB_IDX(C, p - sj, N), pz = CCB_IDX(C, p - sk, N);
-#pragma unroll
-        for (int l = 0; l < NV; ++l) {
-          if (l < nv) {
-            const int o = l * N + p;
-            T acc = Fx[o] - Fx[l * N + px];
-            acc += Fy[o] - Fy[l * N + py];
-            if (three_d) acc += Fz[o] - Fz[l * N + pz];
-            dq[l] = -(double)acc;
-          }
-        }
-      }
+      const int p = CCB_IDX(C, col + sk * k, N);
       double dt;
       if (a.local_dt) {
         T Y[A];
@@ -153,7 +133,33 @@ __global__ void __launch_bounds__(kTX *kTY, MINB)
       } else {
         dt = dt_global;
       }
-      point_update<T, NS>(C, sRec, sRecD, a, p, N, dq, dt, (double)P[5 * N + p], three_d, flags, dt_min);
+      const double dtj = dt / (double)a.G[p];
+      // whether this point's step enters the next global time step, read with
+      // the state rather than behind the stores
+      const bool want_dt = a.dt_next && !((a.skip_dt[p >> 5] >> (p & 31)) & 1u);
+      // dq = -(sum over directions of F(+1/2) - F(-1/2)), the fused kernel's
+      // order, and the new conserved state, each variable's faces and state
+      // read together; the stores follow (Qout may alias Qin)
+      double q[NV];
+      if (a.dq_direct) {  // dq differenced by the face kernel (k_faces_dq)
+#pragma unroll
+        for (int l = 0; l < NV; ++l)
+          if (l < nv) q[l] = conserved_update<T>(C, a, p, N, l, (double)Fx[l * N + p], dtj, three_d);
+      } else {
+        // the minus-side faces (checked in bounds-checked builds)
+        const int px = CCB_IDX(C, p - 1, N), py = CCB_IDX(C, p - sj, N), pz = CCB_IDX(C, p - sk, N);
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          if (l < nv) {
+            const int o = l * N + p;
+            T acc = Fx[o] - Fx[l * N + px];
+            acc += Fy[o] - Fy[l * N + py];
+            if (three_d) acc += Fz[o] - Fz[l * N + pz];
+            q[l] = conserved_update<T>(C, a, p, N, l, -(double)acc, dtj, three_d);
+          }
+        }
+      }
+      point_finish<T, NS>(C, sRec, sRecD, a, p, N, q, (double)P[5 * N + p], three_d, want_dt, flags, dt_min);
     }
   }
   if (a.dt_next) {
