@@ -146,6 +146,9 @@ struct cc_ctx {
   int64_t *d_xidx = nullptr;
   int64_t x_cap = 0;
   bool halo_coop = false;         // the device takes cooperative launches (single-launch halo program)
+  // the steps' halo programs leave the conserved state of ghost points,
+  // which no stage kernel reads; it is written before the state is read out
+  bool q_ghost_stale = false;
   LusgsArgs lu{};                 // LU-SGS work arrays (allocated by the first LU-SGS step)
   std::vector<int64_t> lu_hb;     // sweep positions where each hyperplane begins, + end
   int n_partials = 296;
@@ -707,7 +710,7 @@ HaloArgs<T> halo_args(cc_ctx *c, int pn, int pp, double *qn, const double *qp) {
 // forms run the same device functions: identical results.
 template <typename T, int NS>
 int run_halo(cc_ctx *c, int pn, int pp, double *qn, const double *qp, unsigned long long *dt_next = nullptr,
-             double *vel = nullptr) {
+             double *vel = nullptr, int q_filter = 0) {
   HaloArgs<T> h = halo_args<T, NS>(c, pn, pp, qn, qp);
   h.G = (const T *)c->G;
   h.dt_next = dt_next;
@@ -725,7 +728,22 @@ int run_halo(cc_ctx *c, int pn, int pp, double *qn, const double *qp, unsigned l
     }
   }
   h.begin = 0, h.end = (int64_t)c->plan.copies.size();
-  CK((Launch<T, NS>::halo_copies(h, c->chem, vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream)));
+  CK((Launch<T, NS>::halo_copies(h, c->chem, vel, c->d_vel_zero, (int64_t)c->plan.vel_zero.size(), c->stream,
+                                 q_filter)));
+  return 0;
+}
+
+// The conserved state of the ghost points that the steps' halo programs left
+// (q_filter 1), from the sources of the last one: the current state and the
+// node slots it computed.
+template <typename T, int NS>
+int refresh_ghost_q(cc_ctx *c) {
+  if (!c->q_ghost_stale) return 0;
+  HaloArgs<T> h = halo_args<T, NS>(c, c->cur, 1 - c->cur, c->Q[c->qcur], c->Q[1 - c->qcur]);
+  h.G = (const T *)c->G;
+  h.begin = 0, h.end = (int64_t)c->plan.copies.size();
+  CK((Launch<T, NS>::halo_copies(h, c->chem, nullptr, nullptr, 0, c->stream, 2, true)));
+  c->q_ghost_stale = false;
   return 0;
 }
 
@@ -750,6 +768,7 @@ int derive_state(cc_ctx *c) {
   CK(cudaMemcpyAsync(c->P[1], c->P[0], c->elem * N * np_of(c), cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->Pr[1], c->Pr[0], c->elem * N * npr_of(c), cudaMemcpyDeviceToDevice, c->stream));
   if (int r = run_halo<T, NS>(c, 1, 0, c->Q[0], c->Q[1], nullptr, c->d_vel)) return r;
+  c->q_ghost_stale = false;
   c->cur = 1;
   // inflow transport properties: evaluated once by the same point function
   CK((Launch<T, NS>::dt_reduce(c->chem, c->d_blocks_owned, (int)c->hblocks_owned.size(), (const T *)c->P[1],
@@ -906,7 +925,8 @@ int after_stage(cc_ctx *c, const StageArgs<T> &a, int pn, int pc, double *qout, 
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
   if (int r = exchange_stage(c, stage, pn, pc, qout, const_cast<double *>(qin))) return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
-  if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next, a.vel ? c->d_vel : nullptr)) return r;
+  if (int r = run_halo<T, NS>(c, pn, pc, qout, qin, a.dt_next, a.vel ? c->d_vel : nullptr, c->hook ? 0 : 1))
+    return r;
   if (int r = prof_event(c, c->ev_halo, c->ev_next_halo)) return r;
   return 0;
 }
@@ -1194,6 +1214,7 @@ void destroy_graphs(cc_ctx *c) {
 
 template <typename T, int NS>
 int step_once(cc_ctx *c, int scheme) {
+  c->q_ghost_stale = !c->hook;  // with a hook every halo copy runs
   if (!c->use_graph || c->hook) return enqueue_step<T, NS>(c, scheme);  // the hook runs on the host between launches
   cudaGraphExec_t &ge = c->graph[scheme][c->cur];
   if (!ge) {
@@ -1587,6 +1608,9 @@ int cc_get_state(cc_ctx *c, int block, double *bv, double *yk, double *cv, int l
     if (int r = field_to64(c, c->P[c->cur], 6 + l)) return r;
     if (int r = copy_field_d2h(c, b, c->tmp64, yk + l * ng)) return r;
   }
+  if (cv && c->q_ghost_stale)
+    if (int r = dispatch(c, [&](auto tt, auto nn) { return refresh_ghost_q<typename decltype(tt)::type, decltype(nn)::value>(c); }))
+      return r;
   for (int f = 0; f < nv_of(c) && cv; ++f)
     if (int r = copy_field_d2h(c, b, c->Q[c->qcur] + (int64_t)f * c->N, cv + f * ng)) return r;
   CK(cudaStreamSynchronize(c->stream));
@@ -1707,8 +1731,10 @@ int cc_time_kernels(cc_ctx *c, int n_steps, int scheme, double out_ms[6]) {
   c->profiling = true;
   c->ev_next_stage = c->ev_next_halo = c->ev_next_mid = 0;
   int r = dispatch(c, [&](auto tt, auto nn) -> int {
-    for (int s = 0; s < n_steps; ++s)
+    for (int s = 0; s < n_steps; ++s) {
+      c->q_ghost_stale = !c->hook;
       if (int e = enqueue_step<typename decltype(tt)::type, decltype(nn)::value>(c, scheme)) return e;
+    }
     return 0;
   });
   c->profiling = false;
@@ -1967,6 +1993,10 @@ int ckpt_io(cc_ctx *c, const char *path, bool save) {
     void *dev;
     size_t bytes;
   };
+  if (save && c->q_ghost_stale)
+    if (int r = dispatch(c, [&](auto tt, auto nn) { return refresh_ghost_q<typename decltype(tt)::type, decltype(nn)::value>(c); }))
+      return r;
+  if (!save) c->q_ghost_stale = false;  // the file holds every point's conserved state
   const Part parts[] = {{c->Q[c->qcur], sizeof(double) * N * nv_of(c)},
                         {c->P[c->cur], c->elem * N * np_of(c)},
                         {c->Pr[c->cur], c->elem * N * npr_of(c)},

@@ -261,7 +261,9 @@ struct HaloNode {
   int bc;
 };
 
-// src.pad of a copy: bit 0 = dst is an interior point, bit 1 = its block is 3D.
+// src.pad of a copy: bit 0 = dst is an interior point, bit 1 = its block is
+// 3D, bit 2 = dst is itself read by the halo program (a node operand or a
+// copy source, as a stage or previous value).
 struct HaloCopy {
   int64_t dst;
   HaloRef src;

@@ -327,6 +327,18 @@ bool Replay::run(HaloPlan &plan) {
     if (flags & 1) plan.interior_copies.push_back((int64_t)plan.copies.size());
     plan.copies.push_back(hc);
   }
+  // bit 2: the destination is read by the program itself as a stage or
+  // previous value (a node operand or a copy source), so its every value
+  // matters, not only the last one
+  std::unordered_map<int64_t, char> read;
+  for (const auto &hn : plan.nodes) {
+    if (hn.a.kind == 0 || hn.a.kind == 1) read[hn.a.idx] = 1;
+    if (hn.b.kind == 0 || hn.b.kind == 1) read[hn.b.idx] = 1;
+  }
+  for (const auto &hc : plan.copies)
+    if (hc.src.kind == 0 || hc.src.kind == 1) read[hc.src.idx] = 1;
+  for (auto &hc : plan.copies)
+    if (read.count(hc.dst)) hc.src.pad |= 4;
   return true;
 }
 

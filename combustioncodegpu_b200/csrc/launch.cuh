@@ -294,13 +294,14 @@ cudaError_t Launch<T, NS>::halo_nodes(const HaloArgs<T> &a, const ChemParams &C,
 
 template <typename T, int NS>
 cudaError_t Launch<T, NS>::halo_copies(const HaloArgs<T> &a, const ChemParams &C, double *vel,
-                                       const int64_t *vel_zero, int64_t n_vel_zero, cudaStream_t s) {
+                                       const int64_t *vel_zero, int64_t n_vel_zero, cudaStream_t s, int q_filter,
+                                       bool only_q) {
   const int64_t n = std::max<int64_t>(a.end - a.begin, vel ? n_vel_zero : 0);
   if (n <= 0) return cudaSuccess;
   const int ns = C.ns, np = 6 + ns, npr = 2 + ns, nq = 5 + ns;
   const int tpb = 256;
-  k_halo_copy_fields<T, NS><<<dim3((unsigned)((n + tpb - 1) / tpb), 3), tpb, 0, s>>>(a, C, np, npr, nq, vel,
-                                                                                      vel_zero, n_vel_zero);
+  k_halo_copy_fields<T, NS><<<dim3((unsigned)((n + tpb - 1) / tpb), only_q ? 1 : 3), tpb, 0, s>>>(
+      a, C, np, npr, nq, vel, vel_zero, n_vel_zero, q_filter, only_q ? 2 : 0);
   return cudaGetLastError();
 }
 

@@ -56,8 +56,10 @@ struct Launch {
   static cudaError_t halo_nodes(const HaloArgs<T> &a, const ChemParams &C, cudaStream_t s);
   // the copies of the halo program, with the post-exchange time step
   // (a.dt_next) and the zeroing of |V| at wall faces (vel, when not null)
+  // q_filter: 0 every copy; 1 not the conserved state of ghost points (steps);
+  // 2 only that (before the state is read out); only_q: the Q pass alone
   static cudaError_t halo_copies(const HaloArgs<T> &a, const ChemParams &C, double *vel, const int64_t *vel_zero,
-                                 int64_t n_vel_zero, cudaStream_t s);
+                                 int64_t n_vel_zero, cudaStream_t s, int q_filter = 0, bool only_q = false);
   // every node level of the halo program in one cooperative launch
   static cudaError_t halo_levels(const HaloArgs<T> &a, const ChemParams &C, const HaloLevels &lv, GridBarrier *bar,
                                  unsigned *status, cudaStream_t s);

@@ -798,9 +798,18 @@ __device__ __forceinline__ double halo_copy_dt(const HaloArgs<T> &a, const ChemP
 
 template <typename T, int NS>
 __device__ __forceinline__ double halo_copy(const HaloArgs<T> &a, const ChemParams &C, int64_t e, int which,
-                                            int np, int npr, int nq) {
+                                            int np, int npr, int nq, int q_filter = 0) {
   constexpr int A = SpecCount<NS>::kArr;
   HaloCopy c = a.copies[a.begin + e];
+  if (which == 2 && q_filter != 0) {
+    // a ghost point's conserved state: no stage kernel reads it (they read Q
+    // at interior points only), so steps leave it (q_filter 1) and a later
+    // pass writes it before the state is read out (q_filter 2).  Ghost points
+    // the halo program itself reads (bit 2) and copies of a previous value
+    // keep running every time, so those chains stay exact.
+    const bool ghost = (c.src.pad & 5) == 0 && c.src.kind != 1;
+    if (ghost == (q_filter == 1)) return 1e300;
+  }
   c.dst = CCB_IDX(C, c.dst, a.N);
   RefPtrs<T> r = resolve(a, c.src);
   r.idx = CCB_IDX(C, r.idx, r.stride);
@@ -836,21 +845,24 @@ __device__ __forceinline__ double halo_copy(const HaloArgs<T> &a, const ChemPara
 }
 
 // Phase B in one launch: every changed point from its resolved source (grid
-// y selects P, Pr or Q; consecutive threads take consecutive copies), the
+// y + y0 selects P, Pr or Q; consecutive threads take consecutive copies;
+// q_filter as in halo_copy), the
 // post-exchange time step of the rewritten interior points (a.dt_next), and
 // the zeroing of |V| at wall-face points (vel).
 template <typename T, int NS>
 __global__ void k_halo_copy_fields(const HaloArgs<T> a, const __grid_constant__ ChemParams C, int np, int npr,
-                                   int nq, double *vel, const int64_t *vel_zero, int64_t n_vel_zero) {
+                                   int nq, double *vel, const int64_t *vel_zero, int64_t n_vel_zero, int q_filter,
+                                   int y0) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // copy (grid x)
+  const int which = (int)blockIdx.y + y0;
   double dt = 1e300;
-  if (e < a.end - a.begin) dt = halo_copy<T, NS>(a, C, e, blockIdx.y, np, npr, nq);
-  if (a.dt_next && blockIdx.y == 0) {
+  if (e < a.end - a.begin) dt = halo_copy<T, NS>(a, C, e, which, np, npr, nq, q_filter);
+  if (a.dt_next && which == 0) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
     if ((threadIdx.x & 31) == 0) atomic_min_pos_double(a.dt_next, dt);
   }
-  if (vel && blockIdx.y == 2)
+  if (vel && which == 2)
     for (int64_t z = e; z < n_vel_zero; z += (int64_t)gridDim.x * blockDim.x) vel[vel_zero[z]] = 0.0;
 }
 

@@ -523,3 +523,33 @@ def test_tma_variants_refused_without_tensor_maps():
         with pytest.raises(RuntimeError, match="TMA variants"):
             d.initialize_computation()
         d.close()
+
+
+@pytest.mark.parametrize("name", ["channel", "multiblock", "mixing", "box"])
+@pytest.mark.parametrize("precision,scheme", [("fp64", "rk3"), ("mixed", "rk3"), ("fp64", "steady")])
+def test_ghost_conserved_state_written_before_read_out(name, precision, scheme):
+    """Steps leave the conserved state of ghost points that nothing reads
+    (the stage kernels read Q at interior points only) and cc_get_state
+    writes it first.  A no-op exchange hook makes every step run every halo
+    copy; both runs must give the same states at every point, ghost points
+    included, bit for bit."""
+    import ctypes
+
+    case = CASES[name]
+    out = []
+    for hooked in (False, True):
+        d = cc.Driver.from_case(case, precision)
+        if hooked:
+            def noop(user, event, stage, value):
+                return 0  # the local time step is the global one on one process
+
+            fn = cc.EXCHANGE_FN(noop)
+            assert d.lib.cc_set_exchange(d.ctx, ctypes.cast(fn, ctypes.c_void_p), None) == 0
+        d.initialize_computation()
+        d.simulate(3, scheme)
+        out.append([d.field[b].get_state()[2] for b in range(len(case["blocks"]))])
+        if hooked:
+            d.lib.cc_set_exchange(d.ctx, None, None)
+        d.close()
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
