@@ -164,7 +164,10 @@ int cc_residual(cc_ctx *ctx, double out[4]);
  * has reached the copy (cc_sync, or an event recorded after the call). */
 int cc_residual_async(cc_ctx *ctx, double *out);
 /* Device -> host: bv (6 fields), yk (n_spec), cv (n_var) in `layout`; null
- * skips an array. */
+ * skips an array.  The steps leave the conserved state of ghost points that
+ * no kernel reads; when cv is requested, those values are first written on
+ * the context's stream (once after a cc_step), so cv matches a halo program
+ * that wrote every point. */
 int cc_get_state(cc_ctx *ctx, int block, double *bv, double *yk, double *cv, int layout);
 /* DZone::mul / conductivity / rho_D (Field.h:52-56): [Ng], [Ng], [n_spec][Ng]. */
 int cc_get_props(cc_ctx *ctx, int block, double *mul, double *conductivity, double *rho_d);
