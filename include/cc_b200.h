@@ -299,10 +299,10 @@ int cc_use_closure(cc_ctx *ctx, int on);
 int cc_closure_stats(cc_ctx *ctx, int64_t out[3]);
 /* No counterpart in the reference.  Relative error bound of the closure's
  * run-time check: every 128-point tile is sampled at 4 fixed points (1 in
- * 32) against the exact transport (Transport.cu:43-96, the judge of the
- * network), and a tile whose sampled properties have a root-mean-square
- * relative error above the bound, or one above ten times the bound, takes
- * the exact transport.  Default 1e-3; 0 switches the check off. */
+ * 32) against the exact transport (Transport.cu:43-96, against which
+ * the network's error is measured), and a tile whose sampled properties
+ * have a root-mean-square relative error above the bound, or one above ten
+ * times the bound, takes the exact transport.  Default 1e-3; 0 switches the check off. */
 int cc_set_closure_bound(cc_ctx *ctx, double rel_err);
 /* Transport properties of n points (host arrays): T [n], Y [n_spec][n] ->
  * out [2 + n_spec][n] = (mu, lambda, rhoD_k), by the exact FP64 evaluation

@@ -10,8 +10,8 @@ pointwise transport it replaces.
   come from the ~2^-17 relative residue of the hi/lo pairs and the FP32
   summation order, so log-space errors stay below 1e-3 (max) and 1e-5
   (median);
-* the trained closure's accuracy against the exact transport (the judge of
-  its error) with the run-time check off: median relative error at most
+* the trained closure's accuracy against the exact transport (the measure
+  of its error) with the run-time check off: median relative error at most
   1e-3; and the run-time check itself (4 samples per 128-point tile: a tile
   goes back to the exact transport when its sampled relative error exceeds
   1e-3 in root mean square, or 1e-2 in one output): with the trained weights
