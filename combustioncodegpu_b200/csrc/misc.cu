@@ -1,6 +1,8 @@
 // Small kernels: precision conversion, time-step bookkeeping and the
 // convergence residual of Driver::compute_residual (Driver.cu:219-277,
 // TimeAdvanceFunc.cu:13-24 and 292-303), reduced deterministically in FP64.
+#include <algorithm>
+
 #include "launch.h"
 
 namespace ccb {
@@ -72,23 +74,6 @@ cudaError_t launch_dt_finalize(double *dt, unsigned long long *dt_next, unsigned
   return cudaGetLastError();
 }
 
-__device__ __forceinline__ int64_t interior_point(const BlockInfo *blocks, int nblocks, int64_t g) {
-  int lo = 0, hi = nblocks - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (blocks[mid].interior_off <= g)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  const BlockInfo &B = blocks[lo];
-  const int64_t r = g - B.interior_off;
-  const int64_t i = r % B.mx;
-  const int64_t j = (r / B.mx) % B.my;
-  const int64_t k = r / ((int64_t)B.mx * B.my);
-  return B.base + i + (int64_t)B.nx * j + (int64_t)B.nx * B.ny * k;
-}
-
 __global__ void k_zero_points(double *field, const int64_t *points, int64_t n) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) field[points[i]] = 0.0;
@@ -100,19 +85,53 @@ cudaError_t launch_zero_points(double *field, const int64_t *points, int64_t n, 
   return cudaGetLastError();
 }
 
+// Interior rows: the (j, k) rows of the listed blocks, in block order, then
+// k, then j; a row's points are contiguous both in the arena and in the
+// interior-only arrays.  Each warp walks its rows in increasing order, so the
+// block of a row is found by advancing from the previous one.
+struct RowCursor {
+  int b = 0;
+  int64_t first = 0;  // first row of block b
+  __device__ __forceinline__ void seek(const BlockInfo *blocks, int nblocks, int64_t r) {
+    while (b + 1 < nblocks && r >= first + (int64_t)blocks[b].my * blocks[b].mz) {
+      first += (int64_t)blocks[b].my * blocks[b].mz;
+      ++b;
+    }
+  }
+};
+
+__device__ __forceinline__ int64_t interior_rows(const BlockInfo *blocks, int nblocks) {
+  int64_t n = 0;
+  for (int b = 0; b < nblocks; ++b) n += (int64_t)blocks[b].my * blocks[b].mz;
+  return n;
+}
+
 // store_last_step: (rho, |V|, p, T) of every interior point; |V| is DZone::vel
 // (written by the update, zeroed by wall conditions, untouched by interface
-// exchanges; TimeAdvanceFunc.cu:13-24).
+// exchanges; TimeAdvanceFunc.cu:13-24).  One warp per row, lanes along i.
 template <typename T>
 __global__ void k_store_last(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
                              int64_t n_int, double *last) {
-  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (g >= n_int) return;
-  const int64_t p = interior_point(blocks, nblocks, g);
-  last[g] = P[p];
-  last[n_int + g] = vel[p];
-  last[2 * n_int + g] = P[4 * N + p];
-  last[3 * n_int + g] = P[5 * N + p];
+  const int lane = threadIdx.x & 31;
+  const int64_t n_rows = interior_rows(blocks, nblocks);
+  const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  RowCursor cur;
+  for (int64_t r = w0; r < n_rows; r += nw) {
+    cur.seek(blocks, nblocks, r);
+    const BlockInfo &B = blocks[cur.b];
+    const int64_t rr = r - cur.first;
+    const int j = (int)(rr % B.my), k = (int)(rr / B.my);
+    const int64_t g0 = B.interior_off + (int64_t)B.mx * rr;
+    const int64_t p0 = B.base + (int64_t)B.nx * j + (int64_t)B.nx * B.ny * k;
+    for (int i = lane; i < B.mx; i += 32) {
+      const int64_t g = g0 + i, p = p0 + i;
+      last[g] = P[p];
+      last[n_int + g] = vel[p];
+      last[2 * n_int + g] = P[4 * N + p];
+      last[3 * n_int + g] = P[5 * N + p];
+    }
+  }
 }
 
 // Sum over a warp by shuffles in a fixed tree (the result does not depend on
@@ -123,23 +142,36 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// compute_square_of_dbv + per-CTA sums (warp shuffles, then the warps' sums
-// by the first warp, fixed order), then one warp sums the partials: the
-// result does not depend on scheduling.
+// compute_square_of_dbv + per-CTA sums: each warp takes interior rows in a
+// fixed order (lanes along i), then the warps' sums are added by the first
+// warp in a fixed order, then one warp sums the partials: the result does
+// not depend on scheduling.
 template <typename T>
 __global__ void k_residual_partial(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
                                    int64_t n_int, const double *last, double *partials) {
   double acc[4] = {0, 0, 0, 0};
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_int; g += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t p = interior_point(blocks, nblocks, g);
-    const double d0 = (double)P[p] - last[g];
-    const double d1 = vel[p] - last[n_int + g];
-    const double d2 = (double)P[4 * N + p] - last[2 * n_int + g];
-    const double d3 = (double)P[5 * N + p] - last[3 * n_int + g];
-    acc[0] += d0 * d0, acc[1] += d1 * d1, acc[2] += d2 * d2, acc[3] += d3 * d3;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+  const int64_t n_rows = interior_rows(blocks, nblocks);
+  const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  RowCursor cur;
+  for (int64_t r = w0; r < n_rows; r += nw) {
+    cur.seek(blocks, nblocks, r);
+    const BlockInfo &B = blocks[cur.b];
+    const int64_t rr = r - cur.first;
+    const int j = (int)(rr % B.my), k = (int)(rr / B.my);
+    const int64_t g0 = B.interior_off + (int64_t)B.mx * rr;
+    const int64_t p0 = B.base + (int64_t)B.nx * j + (int64_t)B.nx * B.ny * k;
+    for (int i = lane; i < B.mx; i += 32) {
+      const int64_t g = g0 + i, p = p0 + i;
+      const double d0 = (double)P[p] - last[g];
+      const double d1 = vel[p] - last[n_int + g];
+      const double d2 = (double)P[4 * N + p] - last[2 * n_int + g];
+      const double d3 = (double)P[5 * N + p] - last[3 * n_int + g];
+      acc[0] += d0 * d0, acc[1] += d1 * d1, acc[2] += d2 * d2, acc[3] += d3 * d3;
+    }
   }
   __shared__ double sh[4][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
 #pragma unroll
   for (int l = 0; l < 4; ++l) {
     const double w = warp_sum(acc[l]);
@@ -170,8 +202,8 @@ __global__ void k_residual_final(const double *partials, int n_partials, int64_t
 template <typename T>
 cudaError_t launch_store_last(const BlockInfo *blocks, int nblocks, const T *P, const double *vel, int64_t N,
                               int64_t n_interior, double *bv_last, cudaStream_t s) {
-  k_store_last<T><<<(unsigned)((n_interior + 255) / 256), 256, 0, s>>>(blocks, nblocks, P, vel, N, n_interior,
-                                                                        bv_last);
+  k_store_last<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(1184, (n_interior + 255) / 256)), 256, 0, s>>>(
+      blocks, nblocks, P, vel, N, n_interior, bv_last);
   return cudaGetLastError();
 }
 
