@@ -111,6 +111,7 @@ EXPORTS = {
                    ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "cc_set_tuning": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "cc_set_launch_mode": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "cc_set_tile_width": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_set_closure": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "cc_use_closure": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "cc_closure_stats": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
@@ -462,11 +463,14 @@ class Driver:
         _check(self.lib.cc_tuning(self.ctx, ctypes.byref(v), ctypes.byref(kz), _ptr(ms), tile))
         return {"variant": VARIANTS[v.value], "kz": kz.value, "stage_ms": float(ms[0]), "tile": tuple(tile)}
 
-    def set_tuning(self, variant="auto", kz=0, tile_j=0):
+    def set_tuning(self, variant="auto", kz=0, tile_j=0, tile_i=0):
         """Pin the stage-kernel configuration: variant "auto" or one of
         VARIANTS; kz k-planes per tile (0 = autotune); tile_j points along j
-        of the "dq-tma" tile (4, 8, 16; 0 = autotune)."""
+        of the TMA face kernels' tile (4, 8, 16; 0 = autotune); tile_i points
+        along i of the "split-tma" / "split-tma-p" face tile (32, 16; 0 =
+        autotune)."""
         v = (-1 if variant == "auto" else VARIANTS.index(variant)) if isinstance(variant, str) else int(variant)
+        _check(self.lib.cc_set_tile_width(self.ctx, int(tile_i)))
         _check(self.lib.cc_set_tuning(self.ctx, v, int(kz), int(tile_j)))
 
     def set_launch_mode(self, mode="batched"):

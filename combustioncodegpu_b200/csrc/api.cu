@@ -103,7 +103,9 @@ struct cc_ctx {
   int variant = 0;                // stage kernels: 0 fused (L1 stencil reads), 1 fused TMA planes, 2 split faces/update,
                                   // 3 split with TMA-staged face planes, 4 the same on persistent CTAs,
                                   // 5 face kernel differencing in the tile (dq) + update
-  int face_ty = 8;                // variants 3-5: tile height of the TMA face kernel (32 x face_ty x kz points)
+  int face_ty = 8;                // variants 3-5: tile height of the TMA face kernel (face_tx x face_ty x kz points)
+  int face_tx = 32;               // variants 3-4: tile width of the TMA face kernel (32 or 16; 32 for variant 5)
+  int force_tx = 0;               // cc_set_tile_width: face tile width, 0 = autotune
   int update_occ = 0;             // 1: the FP32 update kernel sized for 4 CTAs per SM (autotuned)
   int force_ty = 0;               // cc_set_tuning: face tile height, 0 = autotune
   std::vector<Tile> hftiles;      // variants 3-5: tiles of the TMA face kernel
@@ -289,14 +291,19 @@ void transpose_fields(const double *src, int64_t ng, int nf, std::vector<double>
 // Whether this process advances block b (cc_set_owned_blocks).
 bool owns(const cc_ctx *c, int b) { return c->owned.empty() || c->owned[(size_t)b]; }
 
-// Tensor-map plane boxes: tile heights 8 (the kTY tiles of the split and
-// fused kernels, and the dq kernel), 4 and 16 (dq kernel), each plus the
-// 2-point halo on both sides.
-constexpr int kTmaTileRows[3] = {8, 4, 16};
-int tma_shape(int ty) { return ty == 4 ? 1 : (ty == 16 ? 2 : 0); }
+// Tensor-map plane boxes, each a tile plus the 2-point halo on both sides:
+// 32 x 8 (the kTX x kTY tiles of the split and fused kernels), 32 x 4,
+// 32 x 16, 16 x 8 and 16 x 16 (the TMA face kernels, i x j).
+constexpr int kTmaShapes = 5;
+constexpr int kTmaTileRows[kTmaShapes] = {8, 4, 16, 8, 16};
+constexpr int kTmaTileCols[kTmaShapes] = {32, 32, 32, 16, 16};
+int tma_shape(int ty, int tx = 32) {
+  if (tx == 16) return ty == 16 ? 4 : 3;
+  return ty == 4 ? 1 : (ty == 16 ? 2 : 0);
+}
 
-// Work list of the TMA face kernels: 32 x ty columns, k split into chunks of kz.
-void build_face_tiles(cc_ctx *c, int ty, int kz) {
+// Work list of the TMA face kernels: tx x ty columns, k split into chunks of kz.
+void build_face_tiles(cc_ctx *c, int ty, int kz, int tx = 32) {
   c->hftiles.clear();
   c->ft_begin.clear();
   for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
@@ -305,7 +312,7 @@ void build_face_tiles(cc_ctx *c, int ty, int kz) {
     if (!owns(c, bi)) continue;
     for (int k0 = 0; k0 < b.mz; k0 += kz)
       for (int j0 = 0; j0 < b.my; j0 += ty)
-        for (int i0 = 0; i0 < b.mx; i0 += 32) {
+        for (int i0 = 0; i0 < b.mx; i0 += tx) {
           Tile t{};
           t.blk = bi, t.i0 = i0, t.j0 = j0, t.k0 = k0, t.k1 = std::min(b.mz, k0 + kz);
           c->hftiles.push_back(t);
@@ -313,11 +320,12 @@ void build_face_tiles(cc_ctx *c, int ty, int kz) {
   }
   c->ft_begin.push_back((int)c->hftiles.size());
   c->face_ty = ty;
+  c->face_tx = tx;
 }
 
 int max_face_tiles(cc_ctx *c) {
   int64_t n = 0;
-  for (const auto &b : c->blocks) n += (int64_t)((b.mx + 31) / 32) * ((b.my + 3) / 4) * b.mz;
+  for (const auto &b : c->blocks) n += (int64_t)((b.mx + 15) / 16) * ((b.my + 3) / 4) * b.mz;
   return (int)n;
 }
 
@@ -416,15 +424,15 @@ int build_tensor_maps(cc_ctx *c) {
   if (!fn || q != cudaDriverEntryPointSuccess) return fail(CC_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   auto encode = reinterpret_cast<EncodeTiledFn>(fn);
   const int nb = (int)c->blocks.size();
-  std::vector<CUtensorMap> maps(3 * 2 * (size_t)nb);
+  std::vector<CUtensorMap> maps(kTmaShapes * 2 * (size_t)nb);
   const size_t E = c->elem;
-  for (int shape = 0; shape < 3; ++shape)
+  for (int shape = 0; shape < kTmaShapes; ++shape)
   for (int buf = 0; buf < 2; ++buf)
     for (int b = 0; b < nb; ++b) {
       const HostBlock &h = c->blocks[b];
       const cuuint64_t dims[4] = {(cuuint64_t)h.nx, (cuuint64_t)h.ny, (cuuint64_t)h.nz, (cuuint64_t)np_of(c)};
       const cuuint64_t strides[3] = {(cuuint64_t)h.nx * E, (cuuint64_t)h.nx * h.ny * E, (cuuint64_t)c->N * E};
-      const cuuint32_t box[4] = {(cuuint32_t)(kTX + 4), (cuuint32_t)(kTmaTileRows[shape] + 4), 1u,
+      const cuuint32_t box[4] = {(cuuint32_t)(kTmaTileCols[shape] + 4), (cuuint32_t)(kTmaTileRows[shape] + 4), 1u,
                                  (cuuint32_t)np_of(c)};
       const cuuint32_t estr[4] = {1, 1, 1, 1};
       void *base = (char *)c->P[buf] + (size_t)h.off * E;
@@ -449,7 +457,7 @@ int build_tensor_maps(cc_ctx *c) {
 // copies that rewrite an owned interior point (their post-exchange time step).
 int apply_ownership(cc_ctx *c) {
   build_tiles_kz(c, c->kz);
-  build_face_tiles(c, c->face_ty, c->kz);
+  build_face_tiles(c, c->face_ty, c->kz, c->face_tx);
   build_edge_tiles(c);
   c->hblocks_owned.clear();
   int64_t off = 0;
@@ -901,11 +909,12 @@ int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, i
     if (variant == 2) {
       CK((Launch<T, NS>::faces(a, c->chem, nt, n_edge, c->stream)));
     } else {  // regular tiles from TMA-staged planes (persistent CTAs for 4), edge tiles through L1
-      const CUtensorMap *maps = c->d_tmaps + ((size_t)tma_shape(c->face_ty) * 2 + pc) * c->blocks.size();
+      const CUtensorMap *maps =
+          c->d_tmaps + ((size_t)tma_shape(c->face_ty, c->face_tx) * 2 + pc) * c->blocks.size();
       if (variant == 3)
-        CK((Launch<T, NS>::faces_tma(a, face_tiles, c->face_ty, maps, c->chem, n_ft, c->stream)));
+        CK((Launch<T, NS>::faces_tma(a, face_tiles, c->face_ty, c->face_tx, maps, c->chem, n_ft, c->stream)));
       else
-        CK((Launch<T, NS>::faces_tma_persistent(a, face_tiles, c->face_ty, maps, c->chem, n_ft, c->d_ticket,
+        CK((Launch<T, NS>::faces_tma_persistent(a, face_tiles, c->face_ty, c->face_tx, maps, c->chem, n_ft, c->d_ticket,
                                                 c->stream)));
       CK((Launch<T, NS>::faces(a, c->chem, 0, n_edge, c->stream)));
     }
@@ -952,7 +961,7 @@ int lusgs_and_halo(cc_ctx *c, StageArgs<T> a, int pn, int pc) {
   a.edge_tiles = c->d_edges;
   if (int r = prof_event(c, c->ev_stage, c->ev_next_stage)) return r;
   if (c->tma_ok && c->d_tmaps) {  // the regular 32 x 8 tiles
-    CK((Launch<T, NS>::faces_tma(a, c->d_tiles, 8, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt,
+    CK((Launch<T, NS>::faces_tma(a, c->d_tiles, 8, kTX, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt,
                                  c->stream)));
     CK((Launch<T, NS>::faces(a, c->chem, 0, n_edge, c->stream)));
   } else {
@@ -1082,7 +1091,7 @@ int autotune(cc_ctx *c) {
   double best = 1e300;
   int best_kz = c->kz;
   int best_variant = 0;
-  int best_ty = c->face_ty;
+  int best_ty = c->face_ty, best_tx = c->face_tx;
   if (c->force_kz > 0) kzs.assign(1, c->force_kz);
   std::vector<int> variants;
   if (c->force_variant >= 0 && !variant_ok(c, c->force_variant))
@@ -1097,21 +1106,38 @@ int autotune(cc_ctx *c) {
   // tiles are 32 x 8), those whose plane ring fits in shared memory
   std::vector<int> tys;
   for (int ty : {4, 8, 16})
-    if ((c->force_ty <= 0 || ty == c->force_ty) && Launch<T, NS>::faces_tma_smem(ty) != 0) tys.push_back(ty);
+    if ((c->force_ty <= 0 || ty == c->force_ty) &&
+        (Launch<T, NS>::faces_tma_smem(ty, 32) != 0 || Launch<T, NS>::faces_tma_smem(ty, 16) != 0))
+      tys.push_back(ty);
   if (tys.empty()) return fail(CC_ERR_ARG, "the face tile height does not fit in shared memory in this precision");
   std::vector<int> occs = c->precision == CC_FP64 ? std::vector<int>{0} : std::vector<int>{0, 1};
   if (const char *oe = std::getenv("CC_UPDATE_OCC"))  // pins it (profiling runs, whose timings are distorted)
     occs.assign(1, c->precision == CC_FP64 ? 0 : (oe[0] == '1' ? 1 : 0));
   int best_occ = 0;
+  // tile widths of the TMA face kernels: 32, and 16 (with heights 8 and 16)
+  // for variants 3-4, whose narrower tiles waste fewer lanes on blocks whose
+  // extent is not a multiple of 32
+  auto txs_of = [&](int variant, int ty) {
+    std::vector<int> v;
+    for (int tx : {32, 16}) {
+      if (c->force_tx > 0 && tx != c->force_tx) continue;
+      if (tx == 16 && (variant < 3 || variant > 4 || ty == 4)) continue;
+      if (Launch<T, NS>::faces_tma_smem(ty, tx) == 0) continue;
+      v.push_back(tx);
+    }
+    if (v.empty() && (variant < 3 || variant > 4)) v.push_back(32);
+    return v;
+  };
   for (int variant : variants) {
     for (int ty : (variant >= 3 ? tys : std::vector<int>{8})) {
+      for (int tx : txs_of(variant, ty)) {
       for (int occ : (variant >= 2 ? occs : std::vector<int>{0})) {
       c->update_occ = occ;
       for (int kz : kzs) {
         build_tiles_kz(c, kz);
         CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
                            c->stream));
-        build_face_tiles(c, ty, kz);
+        build_face_tiles(c, ty, kz, tx);
         CK(cudaMemcpyAsync(c->d_ftiles, c->hftiles.data(), sizeof(Tile) * c->hftiles.size(), cudaMemcpyHostToDevice,
                            c->stream));
         const int nt = (int)c->htiles.size();
@@ -1124,10 +1150,12 @@ int autotune(cc_ctx *c) {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, e0, e1));
         if (verbose)
-          std::fprintf(stderr, "cc autotune: %s tile 32x%dx%d update-occ %d tiles=%d %.4f ms\n",
-                       kVariantName[variant], variant >= 3 ? ty : kTY, kz, occ,
+          std::fprintf(stderr, "cc autotune: %s tile %dx%dx%d update-occ %d tiles=%d %.4f ms\n",
+                       kVariantName[variant], variant >= 3 ? tx : kTX, variant >= 3 ? ty : kTY, kz, occ,
                        variant >= 3 ? (int)c->hftiles.size() : nt, ms / 3);
-        if (ms / 3 < best) best = ms / 3, best_kz = kz, best_variant = variant, best_ty = ty, best_occ = occ;
+        if (ms / 3 < best)
+          best = ms / 3, best_kz = kz, best_variant = variant, best_ty = ty, best_tx = tx, best_occ = occ;
+      }
       }
       }
     }
@@ -1135,10 +1163,11 @@ int autotune(cc_ctx *c) {
   c->update_occ = best_occ;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (best == 1e300) return fail(CC_ERR_ARG, "the face tile does not fit in shared memory in this precision");
   build_tiles_kz(c, best_kz);
   CK(cudaMemcpyAsync(c->d_tiles, c->htiles.data(), sizeof(Tile) * c->htiles.size(), cudaMemcpyHostToDevice,
                      c->stream));
-  build_face_tiles(c, best_variant >= 3 ? best_ty : 8, best_kz);
+  build_face_tiles(c, best_variant >= 3 ? best_ty : 8, best_kz, best_variant >= 3 ? best_tx : 32);
   CK(cudaMemcpyAsync(c->d_ftiles, c->hftiles.data(), sizeof(Tile) * c->hftiles.size(), cudaMemcpyHostToDevice,
                      c->stream));
   c->variant = best_variant;
@@ -1775,10 +1804,17 @@ int cc_tuning(cc_ctx *c, int *variant, int *kz, double *stage_ms, int tile[3]) {
   if (kz) *kz = c->kz;
   if (stage_ms) *stage_ms = c->tuned_ms;
   if (tile) {
-    tile[0] = kTX;
+    tile[0] = c->variant >= 3 ? c->face_tx : kTX;
     tile[1] = c->variant >= 3 ? c->face_ty : kTY;
     tile[2] = c->kz;
   }
+  return 0;
+}
+
+int cc_set_tile_width(cc_ctx *c, int tile_i) {
+  if (int r = check_ctx(c)) return r;
+  if (tile_i != 0 && tile_i != 16 && tile_i != 32) return fail(CC_ERR_ARG, "tile_i must be 0 (autotune), 16 or 32");
+  c->force_tx = tile_i;
   return 0;
 }
 

@@ -1,6 +1,7 @@
 // Definitions of the templated launchers (included by inst_*.cu only).
 #pragma once
 #include <algorithm>
+#include <type_traits>
 
 #include "launch.h"
 #include "stage.cuh"
@@ -42,38 +43,50 @@ cudaError_t Launch<T, NS>::faces(const StageArgs<T> &a, const ChemParams &C, int
   return cudaGetLastError();
 }
 
-template <typename T, int NS>
-size_t Launch<T, NS>::faces_tma_smem(int ty) {
-  size_t b = ty == 4 ? FacesTmaLayout<T, NS, 4>::kBytes
-                     : (ty == 16 ? FacesTmaLayout<T, NS, 16>::kBytes : FacesTmaLayout<T, NS, 8>::kBytes);
-  return b <= 227 * 1024 ? b : 0;
+// (ty, tx) -> the instantiated tile shapes of the TMA face kernel: 32 x 4,
+// 32 x 8, 32 x 16, 16 x 8 and 16 x 16 points (i x j); f gets both as
+// integral constants.
+template <typename F>
+cudaError_t with_face_shape(int ty, int tx, F &&f) {
+  using std::integral_constant;
+  if (tx == 32) {
+    if (ty == 4) return f(integral_constant<int, 4>{}, integral_constant<int, 32>{});
+    if (ty == 8) return f(integral_constant<int, 8>{}, integral_constant<int, 32>{});
+    if (ty == 16) return f(integral_constant<int, 16>{}, integral_constant<int, 32>{});
+  } else if (tx == 16) {
+    if (ty == 8) return f(integral_constant<int, 8>{}, integral_constant<int, 16>{});
+    if (ty == 16) return f(integral_constant<int, 16>{}, integral_constant<int, 16>{});
+  }
+  return cudaErrorInvalidValue;
 }
 
-// Whether the ring of the TMA face kernel of tile height TY fits in shared
-// memory (32 x 16 does not in FP64): only those kernels are instantiated.
-template <typename T, int NS, int TY>
-struct FacesTmaFits {
-  static constexpr bool value = FacesTmaLayout<T, NS, TY>::kOk;
-};
+template <typename T, int NS>
+size_t Launch<T, NS>::faces_tma_smem(int ty, int tx) {
+  size_t b = 0;
+  with_face_shape(ty, tx, [&](auto ty_c, auto tx_c) {
+    using L = FacesTmaLayout<T, NS, decltype(ty_c)::value, decltype(tx_c)::value>;
+    b = L::kOk ? L::kBytes : 0;
+    return cudaSuccess;
+  });
+  return b;
+}
 
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::faces_tma(const StageArgs<T> &a, const Tile *tiles, int ty, const void *maps,
+cudaError_t Launch<T, NS>::faces_tma(const StageArgs<T> &a, const Tile *tiles, int ty, int tx, const void *maps,
                                      const ChemParams &C, int n_tiles, cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;
-  const size_t smem = faces_tma_smem(ty);
+  const size_t smem = faces_tma_smem(ty, tx);
   if (smem == 0) return cudaErrorInvalidConfiguration;
   const CUtensorMap *m = (const CUtensorMap *)maps;
-  if (ty == 4) {
-    k_faces_tma<T, NS, 4><<<n_tiles, dim3(kTX, 4), smem, s>>>(a, tiles, m, C);
-  } else if (ty == 8) {
-    k_faces_tma<T, NS, 8><<<n_tiles, dim3(kTX, 8), smem, s>>>(a, tiles, m, C);
-  } else if (ty == 16) {
-    if constexpr (FacesTmaFits<T, NS, 16>::value)
-      k_faces_tma<T, NS, 16><<<n_tiles, dim3(kTX, 16), smem, s>>>(a, tiles, m, C);
-  } else {
-    return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
+  return with_face_shape(ty, tx, [&](auto ty_c, auto tx_c) -> cudaError_t {
+    constexpr int TY = decltype(ty_c)::value, TX = decltype(tx_c)::value;
+    if constexpr (!FacesTmaLayout<T, NS, TY, TX>::kOk) {
+      return cudaErrorInvalidConfiguration;  // the ring does not fit (32 x 16, 16 x 16 in FP64)
+    } else {
+      k_faces_tma<T, NS, TY, TX><<<n_tiles, dim3(TX, TY), smem, s>>>(a, tiles, m, C);
+      return cudaGetLastError();
+    }
+  });
 }
 
 // y-exchange rounds of the dq face kernel per tile height (shared memory)
@@ -111,41 +124,33 @@ cudaError_t Launch<T, NS>::faces_dq(const StageArgs<T> &a, const Tile *tiles, co
 }
 
 template <typename T, int NS>
-cudaError_t Launch<T, NS>::faces_tma_persistent(const StageArgs<T> &a, const Tile *tiles, int ty, const void *maps,
-                                                const ChemParams &C, int n_tiles, unsigned *ticket, cudaStream_t s) {
+cudaError_t Launch<T, NS>::faces_tma_persistent(const StageArgs<T> &a, const Tile *tiles, int ty, int tx,
+                                                const void *maps, const ChemParams &C, int n_tiles, unsigned *ticket,
+                                                cudaStream_t s) {
   if (n_tiles <= 0) return cudaSuccess;
-  const size_t smem = faces_tma_smem(ty);
-  if (smem == 0 || (ty != 4 && ty != 8 && ty != 16)) return cudaErrorInvalidConfiguration;
-  static int per_sm[3] = {0, 0, 0}, n_sm = 0;  // CTAs per SM for ty = 4, 8, 16
-  const int si = ty == 4 ? 0 : (ty == 8 ? 1 : 2);
-  if (per_sm[si] == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    if (ty == 4) {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[si], k_faces_tma_persistent<T, NS, 4>, kTX * 4, smem);
-    } else if (ty == 8) {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[si], k_faces_tma_persistent<T, NS, 8>, kTX * 8, smem);
-    } else {
-      if constexpr (FacesTmaFits<T, NS, 16>::value)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[si], k_faces_tma_persistent<T, NS, 16>, kTX * 16,
-                                                      smem);
-    }
-    per_sm[si] = std::max(1, per_sm[si]);
-  }
-  cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), s);
-  if (e != cudaSuccess) return e;
-  const int grid = std::min(n_tiles, n_sm * per_sm[si]);
+  const size_t smem = faces_tma_smem(ty, tx);
+  if (smem == 0) return cudaErrorInvalidConfiguration;
   const CUtensorMap *m = (const CUtensorMap *)maps;
-  if (ty == 4) {
-    k_faces_tma_persistent<T, NS, 4><<<grid, dim3(kTX, 4), smem, s>>>(a, tiles, m, C, n_tiles, ticket);
-  } else if (ty == 8) {
-    k_faces_tma_persistent<T, NS, 8><<<grid, dim3(kTX, 8), smem, s>>>(a, tiles, m, C, n_tiles, ticket);
-  } else {
-    if constexpr (FacesTmaFits<T, NS, 16>::value)
-      k_faces_tma_persistent<T, NS, 16><<<grid, dim3(kTX, 16), smem, s>>>(a, tiles, m, C, n_tiles, ticket);
-  }
-  return cudaGetLastError();
+  return with_face_shape(ty, tx, [&](auto ty_c, auto tx_c) -> cudaError_t {
+    constexpr int TY = decltype(ty_c)::value, TX = decltype(tx_c)::value;
+    if constexpr (!FacesTmaLayout<T, NS, TY, TX>::kOk) {
+      return cudaErrorInvalidConfiguration;
+    } else {
+      static int per_sm = 0, n_sm = 0;  // CTAs per SM of this shape, SMs
+      if (per_sm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_faces_tma_persistent<T, NS, TY, TX>, TX * TY, smem);
+        per_sm = std::max(1, per_sm);
+      }
+      cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), s);
+      if (e != cudaSuccess) return e;
+      const int grid = std::min(n_tiles, n_sm * per_sm);
+      k_faces_tma_persistent<T, NS, TY, TX><<<grid, dim3(TX, TY), smem, s>>>(a, tiles, m, C, n_tiles, ticket);
+      return cudaGetLastError();
+    }
+  });
 }
 
 template <typename T, int NS>
@@ -201,17 +206,20 @@ cudaError_t Launch<T, NS>::configure() {
   if (e != cudaSuccess) return e;
   if (stage_tma_smem() <= 227 * 1024)
     e = cudaFuncSetAttribute(k_stage_tma<T, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_tma_smem());
-  auto faces_attr = [&](auto kernel, int ty) {
-    if (e == cudaSuccess && faces_tma_smem(ty) != 0)
-      e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)faces_tma_smem(ty));
-  };
-  faces_attr(k_faces_tma<T, NS, 4>, 4);
-  faces_attr(k_faces_tma<T, NS, 8>, 8);
-  faces_attr(k_faces_tma_persistent<T, NS, 4>, 4);
-  faces_attr(k_faces_tma_persistent<T, NS, 8>, 8);
-  if constexpr (FacesTmaFits<T, NS, 16>::value) {
-    faces_attr(k_faces_tma<T, NS, 16>, 16);
-    faces_attr(k_faces_tma_persistent<T, NS, 16>, 16);
+  for (const int sh : {0, 1, 2, 3, 4}) {  // every tile shape of the TMA face kernel whose ring fits
+    const int ty = sh == 0 ? 4 : (sh == 1 || sh == 3 ? 8 : 16), tx = sh < 3 ? 32 : 16;
+    with_face_shape(ty, tx, [&](auto ty_c, auto tx_c) -> cudaError_t {
+      constexpr int TY = decltype(ty_c)::value, TX = decltype(tx_c)::value;
+      if constexpr (FacesTmaLayout<T, NS, TY, TX>::kOk) {
+        const int bytes = (int)FacesTmaLayout<T, NS, TY, TX>::kBytes;
+        if (e == cudaSuccess)
+          e = cudaFuncSetAttribute(k_faces_tma<T, NS, TY, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e == cudaSuccess)
+          e = cudaFuncSetAttribute(k_faces_tma_persistent<T, NS, TY, TX>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      }
+      return cudaSuccess;
+    });
   }
   if constexpr (NS != 0) {  // the closure kernel (set here too, before any stream capture)
     if (e == cudaSuccess)

@@ -24,22 +24,21 @@ struct Launch {
   // update kernel; high_occ = 1 runs the FP32 form sized for 4 CTAs per SM
   static cudaError_t update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s,
                             int high_occ = 0);
-  // split variant with TMA-staged planes in the face kernel (regular tiles only)
-  // TMA face kernel on tiles of 32 x ty points (ty = 4, 8, 16; 16 in FP32
-  // only): smem 0 when the ring does not fit
-  static size_t faces_tma_smem(int ty = 8);
-  static cudaError_t faces_tma(const StageArgs<T> &a, const Tile *tiles, int ty, const void *maps, const ChemParams &C,
-                               int n_tiles,
-                               cudaStream_t s);
+  // split variant with TMA-staged planes in the face kernel: tiles of tx x ty
+  // points (32 x 4, 32 x 8, 32 x 16, 16 x 8, 16 x 16; the x 16 shapes in FP32
+  // only), smem 0 when the ring does not fit
+  static size_t faces_tma_smem(int ty = 8, int tx = 32);
+  static cudaError_t faces_tma(const StageArgs<T> &a, const Tile *tiles, int ty, int tx, const void *maps,
+                               const ChemParams &C, int n_tiles, cudaStream_t s);
   // persistent form: resident CTAs take the n_tiles regular tiles from *ticket (zeroed here)
+  static cudaError_t faces_tma_persistent(const StageArgs<T> &a, const Tile *tiles, int ty, int tx, const void *maps,
+                                          const ChemParams &C, int n_tiles, unsigned *ticket, cudaStream_t s);
   // face kernel that differences the faces in the tile and writes dq
   // (stage_dq.cuh): tiles of 32 x ty points (ty = 4, 8, 16), FP32 bulk
   // precision with 0 or 9 species only
   static size_t faces_dq_smem(int ty);
   static cudaError_t faces_dq(const StageArgs<T> &a, const Tile *tiles, const void *maps, const ChemParams &C,
                               int n_tiles, int ty, cudaStream_t s);
-  static cudaError_t faces_tma_persistent(const StageArgs<T> &a, const Tile *tiles, int ty, const void *maps,
-                                          const ChemParams &C, int n_tiles, unsigned *ticket, cudaStream_t s);
   // learned transport closure (closure.cuh) over every arena point; cl is a ClosureDev
   static cudaError_t props_mlp(const T *P, T *Pr, int64_t N, const void *cl, unsigned *status, const ChemParams &C,
                                cudaStream_t s);

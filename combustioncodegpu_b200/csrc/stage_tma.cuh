@@ -362,9 +362,9 @@ struct SmemStencilT {
 // TY = 16 (16 warps, FP32 only) once.  Transport and geometry are read
 // through L1; the edge tiles stay with k_faces.  Waits are bounded as in
 // k_stage_tma.
-template <typename T, int NS, int TY = kTY>
+template <typename T, int NS, int TY = kTY, int TX = kTX>
 struct FacesTmaLayout {
-  static constexpr int HX = kTX + 4, HY = TY + 4, PV = HX * HY;
+  static constexpr int HX = TX + 4, HY = TY + 4, PV = HX * HY;
   static constexpr int kRing = 4;
   static constexpr size_t kPlaneBytes = ((sizeof(T) * (6 + SpecCount<NS>::kArr) * PV + 127) / 128) * 128;
   static constexpr size_t kRec = ((sizeof(T) * SpecCount<NS>::kArr * 2 * kRecLen + 15) / 16) * 16;
@@ -388,30 +388,30 @@ struct FacesTmaLayout {
 // of plane kp = k + 2 (1-point halo in j, the tile's i span plus one point
 // on each side), which the faces of plane k + 1 read for the first time
 // through L1.  Rows are spread over the CTA's threads; a hint nothing waits on.
-template <typename T, int TY>
+template <typename T, int TY, int TX>
 __device__ __forceinline__ void prefetch_props_geometry(const StageArgs<T> &a, const BlockInfo &B, const Tile &t,
                                                         int kp, int npr, int tid) {
   const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
   const int j_lo = max(t.j0 - 1, -B.g), j_hi = min(t.j0 + TY + 1, B.my + B.g), nr = j_hi - j_lo;
   const int n = (npr + 10) * nr;
-  for (int e = tid; e < n; e += kTX * TY) {
+  for (int e = tid; e < n; e += TX * TY) {
     const int f = e / nr, j = j_lo + e % nr;
     const T *base = f < npr ? a.Pr + (size_t)f * N : a.G + (size_t)(f - npr) * N;
     const int row = (int)B.base + sk * kp + sj * j;
-    l2_prefetch(base, N, row + t.i0 - 1, row + t.i0 + kTX + 1);
+    l2_prefetch(base, N, row + t.i0 - 1, row + t.i0 + TX + 1);
   }
 }
 
-template <typename T, int NS, int TY>
+template <typename T, int NS, int TY, int TX>
 __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUtensorMap *map, const ChemParams &C,
                                               uint64_t *bars, unsigned char *ring, const T *sRec, const Tile &t,
                                               unsigned pc0, bool &aborted) {
-  using L = FacesTmaLayout<T, NS, TY>;
+  using L = FacesTmaLayout<T, NS, TY, TX>;
   constexpr int NV = 5 + SpecCount<NS>::kArr;
   const int ns = SpecCount<NS>::n(C);
   const int nv = 5 + ns;
   const BlockInfo B = a.blocks[t.blk];
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i = t.i0 + tx, j = t.j0 + ty;
   const bool act = (i < B.mx) && (j < B.my);
   const int N = (int)a.N, sj = B.nx, sk = B.nx * B.ny;
@@ -465,7 +465,7 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
     const int p = col + sk * k;
     // (FP64 only: measured faster there, slower in FP32, whose smaller rows
     // stay in L2 without it)
-    if (sizeof(T) == 8 && k + 2 <= B.mz - 1 + B.g) prefetch_props_geometry<T, TY>(a, B, t, k + 2, 2 + ns, tid);
+    if (sizeof(T) == 8 && k + 2 <= B.mz - 1 + B.g) prefetch_props_geometry<T, TY, TX>(a, B, t, k + 2, 2 + ns, tid);
     if (act) {
       // two faces interleaved in FP32 (their loads overlap: 0.74 -> 0.71 ms
       // per launch at 128^3 despite the spills); one at a time in FP64, and
@@ -504,38 +504,38 @@ __device__ __forceinline__ int faces_tma_tile(const StageArgs<T> &a, const CUten
   return klast - kfirst + 1;
 }
 
-template <typename T, int NS, int TY>
-__global__ void __launch_bounds__(kTX *TY, (FacesTmaLayout<T, NS, TY>::kMinBlocks))
+template <typename T, int NS, int TY, int TX = kTX>
+__global__ void __launch_bounds__(TX *TY, (FacesTmaLayout<T, NS, TY, TX>::kMinBlocks))
     k_faces_tma(const StageArgs<T> a, const Tile *__restrict__ tiles, const CUtensorMap *__restrict__ maps,
                 const __grid_constant__ ChemParams C) {
-  using L = FacesTmaLayout<T, NS, TY>;
+  using L = FacesTmaLayout<T, NS, TY, TX>;
   const int ns = SpecCount<NS>::n(C);
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char *smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
   unsigned char *ring = smem_raw + 128;
   T *sRec = reinterpret_cast<T *>(ring + L::kRing * L::kPlaneBytes);
-  const int tid = threadIdx.y * kTX + threadIdx.x;
+  const int tid = threadIdx.y * TX + threadIdx.x;
   const Tile t = tiles[blockIdx.x];
-  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * TY) sRec[e] = param_rec<T>(C)[e];
+  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += TX * TY) sRec[e] = param_rec<T>(C)[e];
   if (tid == 0) {
     for (int b = 0; b < L::kRing; ++b) mbar_init(&bars[b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
   bool aborted;
-  faces_tma_tile<T, NS, TY>(a, maps + t.blk, C, bars, ring, sRec, t, 0u, aborted);
+  faces_tma_tile<T, NS, TY, TX>(a, maps + t.blk, C, bars, ring, sRec, t, 0u, aborted);
 }
 
 // Persistent form of k_faces_tma: as many CTAs as fit on the GPU take the
 // regular tiles in order from a device counter (zeroed before the launch),
 // initialising the NASA records and the mbarriers once; the plane count
 // carries the mbarrier phases from one tile to the next.
-template <typename T, int NS, int TY>
-__global__ void __launch_bounds__(kTX *TY, (FacesTmaLayout<T, NS, TY>::kMinBlocks))
+template <typename T, int NS, int TY, int TX = kTX>
+__global__ void __launch_bounds__(TX *TY, (FacesTmaLayout<T, NS, TY, TX>::kMinBlocks))
     k_faces_tma_persistent(const StageArgs<T> a, const Tile *__restrict__ tiles, const CUtensorMap *__restrict__ maps,
                            const __grid_constant__ ChemParams C, int n_tiles, unsigned *ticket) {
-  using L = FacesTmaLayout<T, NS, TY>;
+  using L = FacesTmaLayout<T, NS, TY, TX>;
   const int ns = SpecCount<NS>::n(C);
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char *smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
@@ -543,8 +543,8 @@ __global__ void __launch_bounds__(kTX *TY, (FacesTmaLayout<T, NS, TY>::kMinBlock
   unsigned char *ring = smem_raw + 128;
   T *sRec = reinterpret_cast<T *>(ring + L::kRing * L::kPlaneBytes);
   __shared__ int sh_tile;
-  const int tid = threadIdx.y * kTX + threadIdx.x;
-  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * TY) sRec[e] = param_rec<T>(C)[e];
+  const int tid = threadIdx.y * TX + threadIdx.x;
+  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += TX * TY) sRec[e] = param_rec<T>(C)[e];
   if (tid == 0) {
     for (int b = 0; b < L::kRing; ++b) mbar_init(&bars[b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -557,7 +557,7 @@ __global__ void __launch_bounds__(kTX *TY, (FacesTmaLayout<T, NS, TY>::kMinBlock
     __syncthreads();  // every thread has its tile index before the next ticket
     if (ti >= n_tiles) break;
     bool aborted;
-    pc += (unsigned)faces_tma_tile<T, NS, TY>(a, maps + tiles[ti].blk, C, bars, ring, sRec, tiles[ti], pc, aborted);
+    pc += (unsigned)faces_tma_tile<T, NS, TY, TX>(a, maps + tiles[ti].blk, C, bars, ring, sRec, tiles[ti], pc, aborted);
     if (aborted) break;
   }
 }

@@ -230,6 +230,12 @@ int cc_tuning(cc_ctx *ctx, int *variant, int *kz, double *stage_ms, int tile[3])
  * Before cc_init it applies to the first cc_init; after it, the new
  * configuration is timed and used from the next cc_step on. */
 int cc_set_tuning(cc_ctx *ctx, int variant, int kz, int tile_j);
+/* Points along i of the TMA face kernel's tile in variants 3 and 4: 32 (one
+ * warp per row), 16 (two rows per warp, with tile heights 8 and 16; fewer
+ * idle lanes on blocks whose i extent is not a multiple of 32), or 0 =
+ * autotune (default).  Applies from the next tuning: cc_init or
+ * cc_set_tuning. */
+int cc_set_tile_width(cc_ctx *ctx, int tile_i);
 /* Launch granularity of the stage kernels: 0 (default) = one launch per
  * kernel over the tiles of every block; 1 = one launch per block per kernel,
  * the reference's granularity (Driver.cu:144-177 launches per block), kept for

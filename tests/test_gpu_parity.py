@@ -173,17 +173,18 @@ def test_dq_variant_tile_shape_and_chunking_are_bit_identical():
 @pytest.mark.parametrize("name", ["multiblock", "channel", "box_distorted"])
 def test_face_tile_heights_are_bit_identical(name, precision, variant):
     """The TMA face kernel computes every face of a point once, whichever
-    tile (32 x 4, 32 x 8, 32 x 16 points; 32 x 16 in FP32 only) and k-chunk it
-    falls in: the state after two RK3 steps does not depend on the tile
-    shape, bit for bit."""
+    tile (32 x 4, 32 x 8, 32 x 16, 16 x 8, 16 x 16 points; 32 x 16 in FP32
+    only) and k-chunk it falls in: the state after two RK3 steps does not
+    depend on the tile shape, bit for bit."""
     case = CASES[name]
-    shapes = [(8, 4), (4, 2), (4, 64)] + ([(16, 3), (16, 64)] if precision == "mixed" else [])
+    shapes = [(32, 8, 4), (32, 4, 2), (32, 4, 64), (16, 8, 3), (16, 16, 2)]
+    shapes += [(32, 16, 3), (32, 16, 64)] if precision == "mixed" else []
     out = []
-    for tile_j, kz in shapes:
+    for tile_i, tile_j, kz in shapes:
         d = cc.Driver.from_case(case, precision)
-        d.set_tuning(variant, kz, tile_j)
+        d.set_tuning(variant, kz, tile_j, tile_i)
         d.initialize_computation()
-        assert d.tuning()["tile"] == (32, tile_j, kz)
+        assert d.tuning()["tile"] == (tile_i, tile_j, kz)
         d.simulate(2, "rk3")
         assert d.status() == 0
         out.append([d.field[b].get_state()[2] for b in range(len(case["blocks"]))])
@@ -203,9 +204,10 @@ def test_face_tile_heights_close_to_oracle(tile_j):
 
 
 def test_face_tile_height_16_refused_in_fp64():
-    """The 32 x 16 tile's FP64 plane ring does not fit in shared memory."""
+    """The 32 x 16 tile's FP64 plane ring does not fit in shared memory (the
+    16 x 16 one does)."""
     d = cc.Driver.from_case(CASES["box"], "fp64")
-    d.set_tuning("split-tma", 4, 16)
+    d.set_tuning("split-tma", 4, 16, 32)
     with pytest.raises(RuntimeError, match="does not fit"):
         d.initialize_computation()
     d.close()
