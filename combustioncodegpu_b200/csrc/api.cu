@@ -108,6 +108,10 @@ struct cc_ctx {
   int force_tx = 0;               // cc_set_tile_width: face tile width, 0 = autotune
   int update_occ = 0;             // 1: the FP32 update kernel sized for 4 CTAs per SM (autotuned)
   int force_ty = 0;               // cc_set_tuning: face tile height, 0 = autotune
+  std::vector<Tile> hutiles;      // variants 2-5: tiles of the update kernel (upd_tx x 256/upd_tx x kz)
+  std::vector<int> ut_begin;      // per block: first update tile, + end
+  Tile *d_utiles = nullptr;
+  int upd_tx = 32;                // update tile width: the face tile width in variants 3-4, else 32
   std::vector<Tile> hftiles;      // variants 3-5: tiles of the TMA face kernel
   std::vector<int> ft_begin;      // per block: first face tile (block-ordered list), + end
   Tile *d_ftiles = nullptr;
@@ -349,6 +353,35 @@ void build_tiles_kz(cc_ctx *c, int kz) {
   c->kz = kz;
 }
 
+// Work list of the update kernel of the split variants: ux x (256 / ux)
+// columns (32 x 8 or 16 x 16), k split into chunks of kz.
+void build_update_tiles(cc_ctx *c, int kz, int ux) {
+  const int uy = 256 / ux;
+  c->hutiles.clear();
+  c->ut_begin.clear();
+  for (int bi = 0; bi < (int)c->blocks.size(); ++bi) {
+    c->ut_begin.push_back((int)c->hutiles.size());
+    const auto &b = c->blocks[bi];
+    if (!owns(c, bi)) continue;
+    for (int k0 = 0; k0 < b.mz; k0 += kz)
+      for (int j0 = 0; j0 < b.my; j0 += uy)
+        for (int i0 = 0; i0 < b.mx; i0 += ux) {
+          Tile t{};
+          t.blk = bi, t.i0 = i0, t.j0 = j0, t.k0 = k0, t.k1 = std::min(b.mz, k0 + kz);
+          c->hutiles.push_back(t);
+        }
+  }
+  c->ut_begin.push_back((int)c->hutiles.size());
+  c->upd_tx = ux;
+}
+
+int upload_update_tiles(cc_ctx *c) {
+  if (!c->hutiles.empty())
+    CK(cudaMemcpyAsync(c->d_utiles, c->hutiles.data(), sizeof(Tile) * c->hutiles.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+  return 0;
+}
+
 // Tiles of the split variant's minus-side face layers (stage_split.cuh):
 // i = -1 faces with lanes along j and warps along k, j = -1 faces with lanes
 // along i and warps along k, k = -1 faces with lanes along i, warps along j.
@@ -458,6 +491,8 @@ int build_tensor_maps(cc_ctx *c) {
 int apply_ownership(cc_ctx *c) {
   build_tiles_kz(c, c->kz);
   build_face_tiles(c, c->face_ty, c->kz, c->face_tx);
+  build_update_tiles(c, c->kz, c->upd_tx);
+  if (int r = upload_update_tiles(c)) return r;
   build_edge_tiles(c);
   c->hblocks_owned.clear();
   int64_t off = 0;
@@ -554,6 +589,10 @@ int setup_device(cc_ctx *c) {
   c->d_ftiles = (Tile *)p;
   build_face_tiles(c, c->face_ty, c->kz);
   CK(cudaMemcpyAsync(c->d_ftiles, c->hftiles.data(), sizeof(Tile) * c->hftiles.size(), cudaMemcpyHostToDevice, c->stream));
+  if (dev_alloc(c, &p, sizeof(Tile) * (size_t)std::max(1, max_face_tiles(c)))) return CC_ERR_CUDA;
+  c->d_utiles = (Tile *)p;  // at most as many as 16 x 4 face tiles
+  build_update_tiles(c, c->kz, 32);
+  if (int r = upload_update_tiles(c)) return r;
   for (int b = 0; b < 2; ++b) {
     if (dev_alloc(c, &c->P[b], E * N * np_of(c))) return CC_ERR_CUDA;
     if (dev_alloc(c, &c->Pr[b], E * N * npr_of(c))) return CC_ERR_CUDA;
@@ -867,28 +906,37 @@ bool variant_ok(const cc_ctx *c, int v) {
 // one launch per kernel over all blocks, or (per_block) one per block.
 template <typename T, int NS>
 int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge, const Tile *face_tiles,
-                       int n_ft);
+                       int n_ft, const Tile *upd_tiles, int n_ut);
 
 template <typename T, int NS>
 int launch_stage(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt) {
   if (!c->per_block || c->tile_begin.size() != c->blocks.size() + 1)
     return launch_stage_range<T, NS>(c, a, pc, variant, nt, (int)c->hedges.size(), c->d_ftiles,
-                                     (int)c->hftiles.size());
+                                     (int)c->hftiles.size(), c->d_utiles, (int)c->hutiles.size());
   const Tile *tiles = a.tiles;
   for (size_t b = 0; b < c->blocks.size(); ++b) {
     a.tiles = tiles + c->tile_begin[b];
     a.edge_tiles = c->d_edges + c->edge_begin[b];
     if (int r = launch_stage_range<T, NS>(c, a, pc, variant, c->tile_begin[b + 1] - c->tile_begin[b],
                                           c->edge_begin[b + 1] - c->edge_begin[b], c->d_ftiles + c->ft_begin[b],
-                                          c->ft_begin[b + 1] - c->ft_begin[b]))
+                                          c->ft_begin[b + 1] - c->ft_begin[b], c->d_utiles + c->ut_begin[b],
+                                          c->ut_begin[b + 1] - c->ut_begin[b]))
       return r;
   }
   return 0;
 }
 
+// The update kernel of the split variants over its own tile list.
+template <typename T, int NS>
+int launch_update(cc_ctx *c, StageArgs<T> a, const Tile *upd_tiles, int n_ut) {
+  a.tiles = upd_tiles;
+  CK((Launch<T, NS>::update(a, c->chem, n_ut, c->stream, c->update_occ, c->upd_tx)));
+  return 0;
+}
+
 template <typename T, int NS>
 int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, int n_edge, const Tile *face_tiles,
-                       int n_ft) {
+                       int n_ft, const Tile *upd_tiles, int n_ut) {
   if ((variant == 1 || variant == 3 || variant == 4 || variant == 5) && !c->d_tmaps)
     return fail(CC_ERR_STATE, "TMA variant without tensor maps");
   if (variant == 5) {  // faces differenced in the tile (dq), then the update
@@ -898,8 +946,7 @@ int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, i
     CK((Launch<T, NS>::faces_dq(a, face_tiles, c->d_tmaps + ((size_t)tma_shape(c->face_ty) * 2 + pc) * nb, c->chem,
                                 n_ft, c->face_ty, c->stream)));
     if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
-    CK((Launch<T, NS>::update(a, c->chem, nt, c->stream, c->update_occ)));
-    return 0;
+    return launch_update<T, NS>(c, a, upd_tiles, n_ut);
   }
   if (variant == 1) {
     CK((Launch<T, NS>::stage_tma(a, c->d_tmaps + (size_t)pc * c->blocks.size(), c->chem, nt, c->stream)));
@@ -919,7 +966,7 @@ int launch_stage_range(cc_ctx *c, StageArgs<T> a, int pc, int variant, int nt, i
       CK((Launch<T, NS>::faces(a, c->chem, 0, n_edge, c->stream)));
     }
     if (int r = prof_event(c, c->ev_mid, c->ev_next_mid)) return r;
-    CK((Launch<T, NS>::update(a, c->chem, nt, c->stream, c->update_occ)));
+    if (int r = launch_update<T, NS>(c, a, upd_tiles, n_ut)) return r;
   } else {
     CK((Launch<T, NS>::stage(a, c->chem, nt, c->stream)));
   }
@@ -1140,6 +1187,8 @@ int autotune(cc_ctx *c) {
         build_face_tiles(c, ty, kz, tx);
         CK(cudaMemcpyAsync(c->d_ftiles, c->hftiles.data(), sizeof(Tile) * c->hftiles.size(), cudaMemcpyHostToDevice,
                            c->stream));
+        build_update_tiles(c, kz, variant == 3 || variant == 4 ? tx : 32);
+        if (int r = upload_update_tiles(c)) return r;
         const int nt = (int)c->htiles.size();
         if (int r = launch_stage<T, NS>(c, a, pc, variant, nt)) return r;
         CK(cudaEventRecord(e0, c->stream));
@@ -1170,6 +1219,8 @@ int autotune(cc_ctx *c) {
   build_face_tiles(c, best_variant >= 3 ? best_ty : 8, best_kz, best_variant >= 3 ? best_tx : 32);
   CK(cudaMemcpyAsync(c->d_ftiles, c->hftiles.data(), sizeof(Tile) * c->hftiles.size(), cudaMemcpyHostToDevice,
                      c->stream));
+  build_update_tiles(c, best_kz, best_variant == 3 || best_variant == 4 ? best_tx : 32);
+  if (int r = upload_update_tiles(c)) return r;
   c->variant = best_variant;
   c->tuned_ms = best;
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream));

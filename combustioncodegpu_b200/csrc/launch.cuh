@@ -155,15 +155,24 @@ cudaError_t Launch<T, NS>::faces_tma_persistent(const StageArgs<T> &a, const Til
 
 template <typename T, int NS>
 cudaError_t Launch<T, NS>::update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s,
-                                  int high_occ) {
+                                  int high_occ, int ux) {
   if (n_tiles <= 0) return cudaSuccess;
+  if (ux != 32 && ux != 16) return cudaErrorInvalidValue;
+  const dim3 block(ux, 256 / ux);
   if constexpr (sizeof(T) == 4) {
     if (high_occ) {
-      k_update<T, NS, 4><<<n_tiles, dim3(kTX, kTY), update_smem(), s>>>(a, C);
+      if (ux == 16)
+        k_update<T, NS, 4, 16><<<n_tiles, block, update_smem(), s>>>(a, C);
+      else
+        k_update<T, NS, 4, 32><<<n_tiles, block, update_smem(), s>>>(a, C);
       return cudaGetLastError();
     }
   }
-  k_update<T, NS><<<n_tiles, dim3(kTX, kTY), update_smem(), s>>>(a, C);
+  constexpr int kMinb = sizeof(T) == 8 ? 2 : 3;
+  if (ux == 16)
+    k_update<T, NS, kMinb, 16><<<n_tiles, block, update_smem(), s>>>(a, C);
+  else
+    k_update<T, NS, kMinb, 32><<<n_tiles, block, update_smem(), s>>>(a, C);
   return cudaGetLastError();
 }
 

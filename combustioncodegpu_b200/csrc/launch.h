@@ -22,8 +22,9 @@ struct Launch {
   static size_t update_smem();
   static cudaError_t faces(const StageArgs<T> &a, const ChemParams &C, int n_regular, int n_edge, cudaStream_t s);
   // update kernel; high_occ = 1 runs the FP32 form sized for 4 CTAs per SM
+  // ux: tile width, 32 (32 x 8 tiles) or 16 (16 x 16)
   static cudaError_t update(const StageArgs<T> &a, const ChemParams &C, int n_tiles, cudaStream_t s,
-                            int high_occ = 0);
+                            int high_occ = 0, int ux = 32);
   // split variant with TMA-staged planes in the face kernel: tiles of tx x ty
   // points (32 x 4, 32 x 8, 32 x 16, 16 x 8, 16 x 16; the x 16 shapes in FP32
   // only), smem 0 when the ring does not fit

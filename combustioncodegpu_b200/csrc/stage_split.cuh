@@ -83,10 +83,12 @@ __global__ void __launch_bounds__(kTX *kTY, sizeof(T) == 8 ? 1 : 2)
 }
 
 // MINB: CTAs per SM the registers are sized for (the autotuner tries 4 in
-// FP32: 64 registers with some spills against 80 at 3).
-template <typename T, int NS, int MINB = (sizeof(T) == 8 ? 2 : 3)>
-__global__ void __launch_bounds__(kTX *kTY, MINB)
+// FP32: 64 registers with some spills against 80 at 3).  Tiles of UX x
+// (256 / UX) points: 32 x 8, or 16 x 16 beside the 16-wide face tiles.
+template <typename T, int NS, int MINB = (sizeof(T) == 8 ? 2 : 3), int UX = kTX>
+__global__ void __launch_bounds__(256, MINB)
     k_update(const StageArgs<T> a, const __grid_constant__ ChemParams C) {
+  constexpr int UY = 256 / UX;
   constexpr int A = SpecCount<NS>::kArr;
   constexpr int NV = 5 + A;
   const int ns = SpecCount<NS>::n(C);
@@ -94,8 +96,8 @@ __global__ void __launch_bounds__(kTX *kTY, MINB)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *sRecD = reinterpret_cast<double *>(smem_raw);  // [A][2][kRecLen]
   T *sRec = reinterpret_cast<T *>(smem_raw + (sizeof(T) == sizeof(double) ? 0 : StageSmem<T, NS>::kRecD));
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
-  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += kTX * kTY) {
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * UX + tx;
+  for (int e = tid, nrec = ns * 2 * kRecLen; e < nrec; e += UX * UY) {
     sRecD[e] = param_rec<double>(C)[e];
     if (sizeof(T) != sizeof(double)) sRec[e] = param_rec<T>(C)[e];
   }
