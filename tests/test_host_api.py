@@ -124,3 +124,14 @@ def test_multi_process_entry_points_validate_arguments(cclib):
     assert cclib.cc_pack_points(d.ctx, 0, idx.ctypes.data_as(ctypes.c_void_p), 1,
                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == -2  # before cc_init
     d.close()
+
+
+def test_tile_width_argument_checks(cclib):
+    """cc_set_tile_width takes 0 (autotune), 16 or 32 points along i and
+    refuses anything else (no device needed)."""
+    d = cc.Driver.from_case(cases.case_sod(20, 5, 5))
+    for ok in (0, 16, 32):
+        assert cclib.cc_set_tile_width(d.ctx, ok) == 0
+    assert cclib.cc_set_tile_width(d.ctx, 8) == -1
+    assert b"tile_i" in cclib.cc_last_error()
+    d.close()
